@@ -1,0 +1,298 @@
+/*
+ * lbm_b200.h - C ABI of the B200-native D3Q19 step engine.
+ *
+ * This is the drop-in boundary for the per-timestep hot path of the
+ * air-over-waves LES / free-surface solver
+ * (reference: LBM_3D_LES_air_over_waves_CODEX.py).  The reference has no
+ * FFI of its own: its interface is the Python module surface that
+ * run_ab_case.py drives (module globals, Taichi fields, main()).  The
+ * Python host layer of this project re-creates that module surface and
+ * calls down into this ABI through ctypes.
+ *
+ * Conventions
+ *   - Plain C types only; no C++ or torch types cross the boundary.
+ *   - The library never allocates or frees state buffers: the caller owns
+ *     every pointer in lbm_buffers (device pointers for the CUDA library,
+ *     host pointers for the CPU oracle, which exports the same ABI).  The
+ *     CUDA library owns only small scratch arrays, freed by lbm_destroy.
+ *   - Every call returns an int status (LBM_OK or a negative LBM_ERR_*).
+ *     No exceptions cross the ABI.  lbm_last_error() gives a message.
+ *   - A context is bound to one stream and is not thread-safe.  Separate
+ *     contexts may run concurrently on separate streams.
+ *   - 3-D fields are [nz][ny][nx] with x fastest (the reference's Taichi
+ *     field order (Nz, Ny, Nx), CODEX.py:531-620).  Populations are stored
+ *     structure-of-arrays: f[q][nz][ny][nx], q in the D3Q19 order of
+ *     lbm_lattice.py:3-43.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+/* status codes */
+#define LBM_OK 0
+#define LBM_ERR_BAD_ARG (-1)
+#define LBM_ERR_CUDA (-2)
+#define LBM_ERR_NOT_CONVERGED (-3)
+#define LBM_ERR_NONFINITE (-4)
+#define LBM_ERR_UNSUPPORTED (-5)
+#define LBM_ERR_NOT_BOUND (-6)
+
+/* enumerations (values mirror the reference's string options) */
+enum { LBM_FS_NONE = 0, LBM_FS_HEIGHT_STATIC = 1, LBM_FS_HEIGHT_KINEMATIC = 2, LBM_FS_PRESCRIBED_SOLITARY = 3 };
+enum { LBM_TRACK_HEIGHT = 0, LBM_TRACK_VOF = 1 };
+enum { LBM_FSB_CELL = 0, LBM_FSB_HYDROSTATIC = 1 };
+enum { LBM_REFILL_EQUILIBRIUM = 0, LBM_REFILL_NONEQ = 1, LBM_REFILL_DIRECTIONAL = 2 };
+enum { LBM_FSINIT_FLAT = 0, LBM_FSINIT_SOLITARY = 1, LBM_FSINIT_GAUSSIAN = 2 };
+enum { LBM_PRESSURE_TOTAL = 0, LBM_PRESSURE_HYDROSTATIC_BALANCED = 1, LBM_PRESSURE_VOF_COMPONENT_BALANCED = 2 };
+enum { LBM_BED_MOVING_SINE = 0, LBM_BED_FLAT = 1, LBM_BED_PIECEWISE = 2 };
+enum { LBM_COLLIDE_KBC = 0, LBM_COLLIDE_REGULARIZED = 1 };
+enum { LBM_INITVEL_REFERENCE = 0, LBM_INITVEL_UNIFORM = 1 };
+enum { LBM_SOLVEL_NONE = 0, LBM_SOLVEL_SHALLOW = 1, LBM_SOLVEL_SHALLOW_DIVFREE = 2 };
+enum { LBM_STORE_F32 = 0, LBM_STORE_F16S = 1, LBM_STORE_BF16S = 2 };
+
+/* free-surface cell states (CODEX.py:407-409) */
+#define LBM_FS_GAS 0
+#define LBM_FS_LIQUID 1
+#define LBM_FS_INTERFACE 2
+/* wall sources (CODEX.py:401-405) */
+#define LBM_WALL_NONE 0
+#define LBM_WALL_BED 1
+#define LBM_WALL_CUBE 2
+#define LBM_WALL_XMIN 3
+#define LBM_WALL_XMAX 4
+
+/*
+ * Solver constants, exactly as the kernels use them.  The host layer
+ * derives every value from the reference's LBM_* environment options
+ * (CODEX.py:35-529) and rounds to float the way Taichi captures Python
+ * constants into f32 kernels.
+ */
+typedef struct lbm_params {
+    int32_t abi_version;
+    int32_t nx, ny, nz;
+
+    /* ---- modes (CODEX.py:49-208, 355-409, 481-528) ---- */
+    int32_t physics_water;          /* LBM_PHYSICS_MODE: 0 air, 1 water */
+    int32_t fs_mode;                /* LBM_FREE_SURFACE_MODE -> LBM_FS_* */
+    int32_t fs_tracking;            /* LBM_FREE_SURFACE_TRACKING -> LBM_TRACK_* */
+    int32_t fs_boundary;            /* LBM_FREE_SURFACE_BOUNDARY -> LBM_FSB_* */
+    int32_t fs_refill;              /* LBM_FREE_SURFACE_REFILL -> LBM_REFILL_* */
+    int32_t fs_initial;             /* LBM_FREE_SURFACE_INITIAL -> LBM_FSINIT_* */
+    int32_t init_fs_populations;    /* LBM_INIT_FREE_SURFACE_POPULATIONS */
+    int32_t vof_link_aperture;      /* LBM_VOF_LINK_APERTURE */
+    int32_t vof_initial_block;      /* LBM_VOF_INITIAL_SHAPE == block */
+    int32_t pressure_formulation;   /* LBM_PRESSURE_FORMULATION -> LBM_PRESSURE_* */
+    int32_t use_hydrostatic_balanced_pressure;  /* CODEX.py:457-460 */
+    int32_t use_component_balanced_pressure;    /* CODEX.py:454-456 */
+    int32_t x_solid;                /* LBM_X_BOUNDARY == solid */
+    int32_t use_phi_open_fraction;  /* LBM_BOUNDARY_GEOMETRY in (phi_fraction, phi) */
+    int32_t use_phi_open_flags;     /* LBM_BOUNDARY_GEOMETRY == phi */
+    int32_t use_link_wall_velocity; /* LBM_WALL_VELOCITY_SAMPLING == link */
+    int32_t bed_profile;            /* LBM_BED_PROFILE -> LBM_BED_* */
+    int32_t include_bed;            /* LBM_OBSTACLE_MODE in (bed, bed_cube) */
+    int32_t include_cube;           /* LBM_OBSTACLE_MODE in (bed_cube, cube) */
+    int32_t use_les;                /* LBM_USE_LES */
+    int32_t collision;              /* LBM_COLLISION -> LBM_COLLIDE_* */
+    int32_t enable_top_drive;       /* CODEX.py:526 */
+    int32_t enable_x_fringe;        /* CODEX.py:527 */
+    int32_t enable_top_sponge;      /* CODEX.py:528 */
+    int32_t solitary_velocity_mode; /* LBM_SOLITARY_INITIAL_VELOCITY -> LBM_SOLVEL_* */
+    /* extensions (not in the reference; defaults reproduce it) */
+    int32_t top_free_slip;          /* specular top wall for air runs */
+    int32_t init_velocity_mode;     /* LBM_INITVEL_*: reference log-law kick or uniform + noise */
+    int32_t bed_orbital_velocity;   /* 1: reference u_s = c*eta/(h0+eta) terms; 0: u_s = 0 */
+    int32_t pop_storage;            /* LBM_STORE_*: population storage precision */
+
+    /* ---- VOF options (CODEX.py:101-154, 174-184) ---- */
+    int32_t vof_orphan_search_radius;
+    int32_t vof_orphan_max_weak_neighbors;
+    int32_t vof_detached_advection;
+    int32_t vof_detached_max_wet_neighbors;
+    int32_t vof_detached_max_resolved_neighbors;
+    int32_t vof_thin_gap_bridge;
+    int32_t vof_collapse_enabled;
+    int32_t vof_collapse_interval;
+    int32_t vof_collapse_flood_sweeps;
+    int32_t pad0;
+
+    uint64_t seed;                  /* counter-based RNG key (backscatter) */
+
+    /* ---- lattice / physical constants (f32 as the kernels use them) ---- */
+    float dx;                       /* LBM_DX_M */
+    float rho0;                     /* CODEX.py:414 */
+    float tau0;                     /* CODEX.py:466 (or build override) */
+    float nu0;                      /* CODEX.py:465 */
+    float cs_delta_sq;              /* (Cs*Delta)**2, CODEX.py:3094 */
+    float nu_t_max;                 /* CODEX.py:500 */
+    float kappa;                    /* CODEX.py:516 */
+    float z0_phys;                  /* CODEX.py:517 */
+    float wall_dist_floor;          /* 0.001*dx, CODEX.py:3103 */
+    float ti_kick;                  /* TI, CODEX.py:507 */
+    float c_backscatter;            /* LBM_BACKSCATTER */
+    float u_top_lb;                 /* CODEX.py:446 */
+    float u_current_lb;             /* CODEX.py:448 */
+    float g_lb;                     /* CODEX.py:449 */
+    float g_body_lb;                /* CODEX.py:461-463 */
+    float vel_scale;                /* CODEX.py:441 */
+    float dt_phys_f;                /* dt_phys rounded to f32 (in-kernel use) */
+    double dt_phys;                 /* dt_phys in double: t = (step+1)*dt_phys */
+
+    /* bed kinematics (CODEX.py:1082-1162); the reference uses two
+       harmonics: (amp, 0.5k, c) and (amp, k, 0.5c) */
+    float bed_offset_m;
+    float bed_amp1, bed_k1, bed_c1;
+    float bed_amp2, bed_k2, bed_c2;
+    float bed_ramp_time;            /* 2*wave_period (0 = no ramp) */
+    float bed_h0;                   /* depth_swl_m */
+
+    /* cube / prism obstacle (CODEX.py:369-400) */
+    float cube_cx, cube_cy, cube_cz;
+    float cube_hx, cube_hy, cube_hz;
+    float cube_yaw_cos, cube_yaw_sin, cube_pitch_cos, cube_pitch_sin;
+
+    /* free surface (CODEX.py:291-339) */
+    float fs_base_m;
+    float fs_depth_m;
+    float solitary_amp_m, solitary_x0_m, solitary_direction, solitary_celerity, solitary_kappa_inv;
+    float gaussian_amp_m, gaussian_center_x_m, gaussian_sigma_m;
+    float vof_block_xmin, vof_block_xmax, vof_block_ymin, vof_block_ymax, vof_block_zmin, vof_block_zmax;
+
+    /* VOF thresholds */
+    float vof_empty_fill_threshold;
+    float vof_orphan_empty_threshold;
+    float vof_detached_residual_fill_threshold;
+    float vof_thin_gap_bridge_strength;
+    float vof_collapse_max_volume_m3;
+
+    /* extension: uniform initial velocity (LBM_INITVEL_UNIFORM) */
+    float init_u0x, init_u0y, init_u0z, init_noise_amp;
+
+    /* Python-side constant folds the kernels use (Taichi evaluates pure
+       Python sub-expressions in double and captures the result as f32) */
+    float omega0;                   /* 1.0/tau0, CODEX.py:1047 */
+    float half_inv_dx;              /* 0.5/dx, CODEX.py:2459 */
+    float solitary_dir_cel;         /* direction*celerity, CODEX.py:1169 */
+    float nu_lbm_init;              /* (tau0-0.5)/3, CODEX.py:2722 */
+    float u_tau_init;               /* 0.1*u_top_lb, CODEX.py:2721 */
+    float inv_kappa;                /* 1.0/kappa, CODEX.py:2731 */
+    float one_third;                /* 1.0/3.0 as f32 */
+    int32_t magic_end;              /* must equal LBM_PARAMS_MAGIC */
+} lbm_params;
+
+#define LBM_PARAMS_MAGIC 0x1B200D19
+
+/*
+ * Caller-owned buffers.  Pointers not needed by the configured mode may be
+ * NULL (lbm_bind checks what the mode needs).  "n" = nz*ny*nx cells,
+ * "a" = ny*nx columns.
+ */
+typedef struct lbm_buffers {
+    void *f[2];              /* 19*n populations (float, or 16-bit shifted per pop_storage) */
+    float *rho, *ux, *uy, *uz;   /* n each: moments (reference rho/ux/uy/uz) */
+    float *omega;            /* n: persistent local relaxation rate (omegaLoc) */
+    /* 2-D columns */
+    float *water_h, *water_h_last;       /* a: bed height (reference name) */
+    float *u_wave, *v_wave, *w_wave;     /* a: bed velocity, lattice units */
+    float *fs_h, *fs_h_last;             /* a: free_surface_h / _last */
+    float *fs_flux_x, *fs_flux_y;        /* a: column fluxes */
+    float *piecewise_bed_z;              /* nx */
+    float *u_inlet_profile;              /* nz */
+    /* initialisation inputs */
+    float *rho_initial;                  /* n */
+    float *init_noise;                   /* 3*n uniform in [-1,1): kick / noise x,y,z */
+    /* free surface 3-D state */
+    float *fs_fill;                      /* n */
+    int8_t *fs_type, *fs_type_prev;      /* n */
+    float *fs_mass, *fs_mass_excess;     /* n */
+    int8_t *fs_excess_dir;               /* n */
+    /* diagnostics written only by lbm_export_diagnostics (may be NULL) */
+    float *phi;                          /* n */
+    int32_t *obstacle, *near_obstacle;   /* n */
+    int8_t *lattice_open;                /* 19*n, [q][cell] */
+    float *lattice_open_frac;            /* 19*n */
+    int8_t *lattice_wall_type;           /* 19*n */
+    float *pressure_reference_head, *gravity_body_fraction;  /* n */
+    int32_t *vof_exterior_gas;           /* n: flood-fill labels of the last collapse pass */
+} lbm_buffers;
+
+/* Scalar diagnostics (reference CODEX.py:600-620). */
+typedef struct lbm_counters {
+    int32_t boundary_refill_count;
+    int32_t free_surface_refill_count;
+    int32_t free_surface_coalescence_repair_count;
+    int32_t free_surface_thin_gap_bridge_count;
+    int32_t free_surface_cut_link_count;
+    int32_t free_surface_vof_excess_count;
+    int32_t free_surface_vof_orphan_count;
+    int32_t free_surface_vof_collapse_cell_count;
+    int32_t free_surface_vof_detached_advect_count;
+    int32_t free_surface_vof_detached_compress_count;
+    int32_t boundary_cut_link_count;
+    int32_t status_flags;                /* bit 0: non-finite density seen */
+    float free_surface_vof_collapse_candidate_volume_m3;
+    float free_surface_vof_collapse_applied_volume_m3;
+    float free_surface_vof_collapse_removal_scale;
+    float free_surface_vof_collapse_candidate_mass;
+    float free_surface_vof_collapse_exterior_capacity;
+    float free_surface_vof_detached_advect_mass;
+    float free_surface_vof_detached_compress_mass;
+    float pad;
+    int64_t step;                        /* steps completed since init */
+    int32_t current_f;                   /* index (0/1) of the buffer holding f */
+    int32_t flood_sweeps_used;           /* last collapse pass: sweeps until the marks stopped changing */
+} lbm_counters;
+
+typedef struct lbm_ctx lbm_ctx;
+
+/* Library identity: "cuda-sm100a" or "cpu-oracle". */
+const char *lbm_backend_name(void);
+int lbm_abi_version(void);
+/* sizeof(lbm_params), sizeof(lbm_buffers), sizeof(lbm_counters) for
+   which = 0, 1, 2: lets a binding check its struct layout. */
+int64_t lbm_struct_size(int32_t which);
+
+/* Create a context from constants; replaces module import + field
+   allocation (CODEX.py:35-620). */
+int lbm_create(const lbm_params *params, lbm_ctx **out);
+
+/* Bind caller-owned buffers (replaces the ti.field set, CODEX.py:531-620). */
+int lbm_bind(lbm_ctx *ctx, const lbm_buffers *bufs);
+
+/* Initialisation, phase 1: constants, bed at t=0, geometry, initial free
+   surface height, classification, VOF block shape
+   (CODEX.py:3776-3785 up to update_pressure_reference_fields).  After it
+   the caller computes rho_initial on the host (prepare_initial_density_field,
+   CODEX.py:743-818) from water_h and fs_h. */
+int lbm_init_geometry(lbm_ctx *ctx, void *stream);
+
+/* Initialisation, phase 2: init_fields, free-surface boundary populations,
+   VOF mass from fill, interface layer, column height
+   (CODEX.py:3787-3792).  Reads rho_initial and init_noise. */
+int lbm_init_fields(lbm_ctx *ctx, void *stream);
+
+/* Advance nsteps timesteps (the loop body CODEX.py:3873-3925). */
+int lbm_step(lbm_ctx *ctx, int32_t nsteps, void *stream);
+
+/* Write the derived per-cell fields the reference keeps resident (phi,
+   obstacle, lattice_open*, near_obstacle, pressure reference) for the
+   current step's geometry into the bound diagnostic buffers. */
+int lbm_export_diagnostics(lbm_ctx *ctx, void *stream);
+
+/* Copy scalar counters to the host (synchronises the stream). */
+int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out);
+
+int lbm_destroy(lbm_ctx *ctx);
+const char *lbm_last_error(lbm_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H */

@@ -1,0 +1,210 @@
+"""Generate golden vectors by running the reference solver's own kernels.
+
+Run in the development container (the reference is mounted read-only at
+/root/reference; it does not exist on GPU machines):
+
+    python tests/golden/gen_golden.py [--only NAME]
+
+Each case sets LBM_* options, imports LBM_3D_LES_air_over_waves_CODEX.py
+with taichi_shim standing in for Taichi, runs main() for a few steps on a
+tiny grid and saves tests/golden/<case>.npz with:
+  env            the options (JSON)
+  noise          the initial kick fed to ti.random() in init_fields
+  rho_initial    the reference's prepare_initial_density_field output
+  s<k>_<field>   snapshots after init (k = 0) and after step k
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import sys
+import tempfile
+import warnings
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REFERENCE = "/root/reference"
+SOLVER = os.path.join(REFERENCE, "LBM_3D_LES_air_over_waves_CODEX.py")
+
+sys.path.insert(0, HERE)
+import taichi_shim  # noqa: E402
+
+MASK64 = (1 << 64) - 1
+
+
+def splitmix64(x: int) -> int:
+    x = (x + 0x9E3779B97F4A7C15) & MASK64
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & MASK64
+    return x ^ (x >> 31)
+
+
+def uniform01(seed: int, step: int, cell: int) -> float:
+    h = splitmix64(seed ^ splitmix64(step ^ splitmix64((cell + 0x632BE59BD9B4E019) & MASK64)))
+    return float(np.float32(np.float32(h >> 40) * np.float32(1.0 / 16777216.0)))
+
+
+BASE_AIR = {"LBM_PHYSICS_MODE": "air", "LBM_DX_M": "1"}
+
+CASES = {
+    # reference air defaults (KBC + LES + backscatter + fringe + top drive + sponge)
+    "air_kbc_default": dict(BASE_AIR, LBM_LX_M="12", LBM_LY_M="4", LBM_LZ_M="10",
+                            LBM_BED_AMP_M="1.0", LBM_BED_WAVELENGTH_M="8", LBM_WATER_DEPTH_M="6"),
+    # benchmark air configuration: regularized + LES, single-sine bed, free-slip top
+    "air_regularized_sine": dict(BASE_AIR, LBM_LX_M="12", LBM_LY_M="4", LBM_LZ_M="10",
+                                 LBM_COLLISION="regularized", LBM_BACKSCATTER="0", LBM_ENABLE_X_FRINGE="0",
+                                 LBM_ENABLE_TOP_DRIVE="0", LBM_ENABLE_TOP_SPONGE="0",
+                                 LBM_BED_LEVEL_M="3", LBM_BED_AMP_M="1.5", LBM_BED_WAVELENGTH_M="12",
+                                 LBM_U_TOP_MPS="0.6"),
+    # cube obstacle over the moving bed, solid x walls, cell wall sampling
+    "air_bed_cube_solidx": dict(BASE_AIR, LBM_LX_M="12", LBM_LY_M="6", LBM_LZ_M="10",
+                                LBM_OBSTACLE_MODE="bed_cube", LBM_CUBE_SIDE_M="3", LBM_CUBE_CENTER_Z_M="6",
+                                LBM_CUBE_YAW_DEG="20", LBM_X_BOUNDARY="solid", LBM_WALL_VELOCITY_SAMPLING="cell",
+                                LBM_BED_AMP_M="1.0", LBM_BED_WAVELENGTH_M="8", LBM_WATER_DEPTH_M="6",
+                                LBM_BACKSCATTER="0"),
+    # phi-based geometry
+    "air_phi_geometry": dict(BASE_AIR, LBM_LX_M="10", LBM_LY_M="4", LBM_LZ_M="8",
+                             LBM_BOUNDARY_GEOMETRY="phi", LBM_BED_AMP_M="1.0", LBM_BED_WAVELENGTH_M="10",
+                             LBM_WATER_DEPTH_M="6", LBM_COLLISION="regularized"),
+    # water, height-function kinematic path, Gaussian, hydrostatic balanced
+    "water_height_gaussian": {"LBM_PHYSICS_MODE": "water", "LBM_FREE_SURFACE_INITIAL": "gaussian",
+                              "LBM_DX_M": "1", "LBM_LX_M": "16", "LBM_LY_M": "3", "LBM_LZ_M": "10",
+                              "LBM_WATER_DEPTH_M": "5", "LBM_GAUSSIAN_AMPLITUDE_M": "1.5",
+                              "LBM_GAUSSIAN_SIGMA_M": "3", "LBM_WATER_NU_M2S": "0.05"},
+    # water, solitary wave, periodic, total pressure, noneq refill, LES on
+    "water_height_solitary": {"LBM_PHYSICS_MODE": "water", "LBM_DX_M": "1", "LBM_LX_M": "16",
+                              "LBM_LY_M": "3", "LBM_LZ_M": "10", "LBM_WATER_DEPTH_M": "5",
+                              "LBM_SOLITARY_AMPLITUDE_M": "1.5", "LBM_PRESSURE_FORMULATION": "total_pressure",
+                              "LBM_FREE_SURFACE_REFILL": "noneq", "LBM_USE_LES": "1",
+                              "LBM_WATER_NU_M2S": "0.05", "LBM_INIT_FREE_SURFACE_POPULATIONS": "1"},
+    # VOF falling block with KBC, collapse each 2 steps, bridge
+    "vof_block_kbc": {"LBM_PHYSICS_MODE": "water", "LBM_FREE_SURFACE_TRACKING": "vof",
+                      "LBM_FREE_SURFACE_INITIAL": "gaussian", "LBM_X_BOUNDARY": "solid", "LBM_COLLISION": "kbc",
+                      "LBM_VOF_INITIAL_SHAPE": "block", "LBM_GAUSSIAN_AMPLITUDE_M": "0",
+                      "LBM_WATER_DEPTH_M": "4", "LBM_VOF_BLOCK_SIZE_M": "3", "LBM_VOF_BLOCK_SIZE_Y_M": "2",
+                      "LBM_VOF_BLOCK_BOTTOM_M": "6", "LBM_PRESSURE_FORMULATION": "vof_component_balanced",
+                      "LBM_VOF_COLLAPSE_TRAPPED_GAS": "1", "LBM_VOF_COLLAPSE_INTERVAL": "2",
+                      "LBM_VOF_COLLAPSE_MAX_VOLUME_M3": "64", "LBM_VOF_THIN_GAP_BRIDGE": "1",
+                      "LBM_VOF_THIN_GAP_BRIDGE_STRENGTH": "4", "LBM_DX_M": "1", "LBM_LX_M": "10",
+                      "LBM_LY_M": "3", "LBM_LZ_M": "12", "LBM_WATER_NU_M2S": "0.05",
+                      "LBM_VOF_EMPTY_FILL_THRESHOLD": "0.02"},
+    # VOF with hydrostatic refill / directional refill and a Gaussian surface
+    "vof_gaussian_directional": {"LBM_PHYSICS_MODE": "water", "LBM_FREE_SURFACE_TRACKING": "vof",
+                                 "LBM_FREE_SURFACE_INITIAL": "gaussian", "LBM_FREE_SURFACE_REFILL": "directional",
+                                 "LBM_DX_M": "1", "LBM_LX_M": "12", "LBM_LY_M": "3", "LBM_LZ_M": "10",
+                                 "LBM_WATER_DEPTH_M": "5", "LBM_GAUSSIAN_AMPLITUDE_M": "2",
+                                 "LBM_GAUSSIAN_SIGMA_M": "2", "LBM_WATER_NU_M2S": "0.05"},
+}
+
+STEPS = {"air_kbc_default": 3, "air_regularized_sine": 3, "air_bed_cube_solidx": 2, "air_phi_geometry": 2,
+         "water_height_gaussian": 3, "water_height_solitary": 3, "vof_block_kbc": 4, "vof_gaussian_directional": 3}
+
+SCALAR_FIELDS = ["rho", "ux", "uy", "uz", "omegaLoc", "phi", "obstacle", "near_obstacle", "free_surface_fill",
+                 "free_surface_type", "free_surface_type_prev", "free_surface_mass", "free_surface_mass_excess",
+                 "free_surface_mass_excess_dir", "pressure_reference_head", "gravity_body_fraction",
+                 "vof_exterior_gas"]
+PLANE_FIELDS = ["water_h", "water_h_last", "u_wave", "v_wave", "w_wave", "free_surface_h", "free_surface_h_last",
+                "free_surface_flux_x", "free_surface_flux_y", "u_inlet_profile"]
+VECTOR_FIELDS = ["f", "lattice_open", "lattice_open_frac", "lattice_wall_type"]
+COUNTERS = ["boundary_refill_count", "free_surface_refill_count", "free_surface_coalescence_repair_count",
+            "free_surface_thin_gap_bridge_count", "free_surface_cut_link_count", "free_surface_vof_excess_count",
+            "free_surface_vof_orphan_count", "free_surface_vof_collapse_cell_count",
+            "free_surface_vof_collapse_candidate_volume_m3", "free_surface_vof_collapse_applied_volume_m3",
+            "free_surface_vof_collapse_removal_scale", "free_surface_vof_collapse_candidate_mass",
+            "free_surface_vof_collapse_exterior_capacity", "free_surface_vof_detached_advect_count",
+            "free_surface_vof_detached_advect_mass", "free_surface_vof_detached_compress_count",
+            "free_surface_vof_detached_compress_mass", "boundary_cut_link_count"]
+
+
+def snapshot(mod, tag, out):
+    for name in SCALAR_FIELDS + PLANE_FIELDS:
+        out[f"{tag}_{name}"] = getattr(mod, name).to_numpy()
+    for name in VECTOR_FIELDS:
+        arr = getattr(mod, name).to_numpy()          # (Nz, Ny, Nx, 19)
+        out[f"{tag}_{name}"] = np.ascontiguousarray(np.moveaxis(arr, -1, 0))  # (19, Nz, Ny, Nx)
+    for name in COUNTERS:
+        out[f"{tag}_{name}"] = np.array(getattr(mod, name)[None])
+
+
+def run_case(name: str, env: dict, seed: int = 12345) -> dict:
+    saved = dict(os.environ)
+    cache = tempfile.mkdtemp(prefix="ticache_")
+    try:
+        for key in list(os.environ):
+            if key.startswith("LBM_"):
+                del os.environ[key]
+        os.environ.update(env)
+        os.environ["LBM_TI_CACHE_DIR"] = cache
+        sys.modules["taichi"] = taichi_shim
+        sys.path.insert(0, REFERENCE)
+        spec = importlib.util.spec_from_file_location(f"ref_{name}", SOLVER)
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        shape = (mod.Nz, mod.Ny, mod.Nx)
+        rng = np.random.default_rng(seed)
+        noise = rng.uniform(-1.0, 1.0, size=(3,) + shape).astype(np.float32)
+        state = {"kick": 0}
+
+        def hook(kernel, cell):
+            if kernel == "init_fields":
+                v = float(noise[0].reshape(-1)[state["kick"]])
+                state["kick"] += 1
+                return v / 2.0 + 0.5
+            if kernel == "collide_KBC":
+                step = taichi_shim._state["calls"].get("collide_KBC", 0)
+                return uniform01(seed, step, cell)
+            raise RuntimeError(f"unexpected ti.random in {kernel}")
+
+        taichi_shim._state["random_hook"] = hook
+        taichi_shim._state["calls"] = {}
+        out = {"env": np.array(json.dumps(env)), "noise": noise, "seed": np.array(seed)}
+        captured = {"init": False}
+        orig_height = mod.update_free_surface_height_from_vof
+
+        def height_then_snapshot():
+            orig_height()
+            if not captured["init"]:
+                captured["init"] = True
+                snapshot(mod, "s0", out)
+                out["rho_initial"] = mod.rho_initial.to_numpy()
+
+        mod.update_free_surface_height_from_vof = height_then_snapshot
+
+        def visualize(step, time_phys, re_a, re_b):
+            snapshot(mod, f"s{step}", out)
+
+        mod.visualize = visualize
+        mod.steps = STEPS[name]
+        mod.plot_freq = 1
+        mod.plot_step_start = 0
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            with np.errstate(all="ignore"):
+                mod.main()
+        out["nsteps"] = np.array(STEPS[name])
+        return out
+    finally:
+        os.environ.clear()
+        os.environ.update(saved)
+        if REFERENCE in sys.path:
+            sys.path.remove(REFERENCE)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--only", default=None)
+    args = ap.parse_args()
+    for name, env in CASES.items():
+        if args.only and name != args.only:
+            continue
+        out = run_case(name, env)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(f"wrote {path} ({os.path.getsize(path) / 1024:.0f} KiB)", flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,450 @@
+// lbm_api.cu - C ABI of the B200 D3Q19 step engine (include/lbm_b200.h).
+//
+// Step orchestration.  The state of record between calls is the caller's
+// bound buffers; inside one lbm_step call of K steps:
+//
+//   air (no free surface): the loop is rotated so that every step is ONE
+//   pass over the populations -
+//     collide(n+1) from the post-stream state,
+//     fused(m -> m+1) = stream+BC of step m, then condition, macro, LES and
+//       collide of step m+1, for m = n+1 .. n+K-1,
+//     stream(n+K) back to the post-stream state the reference holds after
+//       copy_post_and_swap (CODEX.py:3924).
+//   With LES, each collide is preceded by a pre-pass that writes the
+//   velocity of every cell for the strain-rate stencil.
+//
+//   height-function free surface: per step collide, stream (+ post-stream
+//   macro), column flux, advection, refill (CODEX.py:3873-3925).
+//
+// The 2-D bed of step m lives in scratch slot m & 1, so the fused pass can
+// see the bed of both steps it spans.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "lbm_b200.h"
+#include "lbm_launch.h"
+#include "lbm_step.cuh"
+
+using namespace lbm;
+
+namespace {
+
+enum { CNT_CUT = 0, CNT_FSCUT = 1, CNT_BRIDGE = 2, CNT_FS_REFILL = 3, CNT_COALESCE = 4, CNT_VOF_EXCESS = 5,
+       CNT_ORPHAN = 6, CNT_COLLAPSE = 7, CNT_DET = 8, CNT_CMP = 9, CNT_SWEEPS = 10, CNT_N = 16 };
+
+}  // namespace
+
+struct lbm_ctx {
+    lbm_params P;
+    Dom D;
+    lbm_buffers b;
+    bool bound = false;
+    std::string err;
+    int cur = 0;
+    int64_t nstep = 0;
+    cudaStream_t last_stream = 0;
+    // scratch owned by the library
+    float *bed_h[2] = {nullptr, nullptr}, *bed_hmax[2] = {nullptr, nullptr};
+    float *bed_uw[2] = {nullptr, nullptr}, *bed_vw[2] = {nullptr, nullptr}, *bed_ww[2] = {nullptr, nullptr};
+    float *u_les = nullptr;
+    int *dcount = nullptr;
+    unsigned *dstatus = nullptr;
+    float *dfcount = nullptr;
+    std::vector<void *> owned;
+};
+
+static int fail(lbm_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+static int cuda_check(lbm_ctx *c, cudaError_t e, const char *what) {
+    if (e != cudaSuccess) return fail(c, LBM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return LBM_OK;
+}
+#define CK(expr, what)                                      \
+    do {                                                    \
+        int _s = cuda_check(ctx, (expr), what);             \
+        if (_s != LBM_OK) return _s;                        \
+    } while (0)
+#define CK_LAUNCH(what) CK(cudaGetLastError(), what)
+
+static BedView slot_view(const lbm_ctx *ctx, int s) {
+    BedView v;
+    v.h = ctx->bed_h[s];
+    v.hmax = ctx->bed_hmax[s];
+    v.uw = ctx->bed_uw[s];
+    v.vw = ctx->bed_vw[s];
+    v.ww = ctx->bed_ww[s];
+    return v;
+}
+
+static float step_time(const lbm_ctx *ctx, int64_t step) {
+    return (float)((double)(step + 1) * ctx->P.dt_phys);  // CODEX.py:3874
+}
+
+static InitArgs init_args(lbm_ctx *ctx, int slot) {
+    InitArgs I;
+    memset(&I, 0, sizeof I);
+    const lbm_buffers &b = ctx->b;
+    I.P = ctx->P;
+    I.D = ctx->D;
+    I.bed = slot_view(ctx, slot);
+    I.f_cur = b.f[ctx->cur];
+    I.f_other = b.f[1 - ctx->cur];
+    I.rho = b.rho; I.ux = b.ux; I.uy = b.uy; I.uz = b.uz; I.omega = b.omega;
+    I.water_h = b.water_h; I.water_h_last = b.water_h_last;
+    I.u_wave = b.u_wave; I.v_wave = b.v_wave; I.w_wave = b.w_wave;
+    I.fs_h = b.fs_h; I.fs_h_last = b.fs_h_last; I.fs_flux_x = b.fs_flux_x; I.fs_flux_y = b.fs_flux_y;
+    I.piecewise = b.piecewise_bed_z;
+    I.u_inlet_profile = b.u_inlet_profile;
+    I.rho_initial = b.rho_initial;
+    I.noise = b.init_noise;
+    I.fs_fill = b.fs_fill; I.fs_mass = b.fs_mass; I.fs_mass_excess = b.fs_mass_excess;
+    I.fs_type = b.fs_type; I.fs_type_prev = b.fs_type_prev; I.fs_excess_dir = b.fs_excess_dir;
+    return I;
+}
+
+static StepArgs step_args(lbm_ctx *ctx) {
+    StepArgs A;
+    memset(&A, 0, sizeof A);
+    const lbm_buffers &b = ctx->b;
+    A.P = ctx->P;
+    A.D = ctx->D;
+    A.rho = b.rho; A.ux = b.ux; A.uy = b.uy; A.uz = b.uz; A.omega = b.omega;
+    A.u_les = ctx->u_les;
+    A.u_out = ctx->u_les;
+    A.fs_h = b.fs_h; A.fs_h_last = b.fs_h_last;
+    A.fs_fill = b.fs_fill; A.fs_type = b.fs_type;
+    A.u_inlet_profile = b.u_inlet_profile;
+    A.counters = ctx->dcount;
+    A.status = ctx->dstatus;
+    return A;
+}
+
+// copy the bound bed state into slot s (start of a call)
+static int load_bed_slot(lbm_ctx *ctx, int s, cudaStream_t st) {
+    size_t bytes = ctx->D.a * sizeof(float);
+    CK(cudaMemcpyAsync(ctx->bed_h[s], ctx->b.water_h, bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
+    CK(cudaMemcpyAsync(ctx->bed_uw[s], ctx->b.u_wave, bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
+    CK(cudaMemcpyAsync(ctx->bed_vw[s], ctx->b.v_wave, bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
+    CK(cudaMemcpyAsync(ctx->bed_ww[s], ctx->b.w_wave, bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
+    launch_hmax(ctx->D, ctx->bed_h[s], ctx->bed_hmax[s], st);
+    CK_LAUNCH("hmax");
+    return LBM_OK;
+}
+// copy slot s (and the previous height) back to the bound buffers
+static int store_bed_slot(lbm_ctx *ctx, int s, const float *h_prev, cudaStream_t st) {
+    size_t bytes = ctx->D.a * sizeof(float);
+    CK(cudaMemcpyAsync(ctx->b.water_h_last, h_prev, bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
+    CK(cudaMemcpyAsync(ctx->b.water_h, ctx->bed_h[s], bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
+    CK(cudaMemcpyAsync(ctx->b.u_wave, ctx->bed_uw[s], bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
+    CK(cudaMemcpyAsync(ctx->b.v_wave, ctx->bed_vw[s], bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
+    CK(cudaMemcpyAsync(ctx->b.w_wave, ctx->bed_ww[s], bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
+    return LBM_OK;
+}
+
+static int bed_step(lbm_ctx *ctx, int64_t m, cudaStream_t st) {
+    int s = (int)(m & 1), sp = (int)((m - 1) & 1);
+    launch_bed(ctx->P, ctx->D, ctx->bed_h[sp], ctx->bed_h[s], ctx->bed_hmax[s], ctx->bed_uw[s], ctx->bed_vw[s],
+               ctx->bed_ww[s], ctx->b.piecewise_bed_z, step_time(ctx, m), st);
+    CK_LAUNCH("bed");
+    return LBM_OK;
+}
+
+static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
+    const int64_t n = ctx->nstep;
+    const bool les = ctx->P.use_les != 0;
+    StepArgs A = step_args(ctx);
+    int s;
+    if ((s = bed_step(ctx, n + 1, st)) != LBM_OK) return s;
+    int src = ctx->cur;
+    A.fsrc = ctx->b.f[src];
+    A.fdst = ctx->b.f[1 - src];
+    A.bed_c = slot_view(ctx, (int)((n + 1) & 1));
+    A.bed_s = A.bed_c;
+    A.step = (uint64_t)(n + 1);
+    A.flags = (K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0;
+    if (les) {
+        launch_step_kernel(KER_PREPASS_CANON, A, st);
+        CK_LAUNCH("prepass");
+    }
+    launch_step_kernel(KER_COLLIDE_CANON, A, st);
+    CK_LAUNCH("collide");
+    src = 1 - src;
+    for (int64_t m = n + 1; m < n + K; ++m) {
+        if ((s = bed_step(ctx, m + 1, st)) != LBM_OK) return s;
+        A.fsrc = ctx->b.f[src];
+        A.fdst = ctx->b.f[1 - src];
+        A.bed_s = slot_view(ctx, (int)(m & 1));
+        A.bed_c = slot_view(ctx, (int)((m + 1) & 1));
+        A.step = (uint64_t)(m + 1);
+        A.flags = (m + 1 == n + K) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0;
+        if (les) {
+            launch_step_kernel(KER_PREPASS_FUSED, A, st);
+            CK_LAUNCH("prepass fused");
+        }
+        launch_step_kernel(KER_COLLIDE_FUSED, A, st);
+        CK_LAUNCH("fused");
+        src = 1 - src;
+    }
+    CK(cudaMemsetAsync(ctx->dcount, 0, 3 * sizeof(int), st), "counter reset");
+    A.fsrc = ctx->b.f[src];
+    A.fdst = ctx->b.f[1 - src];
+    A.bed_s = slot_view(ctx, (int)((n + K) & 1));
+    A.bed_c = A.bed_s;
+    A.flags = F_COUNT;
+    launch_step_kernel(KER_STREAM, A, st);
+    CK_LAUNCH("stream");
+    ctx->cur = 1 - src;
+    ctx->nstep = n + K;
+    return LBM_OK;
+}
+
+static int step_height(lbm_ctx *ctx, int K, cudaStream_t st) {
+    const bool les = ctx->P.use_les != 0;
+    int s;
+    for (int it = 0; it < K; ++it) {
+        int64_t m = ctx->nstep + 1;
+        if ((s = bed_step(ctx, m, st)) != LBM_OK) return s;
+        StepArgs A = step_args(ctx);
+        A.bed_s = slot_view(ctx, (int)(m & 1));
+        A.bed_c = A.bed_s;
+        A.step = (uint64_t)m;
+        A.fsrc = ctx->b.f[ctx->cur];
+        A.fdst = ctx->b.f[1 - ctx->cur];
+        A.flags = F_WRITE_MACRO | F_WRITE_ALL_OMEGA;
+        if (les) {
+            launch_step_kernel(KER_PREPASS_CANON, A, st);
+            CK_LAUNCH("prepass");
+        }
+        launch_step_kernel(KER_COLLIDE_CANON, A, st);
+        CK_LAUNCH("collide");
+        CK(cudaMemsetAsync(ctx->dcount, 0, 4 * sizeof(int), st), "counter reset");
+        A.fsrc = ctx->b.f[1 - ctx->cur];
+        A.fdst = ctx->b.f[ctx->cur];
+        A.flags = F_COUNT;
+        launch_step_kernel(KER_STREAM, A, st);
+        CK_LAUNCH("stream");
+        launch_column_flux(A, ctx->b.fs_flux_x, ctx->b.fs_flux_y, st);
+        CK_LAUNCH("column flux");
+        launch_advect(ctx->P, ctx->D, ctx->bed_h[m & 1], ctx->b.fs_flux_x, ctx->b.fs_flux_y, ctx->b.fs_h, ctx->b.fs_h,
+                      ctx->b.fs_h_last, step_time(ctx, m), st);
+        CK_LAUNCH("advect");
+        A.flags = 0;
+        A.fdst = ctx->b.f[ctx->cur];
+        launch_refill(A, nullptr, ctx->dcount + CNT_FS_REFILL, st);
+        CK_LAUNCH("refill");
+        ctx->nstep = m;
+    }
+    StepArgs A = step_args(ctx);
+    A.bed_s = slot_view(ctx, (int)(ctx->nstep & 1));
+    launch_height_types(A, ctx->b.fs_fill, ctx->b.fs_type, ctx->b.fs_type_prev, st);
+    CK_LAUNCH("height types");
+    return LBM_OK;
+}
+
+extern "C" {
+
+const char *lbm_backend_name(void) { return "cuda-sm100a"; }
+int lbm_abi_version(void) { return LBM_ABI_VERSION; }
+int64_t lbm_struct_size(int32_t which) {
+    switch (which) {
+        case 0: return (int64_t)sizeof(lbm_params);
+        case 1: return (int64_t)sizeof(lbm_buffers);
+        case 2: return (int64_t)sizeof(lbm_counters);
+        default: return -1;
+    }
+}
+
+int lbm_create(const lbm_params *params, lbm_ctx **out) {
+    if (!params || !out) return LBM_ERR_BAD_ARG;
+    if (params->abi_version != LBM_ABI_VERSION || params->magic_end != LBM_PARAMS_MAGIC) return LBM_ERR_BAD_ARG;
+    if (params->nx < 1 || params->ny < 1 || params->nz < 2) return LBM_ERR_BAD_ARG;
+    if (params->pop_storage < 0 || params->pop_storage > 2) return LBM_ERR_BAD_ARG;
+    if (params->x_solid && params->nx < 2) return LBM_ERR_BAD_ARG;
+    lbm_ctx *ctx = new lbm_ctx();
+    ctx->P = *params;
+    ctx->D.nx = params->nx;
+    ctx->D.ny = params->ny;
+    ctx->D.nz = params->nz;
+    ctx->D.a = (size_t)params->nx * params->ny;
+    ctx->D.n = ctx->D.a * params->nz;
+    *out = ctx;
+    return LBM_OK;
+}
+
+static int alloc(lbm_ctx *ctx, void **p, size_t bytes) {
+    CK(cudaMalloc(p, bytes), "scratch allocation");
+    ctx->owned.push_back(*p);
+    return LBM_OK;
+}
+
+int lbm_bind(lbm_ctx *ctx, const lbm_buffers *bufs) {
+    if (!ctx || !bufs) return LBM_ERR_BAD_ARG;
+    const lbm_buffers &b = *bufs;
+    if (!b.f[0] || !b.f[1] || !b.rho || !b.ux || !b.uy || !b.uz || !b.omega || !b.water_h || !b.water_h_last ||
+        !b.u_wave || !b.v_wave || !b.w_wave || !b.fs_h || !b.fs_h_last || !b.fs_flux_x || !b.fs_flux_y ||
+        !b.piecewise_bed_z || !b.u_inlet_profile || !b.rho_initial || !b.init_noise || !b.fs_fill ||
+        !b.fs_type || !b.fs_type_prev || !b.fs_mass || !b.fs_mass_excess || !b.fs_excess_dir)
+        return fail(ctx, LBM_ERR_BAD_ARG, "lbm_bind: a required state buffer is NULL");
+    if (ctx->P.fs_mode != LBM_FS_NONE && ctx->P.fs_tracking == LBM_TRACK_VOF)
+        return fail(ctx, LBM_ERR_UNSUPPORTED, "VOF free-surface tracking is not available in this library build");
+    ctx->b = b;
+    if (!ctx->bound) {
+        int s;
+        size_t A = ctx->D.a * sizeof(float);
+        for (int i = 0; i < 2; ++i) {
+            if ((s = alloc(ctx, (void **)&ctx->bed_h[i], A)) || (s = alloc(ctx, (void **)&ctx->bed_hmax[i], A)) ||
+                (s = alloc(ctx, (void **)&ctx->bed_uw[i], A)) || (s = alloc(ctx, (void **)&ctx->bed_vw[i], A)) ||
+                (s = alloc(ctx, (void **)&ctx->bed_ww[i], A)))
+                return s;
+        }
+        if (ctx->P.use_les && (s = alloc(ctx, (void **)&ctx->u_les, 3 * ctx->D.n * sizeof(float)))) return s;
+        if ((s = alloc(ctx, (void **)&ctx->dcount, CNT_N * sizeof(int))) ||
+            (s = alloc(ctx, (void **)&ctx->dstatus, sizeof(unsigned))) ||
+            (s = alloc(ctx, (void **)&ctx->dfcount, 8 * sizeof(float))))
+            return s;
+        CK(cudaMemset(ctx->dcount, 0, CNT_N * sizeof(int)), "memset");
+        CK(cudaMemset(ctx->dstatus, 0, sizeof(unsigned)), "memset");
+        CK(cudaMemset(ctx->dfcount, 0, 8 * sizeof(float)), "memset");
+    }
+    ctx->bound = true;
+    return LBM_OK;
+}
+
+int lbm_init_geometry(lbm_ctx *ctx, void *stream) {
+    if (!ctx) return LBM_ERR_BAD_ARG;
+    if (!ctx->bound) return LBM_ERR_NOT_BOUND;
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->last_stream = st;
+    ctx->cur = 0;
+    ctx->nstep = 0;
+    InitArgs I = init_args(ctx, 0);
+    launch_init_constants(I, st);
+    CK_LAUNCH("init constants");
+    size_t pop_bytes = ctx->D.n * 19 * (ctx->P.pop_storage == LBM_STORE_F32 ? 4 : 2);
+    CK(cudaMemsetAsync(ctx->b.f[0], 0, pop_bytes, st), "memset f");
+    CK(cudaMemsetAsync(ctx->b.f[1], 0, pop_bytes, st), "memset f");
+    CK(cudaMemsetAsync(ctx->dcount, 0, CNT_N * sizeof(int), st), "memset counters");
+    CK(cudaMemsetAsync(ctx->dstatus, 0, sizeof(unsigned), st), "memset status");
+    // update_wave_bed_and_velocities(0.0): previous height = initial level
+    launch_bed(ctx->P, ctx->D, ctx->b.water_h, ctx->bed_h[0], ctx->bed_hmax[0], ctx->bed_uw[0], ctx->bed_vw[0],
+               ctx->bed_ww[0], ctx->b.piecewise_bed_z, 0.0f, st);
+    CK_LAUNCH("bed");
+    int s;
+    if ((s = store_bed_slot(ctx, 0, ctx->b.water_h, st)) != LBM_OK) return s;
+    I = init_args(ctx, 0);
+    launch_fs_height_init(I, st);
+    CK_LAUNCH("free-surface height");
+    launch_classify_store(I, st);
+    CK_LAUNCH("classify");
+    if (ctx->P.fs_mode != LBM_FS_NONE && ctx->P.fs_tracking == LBM_TRACK_VOF && ctx->P.vof_initial_block) {
+        launch_vof_block(I, st);
+        CK_LAUNCH("vof block");
+    }
+    return LBM_OK;
+}
+
+int lbm_init_fields(lbm_ctx *ctx, void *stream) {
+    if (!ctx) return LBM_ERR_BAD_ARG;
+    if (!ctx->bound) return LBM_ERR_NOT_BOUND;
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->last_stream = st;
+    int s;
+    if ((s = load_bed_slot(ctx, (int)(ctx->nstep & 1), st)) != LBM_OK) return s;
+    InitArgs I = init_args(ctx, (int)(ctx->nstep & 1));
+    launch_init_fields(I, st);
+    CK_LAUNCH("init fields");
+    ctx->cur = 1 - ctx->cur;  // copy_post_and_swap, CODEX.py:3789
+    return LBM_OK;
+}
+
+int lbm_step(lbm_ctx *ctx, int32_t nsteps, void *stream) {
+    if (!ctx || nsteps < 0) return LBM_ERR_BAD_ARG;
+    if (!ctx->bound) return LBM_ERR_NOT_BOUND;
+    if (nsteps == 0) return LBM_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->last_stream = st;
+    int s;
+    int64_t n0 = ctx->nstep;
+    if ((s = load_bed_slot(ctx, (int)(n0 & 1), st)) != LBM_OK) return s;
+    if (ctx->P.fs_mode == LBM_FS_NONE) s = step_air(ctx, nsteps, st);
+    else s = step_height(ctx, nsteps, st);
+    if (s != LBM_OK) return s;
+    int64_t n1 = ctx->nstep;
+    return store_bed_slot(ctx, (int)(n1 & 1), ctx->bed_h[(n1 - 1) & 1], st);
+}
+
+int lbm_export_diagnostics(lbm_ctx *ctx, void *stream) {
+    if (!ctx) return LBM_ERR_BAD_ARG;
+    if (!ctx->bound) return LBM_ERR_NOT_BOUND;
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->last_stream = st;
+    int s;
+    if ((s = load_bed_slot(ctx, (int)(ctx->nstep & 1), st)) != LBM_OK) return s;
+    InitArgs I = init_args(ctx, (int)(ctx->nstep & 1));
+    ExportArgs E;
+    E.phi = ctx->b.phi;
+    E.obstacle = ctx->b.obstacle;
+    E.near_obstacle = ctx->b.near_obstacle;
+    E.lattice_open = ctx->b.lattice_open;
+    E.lattice_open_frac = ctx->b.lattice_open_frac;
+    E.lattice_wall_type = ctx->b.lattice_wall_type;
+    E.prh = ctx->b.pressure_reference_head;
+    E.gbf = ctx->b.gravity_body_fraction;
+    launch_export(I, E, st);
+    CK_LAUNCH("export");
+    if (ctx->b.vof_exterior_gas)
+        CK(cudaMemsetAsync(ctx->b.vof_exterior_gas, 0, ctx->D.n * sizeof(int32_t), st), "memset exterior");
+    return LBM_OK;
+}
+
+int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out) {
+    if (!ctx || !out) return LBM_ERR_BAD_ARG;
+    if (!ctx->bound) return LBM_ERR_NOT_BOUND;
+    int h[CNT_N];
+    unsigned status = 0;
+    float fc[8];
+    CK(cudaStreamSynchronize(ctx->last_stream), "synchronize");
+    CK(cudaMemcpy(h, ctx->dcount, sizeof h, cudaMemcpyDeviceToHost), "counter copy");
+    CK(cudaMemcpy(&status, ctx->dstatus, sizeof status, cudaMemcpyDeviceToHost), "status copy");
+    CK(cudaMemcpy(fc, ctx->dfcount, sizeof fc, cudaMemcpyDeviceToHost), "counter copy");
+    memset(out, 0, sizeof *out);
+    out->boundary_cut_link_count = h[CNT_CUT];
+    out->free_surface_cut_link_count = h[CNT_FSCUT];
+    out->free_surface_thin_gap_bridge_count = h[CNT_BRIDGE];
+    out->free_surface_refill_count = h[CNT_FS_REFILL];
+    out->free_surface_coalescence_repair_count = h[CNT_COALESCE];
+    out->free_surface_vof_excess_count = h[CNT_VOF_EXCESS];
+    out->free_surface_vof_orphan_count = h[CNT_ORPHAN];
+    out->free_surface_vof_collapse_cell_count = h[CNT_COLLAPSE];
+    out->free_surface_vof_detached_advect_count = h[CNT_DET];
+    out->free_surface_vof_detached_compress_count = h[CNT_CMP];
+    out->flood_sweeps_used = h[CNT_SWEEPS];
+    out->free_surface_vof_collapse_candidate_volume_m3 = fc[0];
+    out->free_surface_vof_collapse_applied_volume_m3 = fc[1];
+    out->free_surface_vof_collapse_removal_scale = fc[2];
+    out->free_surface_vof_collapse_candidate_mass = fc[3];
+    out->free_surface_vof_collapse_exterior_capacity = fc[4];
+    out->free_surface_vof_detached_advect_mass = fc[5];
+    out->free_surface_vof_detached_compress_mass = fc[6];
+    out->status_flags = (int32_t)status;
+    out->step = ctx->nstep;
+    out->current_f = ctx->cur;
+    return LBM_OK;
+}
+
+int lbm_destroy(lbm_ctx *ctx) {
+    if (!ctx) return LBM_ERR_BAD_ARG;
+    for (void *p : ctx->owned) cudaFree(p);
+    delete ctx;
+    return LBM_OK;
+}
+
+const char *lbm_last_error(lbm_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+}  // extern "C"

@@ -1,0 +1,269 @@
+// lbm_geom.cuh - per-link solid geometry recomputed in registers.
+//
+// The reference stores four per-link fields every step
+// (build_lattice_open_from_free_surface_periodic, CODEX.py:2492-2686:
+// lattice_open, lattice_open_frac, lattice_wall_type, near_obstacle, 232 B
+// per cell).  Here they are recomputed where they are needed from the 2-D
+// bed height, the cube and the x walls; nothing is stored.  A cell whose
+// every link endpoint is more than half a cell above the bed and outside
+// the cube takes a fast path (all links open, fraction 1): the test is
+// conservative, so the fast and full paths give identical results.
+#pragma once
+
+#include "lbm_dev.cuh"
+
+namespace lbm {
+
+struct Geo {
+    uint32_t lo;     // bit q set: lattice_open[q] == 1 (bit 0: the cell is open)
+    uint32_t part;   // bit q set: lattice_open_frac[q] < 1
+    bool near;       // near_obstacle
+    bool fast;       // all links open with fraction 1 (links below not written)
+};
+// per-link fractions and wall sources; written only for cells off the fast
+// path (the fast path reads neither)
+struct GeoLinks {
+    float lf[19];
+    uint8_t wt[19];
+};
+
+// periodic bilinear sampling setup (CODEX.py:665-683, 2570-2588, 941-957)
+LBM_DEV void bl_setup(const lbm_params &P, const Dom &D, float xp, float yp, int &i0, int &j0, int &i1, int &j1,
+                      float &fx, float &fy) {
+    const float dx = P.dx;
+    float Lx = (float)D.nx * dx, Ly = (float)D.ny * dx, Nxf = (float)D.nx, Nyf = (float)D.ny;
+    float xw = xp - floorf(xp / Lx) * Lx;
+    float yw = yp - floorf(yp / Ly) * Ly;
+    float u = xw / dx - 0.5f;
+    float v = yw / dx - 0.5f;
+    u = u - floorf(u / Nxf) * Nxf;
+    v = v - floorf(v / Nyf) * Nyf;
+    i0 = (int)floorf(u);
+    j0 = (int)floorf(v);
+    fx = u - (float)i0;
+    fy = v - (float)j0;
+    if (i0 >= D.nx) i0 -= D.nx;
+    if (j0 >= D.ny) j0 -= D.ny;
+    if (i0 < 0) i0 += D.nx;
+    if (j0 < 0) j0 += D.ny;
+    i1 = (i0 + 1) % D.nx;
+    j1 = (j0 + 1) % D.ny;
+}
+LBM_DEV float bl_sample(const float *a, const Dom &D, int i0, int j0, int i1, int j1, float fx, float fy) {
+    float v00 = __ldg(a + D.col(j0, i0)), v10 = __ldg(a + D.col(j0, i1));
+    float v01 = __ldg(a + D.col(j1, i0)), v11 = __ldg(a + D.col(j1, i1));
+    float x0 = v00 * (1.0f - fx) + v10 * fx;
+    float x1 = v01 * (1.0f - fx) + v11 * fx;
+    return x0 * (1.0f - fy) + x1 * fy;
+}
+LBM_DEV float sample_h(const lbm_params &P, const Dom &D, const float *h, float xp, float yp) {
+    int i0, j0, i1, j1;
+    float fx, fy;
+    bl_setup(P, D, xp, yp, i0, j0, i1, j1, fx, fy);
+    return bl_sample(h, D, i0, j0, i1, j1, fx, fy);
+}
+// sample_wall_velocity_lb, CODEX.py:937-988
+LBM_DEV void sample_wall(const lbm_params &P, const Dom &D, const BedView &B, float xp, float yp, float &wx,
+                         float &wy, float &wz) {
+    int i0, j0, i1, j1;
+    float fx, fy;
+    bl_setup(P, D, xp, yp, i0, j0, i1, j1, fx, fy);
+    wx = bl_sample(B.uw, D, i0, j0, i1, j1, fx, fy);
+    wy = bl_sample(B.vw, D, i0, j0, i1, j1, fx, fy);
+    wz = bl_sample(B.ww, D, i0, j0, i1, j1, fx, fy);
+}
+
+// cube_sdf_at_point, CODEX.py:897-934
+LBM_DEV float cube_sdf(const lbm_params &P, const Dom &D, float xp, float yp, float zp) {
+    float Lx = (float)D.nx * P.dx, Ly = (float)D.ny * P.dx;
+    float dxp = xp - P.cube_cx;
+    float dyp = yp - P.cube_cy;
+    if (!P.x_solid) {
+        if (dxp > 0.5f * Lx) dxp -= Lx;
+        if (dxp < -0.5f * Lx) dxp += Lx;
+    }
+    if (dyp > 0.5f * Ly) dyp -= Ly;
+    if (dyp < -0.5f * Ly) dyp += Ly;
+    float xl = P.cube_yaw_cos * dxp + P.cube_yaw_sin * dyp;
+    float yl = -P.cube_yaw_sin * dxp + P.cube_yaw_cos * dyp;
+    float z1 = zp - P.cube_cz;
+    float xpitch = P.cube_pitch_cos * xl - P.cube_pitch_sin * z1;
+    float zl = P.cube_pitch_sin * xl + P.cube_pitch_cos * z1;
+    float qx = fabsf(xpitch) - P.cube_hx;
+    float qy = fabsf(yl) - P.cube_hy;
+    float qz = fabsf(zl) - P.cube_hz;
+    float ox = fmaxf(qx, 0.0f), oy = fmaxf(qy, 0.0f), oz = fmaxf(qz, 0.0f);
+    float outside = sqrtf(ox * ox + oy * oy + oz * oz);
+    float inside = fminf(fmaxf(qx, fmaxf(qy, qz)), 0.0f);
+    return outside + inside;
+}
+
+// compute_phi_slope_corrected for one cell, CODEX.py:2432-2490
+LBM_DEV float phi_cell(const lbm_params &P, const Dom &D, const float *h, int k, int j, int i) {
+    const float dx = P.dx;
+    int ip = (i + 1) % D.nx, im = (i - 1 + D.nx) % D.nx, jp = (j + 1) % D.ny, jm = (j - 1 + D.ny) % D.ny;
+    float dhdx = (__ldg(h + D.col(j, ip)) - __ldg(h + D.col(j, im))) * P.half_inv_dx;
+    if (P.x_solid) {
+        if (i == 0) dhdx = (__ldg(h + D.col(j, i + 1)) - __ldg(h + D.col(j, i))) / dx;
+        else if (i == D.nx - 1) dhdx = (__ldg(h + D.col(j, i)) - __ldg(h + D.col(j, i - 1))) / dx;
+    }
+    float dhdy = (__ldg(h + D.col(jp, i)) - __ldg(h + D.col(jm, i))) * P.half_inv_dx;
+    float denom = sqrtf(1.0f + dhdx * dhdx + dhdy * dhdy);
+    if (denom < 1e-6f) denom = 1.0f;
+    float hl = __ldg(h + D.col(j, i));
+    float zc = ((float)k + 0.5f) * dx;
+    float xc = ((float)i + 0.5f) * dx;
+    float yc = ((float)j + 0.5f) * dx;
+    float v = 1.0e6f;
+    if (P.include_bed) v = (zc - hl) / denom;
+    if (P.include_cube) {
+        float cp = cube_sdf(P, D, xc, yc, zc);
+        if (cp < v) v = cp;
+    }
+    if (P.x_solid) {
+        float xw = fminf(xc, (float)D.nx * dx - xc);
+        if (xw < v) v = xw;
+    }
+    return v;
+}
+
+// sample_phi_periodic, CODEX.py:661-707 (phi evaluated on the fly)
+static __device__ __noinline__ float sample_phi(const lbm_params &P, const Dom &D, const float *h, float xp, float yp, float zp) {
+    int i0, j0, i1, j1;
+    float fx, fy;
+    bl_setup(P, D, xp, yp, i0, j0, i1, j1, fx, fy);
+    float r = zp / P.dx - 0.5f;
+    int k0 = (int)floorf(r);
+    float fz = r - (float)k0;
+    int k1 = k0 + 1;
+    if (k0 < 0) { k0 = 0; k1 = 0; fz = 0.0f; }
+    if (k1 >= D.nz) { k0 = D.nz - 1; k1 = D.nz - 1; fz = 0.0f; }
+    float p00_0 = phi_cell(P, D, h, k0, j0, i0) * (1.0f - fx) + phi_cell(P, D, h, k0, j0, i1) * fx;
+    float p01_0 = phi_cell(P, D, h, k0, j1, i0) * (1.0f - fx) + phi_cell(P, D, h, k0, j1, i1) * fx;
+    float pxy_0 = p00_0 * (1.0f - fy) + p01_0 * fy;
+    float p00_1 = phi_cell(P, D, h, k1, j0, i0) * (1.0f - fx) + phi_cell(P, D, h, k1, j0, i1) * fx;
+    float p01_1 = phi_cell(P, D, h, k1, j1, i0) * (1.0f - fx) + phi_cell(P, D, h, k1, j1, i1) * fx;
+    float pxy_1 = p00_1 * (1.0f - fy) + p01_1 * fy;
+    return pxy_0 * (1.0f - fz) + pxy_1 * fz;
+}
+
+// conservative "far from every wall" test
+LBM_DEV bool geo_far(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i) {
+    if (P.use_phi_open_fraction || P.use_phi_open_flags) return false;
+    if (P.x_solid && (i == 0 || i == D.nx - 1)) return false;
+    const float dx = P.dx, hdx = 0.5f * dx;
+    float zc = ((float)k + 0.5f) * dx;
+    if (P.include_bed) {
+        float hm = __ldg(B.hmax + D.col(j, i));
+        float margin = 1e-4f * dx + 1e-6f * (fabsf(zc) + fabsf(hm));
+        if (!((zc - hdx) - hm >= hdx + margin)) return false;
+    }
+    if (P.include_cube) {
+        float xc = ((float)i + 0.5f) * dx, yc = ((float)j + 0.5f) * dx;
+        float Lx = (float)D.nx * dx, Ly = (float)D.ny * dx;
+        float dxp = xc - P.cube_cx, dyp = yc - P.cube_cy;
+        if (!P.x_solid) {
+            if (dxp > 0.5f * Lx) dxp -= Lx;
+            if (dxp < -0.5f * Lx) dxp += Lx;
+            if (fabsf(dxp) > 0.5f * Lx - dx) return false;  // near the periodic seam
+        }
+        if (dyp > 0.5f * Ly) dyp -= Ly;
+        if (dyp < -0.5f * Ly) dyp += Ly;
+        if (fabsf(dyp) > 0.5f * Ly - dx) return false;
+        float d = cube_sdf(P, D, xc, yc, zc);
+        float margin = 1e-3f * dx + 1e-6f * (fabsf(xc) + fabsf(yc) + fabsf(zc));
+        if (!(d >= 1.2072f * dx + margin)) return false;
+    }
+    return true;
+}
+
+// build_lattice_open_from_free_surface_periodic for one cell (full path)
+static __device__ __noinline__ Geo geo_slow(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i,
+                                     GeoLinks *L) {
+    Geo g;
+    g.fast = false;
+    const float dx = P.dx, hdx = 0.5f * dx;
+    float xc = ((float)i + 0.5f) * dx, yc = ((float)j + 0.5f) * dx, zc = ((float)k + 0.5f) * dx;
+    float eta_c = sample_h(P, D, B.h, xc, yc);
+    float gap_c = zc - eta_c;
+    float ggc = 1.0e6f;
+    int wtc = LBM_WALL_NONE;
+    if (P.include_bed) { ggc = gap_c; wtc = LBM_WALL_BED; }
+    if (P.include_cube) {
+        float cg = cube_sdf(P, D, xc, yc, zc);
+        if (cg < ggc) { ggc = cg; wtc = LBM_WALL_CUBE; }
+    }
+    float sgc = ggc;
+    if (P.use_phi_open_fraction) sgc = phi_cell(P, D, B.h, k, j, i);
+    float frc = 0.5f + sgc / dx;
+    if (frc < 0.0f) frc = 0.0f;
+    if (frc > 1.0f) frc = 1.0f;
+    L->lf[0] = frc;
+    L->wt[0] = (uint8_t)wtc;
+    uint32_t lo = 0u;
+    for (int q = 1; q < 19; ++q) {
+        float xq = xc + hdx * (float)cxq(q);
+        float yq = yc + hdx * (float)cyq(q);
+        float zq = zc + hdx * (float)czq(q);
+        float eta = sample_h(P, D, B.h, xq, yq);
+        float gap = zq - eta;
+        float gg = 1.0e6f;
+        int wq_ = LBM_WALL_NONE;
+        if (P.include_bed) { gg = gap; wq_ = LBM_WALL_BED; }
+        if (P.include_cube) {
+            float cg = cube_sdf(P, D, xq, yq, zq);
+            if (cg < gg) { gg = cg; wq_ = LBM_WALL_CUBE; }
+        }
+        float sg = gg;
+        if (P.use_phi_open_fraction) sg = sample_phi(P, D, B.h, xq, yq, zq);
+        float fr = 0.5f + sg / dx;
+        if (fr < 0.0f) fr = 0.0f;
+        if (fr > 1.0f) fr = 1.0f;
+        float og = P.use_phi_open_flags ? sg : gg;
+        bool open = !(og < 0.0f);
+        if (P.x_solid) {
+            if (i == 0 && cxq(q) > 0) { open = false; fr = 0.0f; wq_ = LBM_WALL_XMIN; }
+            else if (i == D.nx - 1 && cxq(q) < 0) { open = false; fr = 0.0f; wq_ = LBM_WALL_XMAX; }
+        }
+        L->lf[q] = fr;
+        L->wt[q] = (uint8_t)wq_;
+        if (open) lo |= (1u << q);
+    }
+    if (lo) lo |= 1u;
+    g.near = (lo & 0x7FFFEu) != 0x7FFFEu;
+    if (!(lo & 1u)) {
+        for (int q = 1; q < 19; ++q) L->lf[q] = 0.0f;
+    }
+    uint32_t part = 0u;
+    for (int q = 0; q < 19; ++q)
+        if (L->lf[q] < 1.0f) part |= (1u << q);
+    g.part = part;
+    g.lo = lo;
+    return g;
+}
+
+LBM_DEV Geo geo_cell(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i, GeoLinks &L,
+                     bool allow_fast = true) {
+    if (allow_fast && geo_far(P, D, B, k, j, i)) {
+        Geo g;
+        g.lo = 0x7FFFFu;
+        g.part = 0u;
+        g.near = false;
+        g.fast = true;
+        return g;
+    }
+    return geo_slow(P, D, B, k, j, i, &L);
+}
+
+static __device__ __noinline__ bool cell_open_slow(const lbm_params &P, const Dom &D, const BedView &B, int k, int j,
+                                            int i) {
+    GeoLinks L;
+    return (geo_slow(P, D, B, k, j, i, &L).lo & 1u) != 0u;
+}
+// lattice_open[0] only (cheap when far from walls)
+LBM_DEV bool cell_open(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i) {
+    if (geo_far(P, D, B, k, j, i)) return true;
+    return cell_open_slow(P, D, B, k, j, i);
+}
+
+}  // namespace lbm

@@ -1,0 +1,670 @@
+// lbm_step.cuh - per-cell stages of the D3Q19 step, shared by the kernels.
+//
+//   stream_bc    stream() + apply_x_solid_wall_bounceback() +
+//                apply_open_boundary_conditions()      CODEX.py:3418-3712
+//   condition    update_bed_populations_and_reinit()   CODEX.py:2878-2940
+//   macro        macro_step()                          CODEX.py:2943-3008
+//   les_omega    compute_LES()                         CODEX.py:3011-3141
+//   collide      collide_KBC() / collide_regularized() CODEX.py:3143-3416
+#pragma once
+
+#include "lbm_geom.cuh"
+
+namespace lbm {
+
+enum : int {
+    F_WRITE_MACRO = 1,      // store rho/ux/uy/uz of this collide
+    F_WRITE_ALL_OMEGA = 2,  // store omega for every active cell (else near-wall band only)
+    F_COUNT = 4,            // count cut / free-surface / bridge links in stream
+    F_VOF_STATE = 8,        // free-surface state from stored type/fill (else from column height)
+};
+
+struct StepArgs {
+    lbm_params P;
+    Dom D;
+    const void *fsrc;  // populations read
+    void *fdst;        // populations written
+    BedView bed_s;     // geometry of the stream stage
+    BedView bed_c;     // geometry of the condition/collide stage
+    float *rho, *ux, *uy, *uz, *omega;
+    const float *u_les;  // [3][n] velocities for the LES stencil
+    float *u_out;        // [3][n] pre-pass output
+    const float *fs_h, *fs_h_last;
+    const float *fs_fill;
+    const int8_t *fs_type;
+    const float *u_inlet_profile;
+    int *counters;       // [0] cut, [1] fs cut, [2] bridge
+    unsigned *status;    // bit 0: non-finite density
+    uint64_t step;       // 1-based step number of the collide stage (RNG key)
+    int flags;
+};
+
+// --------------------------------------------------------- free surface
+LBM_DEV void classify_height(const lbm_params &P, float h, int k, bool open, int &type, float &fill) {
+    float zb = (float)k * P.dx;
+    float fl = (h - zb) / P.dx;
+    if (fl < 0.0f) fl = 0.0f;
+    if (fl > 1.0f) fl = 1.0f;
+    int ct;
+    if (fl <= 1e-4f) ct = LBM_FS_GAS;
+    else if (fl >= (float)(1.0 - 1e-4)) ct = LBM_FS_LIQUID;
+    else ct = LBM_FS_INTERFACE;
+    if (!open) { fl = 0.0f; ct = LBM_FS_GAS; }
+    type = ct;
+    fill = fl;
+}
+
+// free-surface state of a cell at the start of the step
+LBM_DEV void fs_state(const StepArgs &A, size_t c, int k, int j, bool open, int &type, float &fill) {
+    if (A.flags & F_VOF_STATE) {
+        type = A.fs_type[c];
+        fill = A.fs_fill[c];
+    } else {
+        classify_height(A.P, __ldg(A.fs_h + A.D.col(j, 0) + (c % A.D.nx)), k, open, type, fill);
+    }
+}
+
+// gravity_body_fraction (update_pressure_reference_fields, CODEX.py:710-740)
+LBM_DEV float gbf_of(const lbm_params &P, int k, bool open, int type) {
+    if (!(P.fs_mode != LBM_FS_NONE && open && type != LBM_FS_GAS)) return 0.0f;
+    if (P.pressure_formulation == LBM_PRESSURE_HYDROSTATIC_BALANCED) return 0.0f;
+    if (P.pressure_formulation == LBM_PRESSURE_VOF_COMPONENT_BALANCED) {
+        float zc = ((float)k + 0.5f) * P.dx;
+        return zc < P.fs_base_m ? 0.0f : 1.0f;
+    }
+    return 1.0f;
+}
+LBM_DEV float prh_of(const lbm_params &P, int k, bool open, int type) {
+    if (!(P.fs_mode != LBM_FS_NONE && open && type != LBM_FS_GAS)) return 0.0f;
+    float zc = ((float)k + 0.5f) * P.dx;
+    if (P.pressure_formulation == LBM_PRESSURE_HYDROSTATIC_BALANCED) return P.fs_base_m - zc;
+    if (P.pressure_formulation == LBM_PRESSURE_VOF_COMPONENT_BALANCED) return zc < P.fs_base_m ? P.fs_base_m - zc : 0.0f;
+    return 0.0f;
+}
+// local_g_body_lb, CODEX.py:646-651
+LBM_DEV float g_local(const lbm_params &P, float gbf) {
+    return P.use_component_balanced_pressure ? P.g_lb * gbf : P.g_body_lb;
+}
+// free_surface_hydrostatic_density_at_cell, CODEX.py:821-845
+LBM_DEV float fs_density_cell(const lbm_params &P, float h_col, int k, float gbf) {
+    float head = 0.0f;
+    if (P.use_component_balanced_pressure) {
+        float zc = ((float)k + 0.5f) * P.dx;
+        head = gbf < 0.5f ? zc - P.fs_base_m : 0.0f;
+    } else if (P.use_hydrostatic_balanced_pressure) {
+        head = h_col - P.fs_base_m;
+    } else {
+        float zc = ((float)k + 0.5f) * P.dx;
+        head = h_col - zc;
+    }
+    if (head < 0.0f && !P.use_hydrostatic_balanced_pressure) head = 0.0f;
+    return P.rho0 + P.g_lb * (head / P.dx) / P.one_third;
+}
+// free_surface_pressure_density_at_link, CODEX.py:848-867
+LBM_DEV float fs_density_link(const lbm_params &P, float h_col, int k, int cz, float gbf) {
+    if (P.use_component_balanced_pressure) {
+        float zi = ((float)k + 0.5f) * P.dx - 0.5f * (float)cz * P.dx;
+        float head = 0.0f;
+        if (gbf < 0.5f) head += zi - P.fs_base_m;
+        return P.rho0 + P.g_lb * (head / P.dx) / P.one_third;
+    }
+    if (P.use_hydrostatic_balanced_pressure && P.fs_tracking == LBM_TRACK_VOF) {
+        float zi = ((float)k + 0.5f) * P.dx - 0.5f * (float)cz * P.dx;
+        float head = zi - P.fs_base_m;
+        return P.rho0 + P.g_lb * (head / P.dx) / P.one_third;
+    }
+    return fs_density_cell(P, h_col, k, gbf);
+}
+
+LBM_DEV float smooth01(float x) { return x * x * (3.0f - 2.0f * x); }
+
+// ------------------------------------------------------------ stream + BC
+// post-stream populations of cell (k,j,i) from post-collision fs[]
+template <int S>
+LBM_DEV void stream_bc(const StepArgs &A, const typename Store<S>::T *__restrict__ fs, const Geo &g,
+                       const GeoLinks &L, int k, int j, int i, size_t c, float out[19], int &cut, int &fscut,
+                       int &bridge) {
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    const size_t n = D.n;
+    const bool water = P.fs_mode != LBM_FS_NONE;
+    const bool vof = water && P.fs_tracking == LBM_TRACK_VOF;
+    const float rho0 = P.rho0;
+    const bool open_c = (g.lo & 1u) != 0u;
+    int type_c = LBM_FS_LIQUID;
+    float fill_c = 1.0f;
+    bool dest_gas = false;
+    float gbf_c = 0.0f, hcol = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
+    if (water) {
+        fs_state(A, c, k, j, open_c, type_c, fill_c);
+        dest_gas = type_c == LBM_FS_GAS && open_c;
+        gbf_c = gbf_of(P, k, open_c, type_c);
+        hcol = __ldg(A.fs_h + D.col(j, i));
+        vx = A.ux[c]; vy = A.uy[c]; vz = A.uz[c];
+    }
+#define LDS(q, cell) Store<S>::ld(fs, (size_t)(q) * n + (cell), (q), rho0)
+    out[0] = dest_gas ? feq<0>(rho0, 0.0f, 0.0f, 0.0f, 0.0f) : LDS(0, c);
+#pragma unroll
+    for (int q = 1; q < 19; ++q) {
+        const int cx = cxq(q), cy = cyq(q), cz = czq(q), qb = oppq(q);
+        int sir = i - cx;
+        int si = sir;
+        bool sf = true;
+        if (!P.x_solid) si = sir < 0 ? sir + D.nx : (sir >= D.nx ? sir - D.nx : sir);
+        else if (sir < 0) { si = 0; sf = false; }
+        else if (sir >= D.nx) { si = D.nx - 1; sf = false; }
+        int sj = j - cy;
+        sj = sj < 0 ? sj + D.ny : (sj >= D.ny ? sj - D.ny : sj);
+        int sk = k - cz;
+        float v;
+        if (water) {
+            bool src_gas = false;
+            size_t s = 0;
+            if (sf && sk >= 0 && sk < D.nz) {
+                s = D.cell(sk, sj, si);
+                int ts;
+                float fls;
+                if (A.flags & F_VOF_STATE) {
+                    ts = A.fs_type[s];
+                    if (ts == LBM_FS_GAS) src_gas = cell_open(P, D, A.bed_s, sk, sj, si);
+                } else {
+                    classify_height(P, __ldg(A.fs_h + D.col(sj, si)), sk, true, ts, fls);
+                    if (ts == LBM_FS_GAS) src_gas = cell_open(P, D, A.bed_s, sk, sj, si);
+                }
+            } else if (sk >= D.nz) {
+                src_gas = true;
+            }
+            if (dest_gas) {
+                float e = 0.0f;
+                switch (q) {
+#define FQ(Q) case Q: e = feq<Q>(rho0, 0.0f, 0.0f, 0.0f, 0.0f); break;
+                    FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+                    FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+                }
+                v = e;
+            } else if (!sf) {
+                v = LDS(qb, c);
+                cut++;
+            } else if (sk >= 0 && sk < D.nz && !src_gas) {
+                float fr = (g.part & (1u << q)) ? L.lf[q] : 1.0f;
+                float fst;
+                if (fr < 1.0f) fst = fr * LDS(q, s) + (1.0f - fr) * LDS(qb, c);
+                else fst = LDS(q, s);
+                float o = fst;
+                if (vof && P.vof_link_aperture) {
+                    // vof_link_liquid_aperture of the source, CODEX.py:870-894
+                    float la = 1.0f;
+                    int ts = A.fs_type[s];
+                    if (ts != LBM_FS_LIQUID && cell_open(P, D, A.bed_s, sk, sj, si)) {
+                        if (ts == LBM_FS_GAS) la = 0.0f;
+                        else if (ts == LBM_FS_INTERFACE) {
+                            la = A.fs_fill[s];
+                            if (la < 0.0f) la = 0.0f;
+                            if (la > 1.0f) la = 1.0f;
+                        }
+                    }
+                    if (la < 1.0f) {
+                        float rfs = rho0;
+                        if (P.use_hydrostatic_balanced_pressure || P.fs_boundary == LBM_FSB_HYDROSTATIC)
+                            rfs = fs_density_link(P, hcol, k, cz, gbf_c);
+                        float u2 = usq(vx, vy, vz);
+                        float ffs = 0.0f;
+                        switch (q) {
+#define FQ(Q) case Q: ffs = feq<Q>(rfs, vx, vy, vz, u2) + feq<oppq(Q)>(rfs, vx, vy, vz, u2) - LDS(oppq(Q), c); break;
+                            FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+                            FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+                        }
+                        o = la * fst + (1.0f - la) * ffs;
+                        fscut++;
+                    }
+                }
+                v = o;
+                if (fr < 1.0f) cut++;
+            } else if (sk < 0) {
+                v = LDS(qb, c);
+                cut++;
+            } else {
+                float rfs = rho0;
+                if (P.use_hydrostatic_balanced_pressure || P.fs_boundary == LBM_FSB_HYDROSTATIC)
+                    rfs = fs_density_link(P, hcol, k, cz, gbf_c);
+                float u2 = usq(vx, vy, vz);
+                float ffs = 0.0f;
+                switch (q) {
+#define FQ(Q) case Q: ffs = feq<Q>(rfs, vx, vy, vz, u2) + feq<oppq(Q)>(rfs, vx, vy, vz, u2) - LDS(oppq(Q), c); break;
+                    FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+                    FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+                }
+                float o = ffs;
+                if (vof && P.vof_thin_gap_bridge && sk >= 0 && sk < D.nz && src_gas) {
+                    int bir = si - cx;
+                    int bi = bir;
+                    int bj = pymod(sj - cy + D.ny, D.ny);
+                    int bk = sk - cz;
+                    bool bv = true;
+                    if (!P.x_solid) bi = pymod(bir + D.nx, D.nx);
+                    else if (bir < 0 || bir >= D.nx) bv = false;
+                    if (bk < 0 || bk >= D.nz) bv = false;
+                    if (bv) {
+                        size_t bc = D.cell(bk, bj, bi);
+                        if (A.fs_type[bc] != LBM_FS_GAS && cell_open(P, D, A.bed_s, bk, bj, bi)) {
+                            float bw = fill_c;
+                            float fb = A.fs_fill[bc];
+                            if (fb < bw) bw = fb;
+                            bw *= P.vof_thin_gap_bridge_strength;
+                            if (bw > 0.0f) {
+                                if (bw > 1.0f) bw = 1.0f;
+                                o = (1.0f - bw) * ffs + bw * LDS(q, bc);
+                                bridge++;
+                            }
+                        }
+                    }
+                }
+                v = o;
+                fscut++;
+            }
+        } else {
+            if (!sf) {
+                v = LDS(qb, c);
+                cut++;
+            } else if (sk >= 0 && sk < D.nz) {
+                float fr = (g.part & (1u << q)) ? L.lf[q] : 1.0f;
+                size_t s = D.cell(sk, sj, si);
+                if (fr < 1.0f) {
+                    v = fr * LDS(q, s) + (1.0f - fr) * LDS(qb, c);
+                    cut++;
+                } else {
+                    v = LDS(q, s);
+                }
+            } else if (P.top_free_slip && sk >= D.nz) {
+                // specular wall above the top row (extension)
+                v = LDS(mirzq(q), D.cell(D.nz - 1, sj, si));
+            } else {
+                v = LDS(q, c);
+            }
+        }
+        out[q] = v;
+    }
+    // apply_x_solid_wall_bounceback, CODEX.py:3554-3580
+    if (P.x_solid && (i == 0 || i == D.nx - 1)) {
+        bool active = !(water && dest_gas);
+        if (active) {
+#pragma unroll
+            for (int q = 1; q < 19; ++q) {
+                if ((i == 0 && cxq(q) > 0) || (i == D.nx - 1 && cxq(q) < 0)) out[q] = LDS(oppq(q), c);
+            }
+        }
+    }
+    // (A) x-fringe, CODEX.py:3616-3645
+    if (P.enable_x_fringe && i < 5 && open_c && k > D.nz / 2) {
+        float s_ = 1.0f - (float)i / 4.0f;
+        float kr = (float)k / (float)(D.nz - 1);
+        float strength = 0.05f * (kr * kr - 0.25f);
+        float sigma = strength * smooth01(s_);
+        float uxt = __ldg(A.u_inlet_profile + k) + 0.0f;
+        float u2 = usq(uxt, 0.0f, 0.0f);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            float ft = 0.0f;
+            switch (q) {
+#define FQ(Q) case Q: ft = feq<Q>(rho0, uxt, 0.0f, 0.0f, u2); break;
+                FQ(0) FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+                FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+            }
+            out[q] = (1.0f - sigma) * out[q] + sigma * ft;
+        }
+    }
+    // (B) top drive, CODEX.py:3651-3663
+    if (P.enable_top_drive && k == D.nz - 1 && open_c) {
+        float ut = P.u_top_lb;
+        float u2 = usq(ut, 0.0f, 0.0f);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            switch (q) {
+#define FQ(Q) case Q: out[q] = feq<Q>(rho0, ut, 0.0f, 0.0f, u2); break;
+                FQ(0) FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+                FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+            }
+        }
+    }
+    // (C) moving-wall IBB on near-obstacle cells, CODEX.py:3674-3712
+    if (g.near) {
+        const float hdx = 0.5f * P.dx;
+        float xc = ((float)i + 0.5f) * P.dx, yc = ((float)j + 0.5f) * P.dx;
+        const BedView &B = A.bed_s;
+#pragma unroll
+        for (int q = 1; q < 19; ++q) {
+            if (!(g.part & (1u << q))) continue;   // fraction 1: identity
+            const int qb = oppq(q);
+            float fo = L.lf[q];
+            float wx = 0.0f, wy = 0.0f, wz = 0.0f;
+            if (L.wt[q] == LBM_WALL_BED) {
+                size_t a = D.col(j, i);
+                wx = __ldg(B.uw + a); wy = __ldg(B.vw + a); wz = __ldg(B.ww + a);
+                if (P.use_link_wall_velocity)
+                    sample_wall(P, D, B, xc + hdx * (float)cxq(q), yc + hdx * (float)cyq(q), wx, wy, wz);
+            }
+            float cuw = (float)cxq(qb) * wx + (float)cyq(qb) * wy + (float)czq(qb) * wz;
+            float fwall = LDS(qb, c) - 6.0f * wq(qb) * rho0 * cuw;
+            out[q] = out[q] * fo + fwall * (1.0f - fo);
+        }
+    }
+#undef LDS
+}
+
+// ---------------------------------------------------- pre-collision stages
+// update_bed_populations_and_reinit for one cell (geometry of the collide step)
+LBM_DEV void condition(const lbm_params &P, const Dom &D, const BedView &B, const Geo &g, const GeoLinks &L, int k,
+                       int j, int i, float f[19]) {
+    if (g.fast || (g.lo == 0x7FFFFu)) return;   // no closed link
+    const bool moving = P.bed_profile == LBM_BED_MOVING_SINE;
+    const float hdx = 0.5f * P.dx;
+    size_t a = D.col(j, i);
+    float ux_ = __ldg(B.uw + a), uy_ = __ldg(B.vw + a), uz_ = __ldg(B.ww + a);
+    float xc = ((float)i + 0.5f) * P.dx, yc = ((float)j + 0.5f) * P.dx;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        if (g.lo & (1u << q)) continue;
+        float fr = (g.part & (1u << q)) ? L.lf[q] : 1.0f;
+        int wt = L.wt[q];
+        bool apply = false;
+        float vx = 0.0f, vy = 0.0f, vz = 0.0f;
+        if (wt == LBM_WALL_BED && moving) {
+            apply = true;
+            vx = ux_; vy = uy_; vz = uz_;
+        } else if (!P.physics_water) {
+            apply = true;
+            if (wt == LBM_WALL_BED) { vx = ux_; vy = uy_; vz = uz_; }
+        }
+        if (!apply) continue;
+        if (wt == LBM_WALL_BED && P.use_link_wall_velocity)
+            sample_wall(P, D, B, xc + hdx * (float)cxq(q), yc + hdx * (float)cyq(q), vx, vy, vz);
+        float u2 = usq(vx, vy, vz);
+        float fe = 0.0f;
+        switch (q) {
+#define FQ(Q) case Q: fe = feq<Q>(P.rho0, vx, vy, vz, u2); break;
+            FQ(0) FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+            FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+        }
+        f[q] = fr * f[q] + (1.0f - fr) * fe;
+    }
+}
+
+// macro_step for one cell; returns rho, u (gas/Guo/top-drive rules)
+LBM_DEV void macro(const lbm_params &P, const Dom &D, const float f[19], int k, bool water, int type, float gbf,
+                   float &r, float &vx, float &vy, float &vz) {
+    float rr = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) rr += f[q];
+    float jx = 0.0f, jy = 0.0f, jz = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        if (cxq(q) > 0) jx += f[q]; else if (cxq(q) < 0) jx += -f[q];
+        if (cyq(q) > 0) jy += f[q]; else if (cyq(q) < 0) jy += -f[q];
+        if (czq(q) > 0) jz += f[q]; else if (czq(q) < 0) jz += -f[q];
+    }
+    r = rr;
+    if (water) {
+        if (type == LBM_FS_GAS) {
+            r = P.rho0; vx = 0.0f; vy = 0.0f; vz = 0.0f;
+        } else {
+            float fz = -rr * g_local(P, gbf);
+            float inv = 1.0f / rr;
+            vx = jx * inv;
+            vy = jy * inv;
+            vz = (jz + 0.5f * fz) * inv;
+        }
+    } else {
+        float inv = 1.0f / rr;
+        vx = jx * inv;
+        vy = jy * inv;
+        vz = jz * inv;
+    }
+    if (P.enable_top_drive && k == D.nz - 1) {
+        vx = P.u_top_lb; vy = 0.0f; vz = 0.0f;
+    }
+}
+
+// log-law wall model of compute_LES (CODEX.py:3097-3129), applied when the
+// cell below is solid; out of line because it runs only next to the bed
+static __device__ __noinline__ float wall_model_nu(const StepArgs &A, int k, int j, int i, float vx, float vy, float nu_t) {
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    GeoLinks Lb;
+    Geo gb = geo_slow(P, D, A.bed_c, k - 1, j, i, &Lb);
+    if (gb.lo & 1u) return nu_t;
+    float phi = phi_cell(P, D, A.bed_c.h, k, j, i);
+    float dist = fmaxf(phi, P.wall_dist_floor);
+    float lv = lbm_logf(dist / P.z0_phys);
+    if (lv < 2.0f) lv = 2.0f;
+    float uwx = 0.0f, uwy = 0.0f;
+    if (Lb.wt[0] == LBM_WALL_BED) {
+        uwx = __ldg(A.bed_c.uw + D.col(j, i));
+        uwy = __ldg(A.bed_c.vw + D.col(j, i));
+    }
+    float rx = vx - uwx, ry = vy - uwy;
+    float sp = sqrtf(rx * rx + ry * ry);
+    if (sp > 1e-6f) {
+        float ut = sp * P.kappa / lv;
+        float tw = ut * ut;
+        float sa = sp / 0.5f;
+        float nwm = tw / sa;
+        float ntw = nwm - P.nu0;
+        if (ntw < 0.0f) ntw = 0.0f;
+        nu_t = fmaxf(nu_t, ntw);
+    }
+    return nu_t;
+}
+
+// compute_LES for one active cell: omega from the 7-point velocity stencil
+LBM_DEV float les_omega(const StepArgs &A, int k, int j, int i, size_t c, float vx, float vy, float vz) {
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    const size_t n = D.n;
+    int ip = i + 1 == D.nx ? 0 : i + 1, im = i == 0 ? D.nx - 1 : i - 1;
+    int jp = j + 1 == D.ny ? 0 : j + 1, jm = j == 0 ? D.ny - 1 : j - 1;
+    int kp = k + 1 >= D.nz ? D.nz - 1 : k + 1, km = k - 1 < 0 ? 0 : k - 1;
+    const float *U = A.u_les, *V = A.u_les + n, *W = A.u_les + 2 * n;
+    size_t cxp = D.cell(k, j, ip), cxm = D.cell(k, j, im), cyp = D.cell(k, jp, i), cym = D.cell(k, jm, i);
+    size_t czp = D.cell(kp, j, i), czm = D.cell(km, j, i);
+    float du_dx = 0.5f * (__ldg(U + cxp) - __ldg(U + cxm));
+    float du_dy = 0.5f * (__ldg(U + cyp) - __ldg(U + cym));
+    float du_dz = 0.5f * (__ldg(U + czp) - __ldg(U + czm));
+    float dv_dx = 0.5f * (__ldg(V + cxp) - __ldg(V + cxm));
+    float dv_dy = 0.5f * (__ldg(V + cyp) - __ldg(V + cym));
+    float dv_dz = 0.5f * (__ldg(V + czp) - __ldg(V + czm));
+    float dw_dx = 0.5f * (__ldg(W + cxp) - __ldg(W + cxm));
+    float dw_dy = 0.5f * (__ldg(W + cyp) - __ldg(W + cym));
+    float dw_dz = 0.5f * (__ldg(W + czp) - __ldg(W + czm));
+    float Sxx = du_dx, Syy = dv_dy, Szz = dw_dz;
+    float Sxy = 0.5f * (du_dy + dv_dx);
+    float Sxz = 0.5f * (du_dz + dw_dx);
+    float Syz = 0.5f * (dv_dz + dw_dy);
+    float Sc = (Sxx * Sxx + Syy * Syy + Szz * Szz + 2.0f * (Sxy * Sxy + Sxz * Sxz + Syz * Syz));
+    float Smag = sqrtf(2.0f * Sc + 1e-6f);
+    float nu_t = P.cs_delta_sq * Smag;
+    if (nu_t > P.nu_t_max) nu_t = P.nu_t_max;
+    if (k > 0 && !geo_far(P, D, A.bed_c, k - 1, j, i)) nu_t = wall_model_nu(A, k, j, i, vx, vy, nu_t);
+    float nu_eff = P.nu0 + nu_t;
+    float tau_eff = 0.5f + 3.0f * nu_eff;
+    if (tau_eff > 2.0f) tau_eff = 2.0f;
+    return 1.0f / tau_eff;
+}
+
+// Guo forcing term (CODEX.py:3223-3232, 3389-3396)
+template <int Q>
+LBM_DEV float guo(const lbm_params &P, float om, float vx, float vy, float vz, float fz) {
+    const float cs2 = P.one_third;
+    float czi = (float)czq(Q);
+    float cdu = cdot<Q>(vx, vy, vz);
+    return wq(Q) * (1.0f - 0.5f * om) * (((czi - vz) / cs2) + (cdu * czi / (cs2 * cs2))) * fz;
+}
+
+// collide_KBC / collide_regularized for one cell (in place on f[])
+LBM_DEV void collide(const StepArgs &A, size_t c, int k, bool solid, bool water, bool gas, float gbf, float r,
+                     float vx, float vy, float vz, float om, float f[19]) {
+    const lbm_params &P = A.P;
+    const float cs2 = P.one_third;
+    const float inv_2cs4 = 1.0f / (2.0f * cs2 * cs2);
+    const float eps = 1e-6f;
+    if (gas) { r = P.rho0; vx = 0.0f; vy = 0.0f; vz = 0.0f; }
+    float u2 = usq(vx, vy, vz);
+    float fe[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        switch (q) {
+#define FQ(Q) case Q: fe[q] = feq<Q>(r, vx, vy, vz, u2); break;
+            FQ(0) FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+            FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+        }
+    }
+    if (P.collision == LBM_COLLIDE_REGULARIZED) {
+        if (gas) {
+#pragma unroll
+            for (int q = 0; q < 19; ++q) f[q] = fe[q];
+            return;
+        }
+        float Pxx = 0.0f, Pyy = 0.0f, Pzz = 0.0f, Pxy = 0.0f, Pxz = 0.0f, Pyz = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            float fn = f[q] - fe[q];
+            const int a = cxq(q), b = cyq(q), d = czq(q);
+            if (a != 0) Pxx += fn;
+            if (b != 0) Pyy += fn;
+            if (d != 0) Pzz += fn;
+            if (a * b != 0) Pxy += a * b > 0 ? fn : -fn;
+            if (a * d != 0) Pxz += a * d > 0 ? fn : -fn;
+            if (b * d != 0) Pyz += b * d > 0 ? fn : -fn;
+        }
+        float fz = water ? -r * g_local(P, gbf) : 0.0f;
+        float fsv[19];
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const int a = cxq(q), b = cyq(q), d = czq(q);
+            float Qxx = (float)(a * a) - cs2, Qyy = (float)(b * b) - cs2, Qzz = (float)(d * d) - cs2;
+            float t = Qxx * Pxx + Qyy * Pyy + Qzz * Pzz;
+            float s2 = (a * b != 0 ? (a * b > 0 ? Pxy : -Pxy) : 0.0f);
+            if (a * d != 0) s2 = (a * b != 0) ? s2 + (a * d > 0 ? Pxz : -Pxz) : (a * d > 0 ? Pxz : -Pxz);
+            if (b * d != 0) s2 = (a * b != 0 || a * d != 0) ? s2 + (b * d > 0 ? Pyz : -Pyz) : (b * d > 0 ? Pyz : -Pyz);
+            float fnr = wq(q) * inv_2cs4 * (t + 2.0f * s2);
+            float fi = 0.0f;
+            if (water) {
+                switch (q) {
+#define FQ(Q) case Q: fi = guo<Q>(P, om, vx, vy, vz, fz); break;
+                    FQ(0) FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+                    FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+                }
+            }
+            fsv[q] = fe[q] + (1.0f - om) * fnr + fi;
+        }
+        float alpha = 1.0f;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            if (fsv[q] < eps) {
+                float den = fsv[q] - fe[q];
+                if (den < 0.0f) {
+                    float cand = (eps - fe[q]) / den;
+                    if (cand < alpha) alpha = cand;
+                }
+            }
+        }
+        if (alpha < 0.0f) alpha = 0.0f;
+        if (alpha > 1.0f) alpha = 1.0f;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) f[q] = fe[q] + alpha * (fsv[q] - fe[q]);
+        return;
+    }
+    // KBC-style BGK with positivity limiter, top sponge and backscatter
+    if (P.enable_top_sponge && k > A.D.nz - 3) {
+        const float om_sp = 1.0f / 0.95f;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) f[q] = f[q] - om_sp * (f[q] - fe[q]);
+        return;
+    }
+    float fz = (water && !gas) ? -r * g_local(P, gbf) : 0.0f;
+    float fsv[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        float fi = 0.0f;
+        if (water && !gas) {
+            switch (q) {
+#define FQ(Q) case Q: fi = guo<Q>(P, om, vx, vy, vz, fz); break;
+                FQ(0) FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+                FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+            }
+        }
+        fsv[q] = f[q] - om * (f[q] - fe[q]) + fi;
+    }
+    float alpha = 1.0f;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        if (fsv[q] < eps) {
+            float den = fsv[q] - fe[q];
+            if (den < 0.0f) {
+                float cand = (eps - fe[q]) / den;
+                if (cand < alpha) alpha = cand;
+            }
+        }
+    }
+    if (alpha < 0.0f) alpha = 0.0f;
+    if (alpha > 1.0f) alpha = 1.0f;
+    float fp[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) fp[q] = fe[q] + alpha * (fsv[q] - fe[q]);
+    if (P.c_backscatter > 0.0f && !solid) {
+        float Pxx = 0.0f, Pyy = 0.0f, Pzz = 0.0f, Pxy = 0.0f, Pxz = 0.0f, Pyz = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            float fn = fp[q] - fe[q];
+            const int a = cxq(q), b = cyq(q), d = czq(q);
+            if (a != 0) Pxx += fn;
+            if (b != 0) Pyy += fn;
+            if (d != 0) Pzz += fn;
+            if (a * b != 0) Pxy += a * b > 0 ? fn : -fn;
+            if (a * d != 0) Pxz += a * d > 0 ? fn : -fn;
+            if (b * d != 0) Pyz += b * d > 0 ? fn : -fn;
+        }
+        float tr = (Pxx + Pyy + Pzz) / 3.0f;
+        Pxx -= tr; Pyy -= tr; Pzz -= tr;
+        float xi = 2.0f * lbm_uniform01(P.seed, A.step, (uint64_t)c) - 1.0f;
+        float scale = P.c_backscatter * xi;
+        float dl[19];
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const int a = cxq(q), b = cyq(q), d = czq(q);
+            float Qxx = (float)(a * a) - cs2, Qyy = (float)(b * b) - cs2, Qzz = (float)(d * d) - cs2;
+            float t = Qxx * (scale * Pxx) + Qyy * (scale * Pyy) + Qzz * (scale * Pzz);
+            float s2 = 0.0f;
+            bool have = false;
+            if (a * b != 0) { float v = scale * Pxy; s2 = a * b > 0 ? v : -v; have = true; }
+            if (a * d != 0) { float v = scale * Pxz; v = a * d > 0 ? v : -v; s2 = have ? s2 + v : v; have = true; }
+            if (b * d != 0) { float v = scale * Pyz; v = b * d > 0 ? v : -v; s2 = have ? s2 + v : v; have = true; }
+            float contr = t + 2.0f * s2;
+            dl[q] = wq(q) * inv_2cs4 * contr;
+        }
+        float gamma = 1.0f;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            if (dl[q] < 0.0f) {
+                float cand = (eps - fp[q]) / dl[q];
+                if (cand < gamma) gamma = cand;
+            }
+        }
+        if (gamma < 0.0f) gamma = 0.0f;
+        if (gamma > 1.0f) gamma = 1.0f;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) fp[q] = fp[q] + gamma * dl[q];
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = fp[q];
+}
+
+}  // namespace lbm

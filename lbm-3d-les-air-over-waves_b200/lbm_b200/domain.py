@@ -1,0 +1,102 @@
+"""One simulation domain on a CUDA device: torch-owned buffers, the C ABI.
+
+    dom = Domain(config_or_env, device="cuda:0")
+    dom.step(100)
+    ux = dom.field("ux")          # torch tensor on the device
+    dom.close()
+
+Buffers are allocated by torch on the device and passed to the library as
+raw pointers; the library owns only scratch (bed slots, the LES velocity
+stencil, counters).  All calls are issued on the domain's CUDA stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import abi, native, state
+from .config import SolverConfig, load_config
+from .hostinit import make_init_noise, prepare_initial_density
+
+
+class Domain:
+    def __init__(self, cfg, device="cuda:0", stream=None, noise=None, rho_initial=None, with_diag: bool = True,
+                 init: bool = True):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise native.NativeUnavailable("a CUDA device is required (no CPU fallback)")
+        if not isinstance(cfg, SolverConfig):
+            cfg = load_config(cfg)
+        self.cfg = cfg
+        self.device = torch.device(device)
+        self.lib = native.load()
+        self.stream = stream if stream is not None else torch.cuda.Stream(self.device)
+        self.params = abi.make_params(cfg)
+        self.arrays = state.allocate_torch(cfg, self.device, with_diag=with_diag)
+        self.arrays["piecewise_bed_z"].copy_(torch.as_tensor(np.asarray(cfg.piecewise_bed_z_np, dtype=np.float32)))
+        self.ctx = C.c_void_p()
+        self._check(self.lib.lbm_create(C.byref(self.params), C.byref(self.ctx)), "lbm_create")
+        self.bufs = state.make_buffers(self.arrays)
+        self._check(self.lib.lbm_bind(self.ctx, C.byref(self.bufs)), "lbm_bind")
+        if init:
+            self.initialize(noise=noise, rho_initial=rho_initial)
+
+    # ------------------------------------------------------------------
+    def _check(self, status, what):
+        abi.check(self.lib, self.ctx, status, what)
+
+    def _sp(self):
+        return C.c_void_p(self.stream.cuda_stream)
+
+    def initialize(self, noise=None, rho_initial=None):
+        """init sequence of main() (CODEX.py:3776-3792)."""
+        import torch
+
+        torch.cuda.synchronize(self.device)
+        self._check(self.lib.lbm_init_geometry(self.ctx, self._sp()), "lbm_init_geometry")
+        self.stream.synchronize()
+        a = self.arrays
+        if noise is None:
+            noise = make_init_noise(self.cfg)
+        if rho_initial is None:
+            rho_initial = prepare_initial_density(self.cfg, a["fs_h"].cpu().numpy(), a["water_h"].cpu().numpy())
+        a["init_noise"].copy_(torch.as_tensor(np.ascontiguousarray(noise)))
+        a["rho_initial"].copy_(torch.as_tensor(np.ascontiguousarray(rho_initial)))
+        torch.cuda.synchronize(self.device)
+        self._check(self.lib.lbm_init_fields(self.ctx, self._sp()), "lbm_init_fields")
+        self.stream.synchronize()
+
+    def step(self, n: int = 1):
+        self._check(self.lib.lbm_step(self.ctx, int(n), self._sp()), "lbm_step")
+
+    def export_diagnostics(self):
+        self._check(self.lib.lbm_export_diagnostics(self.ctx, self._sp()), "lbm_export_diagnostics")
+
+    def counters(self) -> dict:
+        c = abi.LbmCounters()
+        self._check(self.lib.lbm_read_counters(self.ctx, C.byref(c)), "lbm_read_counters")
+        return c.as_dict()
+
+    def synchronize(self):
+        self.stream.synchronize()
+
+    def f(self):
+        """Current populations (the buffer the reference calls f)."""
+        return self.arrays["f1" if self.counters()["current_f"] else "f0"]
+
+    def field(self, name: str):
+        return self.arrays[name]
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.stream.synchronize()
+            self.lib.lbm_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

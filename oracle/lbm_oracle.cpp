@@ -269,6 +269,8 @@ struct Sim : CtxBase {
            in the reference; wrap it */
         if (i0 >= Nx) i0 -= Nx;
         if (j0 >= Ny) j0 -= Ny;
+        if (i0 < 0) i0 += Nx;
+        if (j0 < 0) j0 += Ny;
         i1 = (i0 + 1) % Nx;
         j1 = (j0 + 1) % Ny;
     }
@@ -680,6 +682,7 @@ static int make_ctx(const lbm_params *params, lbm_ctx **out, bool fp64) {
     if (!params || !out) return LBM_ERR_BAD_ARG;
     if (params->abi_version != LBM_ABI_VERSION || params->magic_end != LBM_PARAMS_MAGIC) return LBM_ERR_BAD_ARG;
     if (params->nx < 1 || params->ny < 1 || params->nz < 2) return LBM_ERR_BAD_ARG;
+    if (params->x_solid && params->nx < 2) return LBM_ERR_BAD_ARG;
     lbm_ctx *c = new lbm_ctx;
     if (fp64) {
         auto *s = new Sim<double>();

@@ -288,6 +288,15 @@ int lbm_export_diagnostics(lbm_ctx *ctx, void *stream);
 /* Copy scalar counters to the host (synchronises the stream). */
 int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out);
 
+/* Measurement hook (no counterpart in the reference): when enabled, the
+   library brackets every launch of its dominant step kernel (the interior
+   one-pass kernel) with CUDA events on the caller's stream.
+   lbm_kernel_timing synchronises and returns the summed device time, the
+   number of launches and the cells one launch updates.  The CPU oracle
+   reports zeros. */
+int lbm_set_kernel_timing(lbm_ctx *ctx, int32_t enable);
+int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t *cells_per_launch);
+
 int lbm_destroy(lbm_ctx *ctx);
 const char *lbm_last_error(lbm_ctx *ctx);
 

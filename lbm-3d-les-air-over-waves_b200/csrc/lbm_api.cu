@@ -21,13 +21,15 @@
 #include <cuda_runtime.h>
 
 #include <cstdio>
+#include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "lbm_b200.h"
 #include "lbm_launch.h"
-#include "lbm_step.cuh"
 
 using namespace lbm;
 
@@ -36,10 +38,29 @@ namespace {
 enum { CNT_CUT = 0, CNT_FSCUT = 1, CNT_BRIDGE = 2, CNT_FS_REFILL = 3, CNT_COALESCE = 4, CNT_VOF_EXCESS = 5,
        CNT_ORPHAN = 6, CNT_COLLAPSE = 7, CNT_DET = 8, CNT_CMP = 9, CNT_SWEEPS = 10, CNT_N = 16 };
 
+// constant-memory parameter slots (LBM_MAX_SLOTS live contexts at a time)
+std::mutex g_slot_mutex;
+bool g_slot_used[LBM_MAX_SLOTS] = {false};
+
+int acquire_slot() {
+    std::lock_guard<std::mutex> lock(g_slot_mutex);
+    for (int s = 0; s < LBM_MAX_SLOTS; ++s)
+        if (!g_slot_used[s]) {
+            g_slot_used[s] = true;
+            return s;
+        }
+    return -1;
+}
+void release_slot(int s) {
+    std::lock_guard<std::mutex> lock(g_slot_mutex);
+    if (s >= 0 && s < LBM_MAX_SLOTS) g_slot_used[s] = false;
+}
+
 }  // namespace
 
 struct lbm_ctx {
     lbm_params P;
+    int slot = -1;
     Dom D;
     lbm_buffers b;
     bool bound = false;
@@ -55,7 +76,22 @@ struct lbm_ctx {
     unsigned *dstatus = nullptr;
     float *dfcount = nullptr;
     std::vector<void *> owned;
+    double bed_bound = 0.0;   // upper bound of the bed height over the run
+    // optional per-launch timing of the interior kernel
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;  // pairs (start, stop)
+    size_t ev_used = 0;
+    int64_t timed_cells = 0;
 };
+
+static void timed_mark(lbm_ctx *ctx, cudaStream_t st) {
+    if (ctx->ev_used == ctx->ev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ctx->ev.push_back(e);
+    }
+    cudaEventRecord(ctx->ev[ctx->ev_used++], st);
+}
 
 static int fail(lbm_ctx *c, int code, const std::string &msg) {
     if (c) c->err = msg;
@@ -71,6 +107,9 @@ static int cuda_check(lbm_ctx *c, cudaError_t e, const char *what) {
         if (_s != LBM_OK) return _s;                        \
     } while (0)
 #define CK_LAUNCH(what) CK(cudaGetLastError(), what)
+
+static inline int64_t P_nx(const lbm_ctx *c) { return c->P.nx; }
+static inline int64_t P_ny(const lbm_ctx *c) { return c->P.ny; }
 
 static BedView slot_view(const lbm_ctx *ctx, int s) {
     BedView v;
@@ -91,6 +130,7 @@ static InitArgs init_args(lbm_ctx *ctx, int slot) {
     memset(&I, 0, sizeof I);
     const lbm_buffers &b = ctx->b;
     I.P = ctx->P;
+    I.slot = ctx->slot;
     I.D = ctx->D;
     I.bed = slot_view(ctx, slot);
     I.f_cur = b.f[ctx->cur];
@@ -113,6 +153,7 @@ static StepArgs step_args(lbm_ctx *ctx) {
     memset(&A, 0, sizeof A);
     const lbm_buffers &b = ctx->b;
     A.P = ctx->P;
+    A.slot = ctx->slot;
     A.D = ctx->D;
     A.rho = b.rho; A.ux = b.ux; A.uy = b.uy; A.uz = b.uz; A.omega = b.omega;
     A.u_les = ctx->u_les;
@@ -122,6 +163,11 @@ static StepArgs step_args(lbm_ctx *ctx) {
     A.u_inlet_profile = b.u_inlet_profile;
     A.counters = ctx->dcount;
     A.status = ctx->dstatus;
+    A.zlo[0] = 0;
+    A.zcnt[0] = ctx->P.nz;
+    A.zi0 = 0;
+    A.zi1 = -1;
+    A.chunk = 0;
     return A;
 }
 
@@ -155,10 +201,75 @@ static int bed_step(lbm_ctx *ctx, int64_t m, cudaStream_t st) {
     return LBM_OK;
 }
 
+// Split of the planes between the interior tile kernel and the general
+// kernels.  The tile path needs: air mode without free surface, periodic x
+// without the x fringe, no cube, no phi geometry, nx and ny multiples of
+// the tile.  Interior planes start one plane above the first plane that is
+// provably above the bed at all times (so no link there is cut and the
+// cell below is fluid) and end below the top row.
+struct Plan {
+    bool tile = false;
+    int zi0 = 0, zi1 = -1, chunk = 64;
+    int zlo[3] = {0, 0, 0}, zcnt[3] = {0, 0, 0};
+};
+
+static Plan plan_planes(const lbm_ctx *ctx) {
+    const lbm_params &P = ctx->P;
+    Plan R;
+    R.zlo[0] = 0;
+    R.zcnt[0] = P.nz;
+    const char *off = getenv("LBM_B200_NO_TILE");
+    if (off && off[0] == '1') return R;
+    if (P.fs_mode != LBM_FS_NONE || P.x_solid || P.enable_x_fringe || P.include_cube || P.use_phi_open_fraction ||
+        P.use_phi_open_flags || P.nx % LBM_TILE || P.ny % LBM_TILE)
+        return R;
+    int kf = 0;
+    if (P.include_bed) {
+        double hb = ctx->bed_bound;
+        double dx = (double)P.dx;
+        kf = (int)ceil(hb / dx + 0.5 + 1e-3 + 1e-5 * ((double)P.nz + fabs(hb) / dx));
+        if (kf < 0) kf = 0;
+    }
+    int zi0 = kf + 1, zi1 = P.nz - 2;
+    if (zi0 < 1) zi0 = 1;
+    if (zi1 < zi0) return R;
+    R.tile = true;
+    R.zi0 = zi0;
+    R.zi1 = zi1;
+    // planes per block: enough blocks for ~4 waves of 2 blocks per SM, at
+    // least 8 planes (each chunk recomputes 2 neighbour planes), at most 64
+    const int ni = zi1 - zi0 + 1;
+    const int tiles = (P.nx / LBM_TILE) * (P.ny / LBM_TILE);
+    const int want_chunks = (4 * 2 * 148 + tiles - 1) / tiles;
+    int chunk = (ni + want_chunks - 1) / want_chunks;
+    if (chunk < 8) chunk = 8;
+    if (chunk > 64) chunk = 64;
+    const char *ch = getenv("LBM_B200_TILE_CHUNK");
+    if (ch && atoi(ch) > 0) chunk = atoi(ch);
+    R.chunk = chunk;
+    R.zlo[0] = 0;
+    R.zcnt[0] = zi0;
+    R.zlo[1] = zi1 + 1;
+    R.zcnt[1] = P.nz - (zi1 + 1);
+    return R;
+}
+
+static void apply_plan(StepArgs &A, const Plan &R) {
+    for (int r = 0; r < 3; ++r) {
+        A.zlo[r] = R.zlo[r];
+        A.zcnt[r] = R.zcnt[r];
+    }
+    A.zi0 = R.zi0;
+    A.zi1 = R.zi1;
+    A.chunk = R.chunk;
+}
+
 static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     const int64_t n = ctx->nstep;
     const bool les = ctx->P.use_les != 0;
+    const Plan R = plan_planes(ctx);
     StepArgs A = step_args(ctx);
+    apply_plan(A, R);
     int s;
     if ((s = bed_step(ctx, n + 1, st)) != LBM_OK) return s;
     int src = ctx->cur;
@@ -171,6 +282,10 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     if (les) {
         launch_step_kernel(KER_PREPASS_CANON, A, st);
         CK_LAUNCH("prepass");
+    }
+    if (R.tile) {
+        launch_step_kernel(KER_TILE_CANON, A, st);
+        CK_LAUNCH("tile");
     }
     launch_step_kernel(KER_COLLIDE_CANON, A, st);
     CK_LAUNCH("collide");
@@ -187,6 +302,15 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
             launch_step_kernel(KER_PREPASS_FUSED, A, st);
             CK_LAUNCH("prepass fused");
         }
+        if (R.tile) {
+            if (ctx->timing) timed_mark(ctx, st);
+            launch_step_kernel(KER_TILE_FUSED, A, st);
+            CK_LAUNCH("tile fused");
+            if (ctx->timing) {
+                timed_mark(ctx, st);
+                ctx->timed_cells = (int64_t)(R.zi1 - R.zi0 + 1) * P_nx(ctx) * P_ny(ctx);
+            }
+        }
         launch_step_kernel(KER_COLLIDE_FUSED, A, st);
         CK_LAUNCH("fused");
         src = 1 - src;
@@ -199,6 +323,10 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     A.flags = F_COUNT;
     launch_step_kernel(KER_STREAM, A, st);
     CK_LAUNCH("stream");
+    if (R.tile) {
+        launch_step_kernel(KER_STREAM_INTERIOR, A, st);
+        CK_LAUNCH("stream interior");
+    }
     ctx->cur = 1 - src;
     ctx->nstep = n + K;
     return LBM_OK;
@@ -211,6 +339,8 @@ static int step_height(lbm_ctx *ctx, int K, cudaStream_t st) {
         int64_t m = ctx->nstep + 1;
         if ((s = bed_step(ctx, m, st)) != LBM_OK) return s;
         StepArgs A = step_args(ctx);
+        A.zlo[0] = 0;
+        A.zcnt[0] = ctx->P.nz;
         A.bed_s = slot_view(ctx, (int)(m & 1));
         A.bed_c = A.bed_s;
         A.step = (uint64_t)m;
@@ -273,6 +403,21 @@ int lbm_create(const lbm_params *params, lbm_ctx **out) {
     ctx->D.nz = params->nz;
     ctx->D.a = (size_t)params->nx * params->ny;
     ctx->D.n = ctx->D.a * params->nz;
+    if (ctx->D.n > 0x7fffffffULL) {
+        delete ctx;
+        return LBM_ERR_BAD_ARG;
+    }
+    ctx->slot = acquire_slot();
+    if (ctx->slot < 0) {
+        delete ctx;
+        return LBM_ERR_UNSUPPORTED;
+    }
+    cudaError_t e = upload_params(ctx->slot, ctx->P);
+    if (e != cudaSuccess) {
+        release_slot(ctx->slot);
+        delete ctx;
+        return LBM_ERR_CUDA;
+    }
     *out = ctx;
     return LBM_OK;
 }
@@ -323,6 +468,20 @@ int lbm_init_geometry(lbm_ctx *ctx, void *stream) {
     ctx->last_stream = st;
     ctx->cur = 0;
     ctx->nstep = 0;
+    {
+        // upper bound of the bed height for the interior-plane split
+        const lbm_params &P = ctx->P;
+        double hb = (double)P.bed_offset_m;
+        if (P.bed_profile == LBM_BED_MOVING_SINE) hb += fabs((double)P.bed_amp1) + fabs((double)P.bed_amp2);
+        if (P.bed_profile == LBM_BED_PIECEWISE) {
+            std::vector<float> pw(P.nx);
+            CK(cudaMemcpy(pw.data(), ctx->b.piecewise_bed_z, P.nx * sizeof(float), cudaMemcpyDeviceToHost),
+               "piecewise copy");
+            hb = -1e30;
+            for (float v : pw) hb = v > hb ? v : hb;
+        }
+        ctx->bed_bound = hb;
+    }
     InitArgs I = init_args(ctx, 0);
     launch_init_constants(I, st);
     CK_LAUNCH("init constants");
@@ -396,6 +555,7 @@ int lbm_export_diagnostics(lbm_ctx *ctx, void *stream) {
     E.lattice_wall_type = ctx->b.lattice_wall_type;
     E.prh = ctx->b.pressure_reference_head;
     E.gbf = ctx->b.gravity_body_fraction;
+    E.types_are_prev = ctx->nstep > 0 ? 1 : 0;
     launch_export(I, E, st);
     CK_LAUNCH("export");
     if (ctx->b.vof_exterior_gas)
@@ -438,9 +598,33 @@ int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out) {
     return LBM_OK;
 }
 
+int lbm_set_kernel_timing(lbm_ctx *ctx, int32_t enable) {
+    if (!ctx) return LBM_ERR_BAD_ARG;
+    ctx->timing = enable != 0;
+    ctx->ev_used = 0;
+    return LBM_OK;
+}
+
+int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t *cells_per_launch) {
+    if (!ctx || !total_ms || !launches || !cells_per_launch) return LBM_ERR_BAD_ARG;
+    double tot = 0.0;
+    for (size_t e = 0; e + 1 < ctx->ev_used; e += 2) {
+        float ms = 0.0f;
+        CK(cudaEventSynchronize(ctx->ev[e + 1]), "event sync");
+        CK(cudaEventElapsedTime(&ms, ctx->ev[e], ctx->ev[e + 1]), "event time");
+        tot += ms;
+    }
+    *total_ms = tot;
+    *launches = (int64_t)(ctx->ev_used / 2);
+    *cells_per_launch = ctx->timed_cells;
+    return LBM_OK;
+}
+
 int lbm_destroy(lbm_ctx *ctx) {
     if (!ctx) return LBM_ERR_BAD_ARG;
+    for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
     for (void *p : ctx->owned) cudaFree(p);
+    release_slot(ctx->slot);
     delete ctx;
     return LBM_OK;
 }

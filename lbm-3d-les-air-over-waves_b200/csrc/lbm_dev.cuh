@@ -20,6 +20,22 @@
 
 namespace lbm {
 
+// Solver constants of every live context, for device code that is not
+// inlined into a kernel (the near-wall paths).  Inlined code reads the
+// copy passed by value in the kernel arguments instead.
+#define LBM_MAX_SLOTS 64
+#ifdef LBM_DEVICE_TU
+__constant__ lbm_params c_params[LBM_MAX_SLOTS];
+#endif
+
+// f32 constants of the collision kernels (CODEX.py:3165-3171, 3326-3328),
+// evaluated exactly as Taichi does in f32: c_s2 = f32(1/3),
+// inv_2cs4 = 1/(2*c_s2*c_s2) in f32 arithmetic = 4.4999995,
+// 1/tau_sponge = 1/f32(0.95) in f32 arithmetic.
+#define LBM_CS2 0.333333343267440796f
+#define LBM_INV_2CS4 4.49999952316284180f
+#define LBM_OM_SPONGE 1.05263161659240723f
+
 // ---------------------------------------------------------------- lattice
 // D3Q19 in the order of lbm_lattice.py:3-43, as constexpr functions so that
 // unrolled loops fold them into immediates.
@@ -114,10 +130,10 @@ template <> struct Store<LBM_STORE_BF16S> {
 // ------------------------------------------------------------- domain view
 struct Dom {
     int nx, ny, nz;
-    size_t n;   // cells
+    size_t n;   // cells (< 2^31)
     size_t a;   // columns
-    LBM_DEV size_t cell(int k, int j, int i) const { return ((size_t)k * ny + j) * nx + i; }
-    LBM_DEV size_t col(int j, int i) const { return (size_t)j * nx + i; }
+    LBM_DEV int cell(int k, int j, int i) const { return (k * ny + j) * nx + i; }
+    LBM_DEV int col(int j, int i) const { return j * nx + i; }
 };
 
 // 2-D bed state of one step

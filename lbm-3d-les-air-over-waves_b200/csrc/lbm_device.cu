@@ -1,0 +1,952 @@
+// lbm_device.cu - every kernel of the B200 D3Q19 step engine and its
+// launcher (one translation unit, so the constant-slot parameter copies
+// c_params[] exist once).
+//
+// Kernel map (reference kernel -> here):
+//   update_wave_bed_and_velocities           k_bed + k_hmax (2-D)
+//   compute_phi / build_lattice_open         recomputed per cell (lbm_geom.cuh)
+//   update_bed_populations + macro_step +
+//   compute_LES + collide_*                  k_collide<IN=0> (from the post-stream state)
+//   stream + x walls + open BCs, then the
+//   next step's condition + macro + LES +
+//   collide                                  k_collide<IN=1> (air path, one pass per step)
+//   stream + x walls + open BCs (+ water
+//   post-stream macro_step)                  k_stream
+//   velocity stencil of compute_LES          k_prepass (u of every cell)
+//   compute_free_surface_column_flux         k_column_flux
+//   advect_free_surface_height               k_advect
+//   refill_new_free_surface_cells            k_refill
+//   init_constants ... init_fields           k_init_* (setup)
+#define LBM_DEVICE_TU
+#include <cuda_runtime.h>
+
+#include "lbm_launch.h"
+#include "lbm_stages.cuh"
+#include "lbm_tile.cuh"
+
+namespace lbm {
+
+cudaError_t upload_params(int slot, const lbm_params &P) {
+    return cudaMemcpyToSymbol(c_params, &P, sizeof(lbm_params), (size_t)slot * sizeof(lbm_params),
+                              cudaMemcpyHostToDevice);
+}
+
+static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// 3-D launch of the general kernels: block (32, 8), grid (ceil(nx/32),
+// ceil(ny/8), planes), blockIdx.z walking the launch's z ranges
+__device__ __forceinline__ bool cell_xyz(const StepArgs &A, int &i, int &j, int &k, int &c) {
+    const Dom &D = A.D;
+    i = blockIdx.x * blockDim.x + threadIdx.x;
+    j = blockIdx.y * blockDim.y + threadIdx.y;
+    int bz = blockIdx.z;
+    if (bz < A.zcnt[0]) k = A.zlo[0] + bz;
+    else if (bz < A.zcnt[0] + A.zcnt[1]) k = A.zlo[1] + (bz - A.zcnt[0]);
+    else k = A.zlo[2] + (bz - A.zcnt[0] - A.zcnt[1]);
+    if (i >= D.nx || j >= D.ny) return false;
+    c = (k * D.ny + j) * D.nx + i;
+    return true;
+}
+static inline dim3 grid3(const StepArgs &A) {
+    return dim3((A.D.nx + 31) / 32, (A.D.ny + 7) / 8, A.zcnt[0] + A.zcnt[1] + A.zcnt[2]);
+}
+static const dim3 kBlock3(32, 8, 1);
+
+__device__ __forceinline__ void cell_of(const Dom &D, int c, int &k, int &j, int &i) {
+    k = c / (int)D.a;
+    int r = c - k * (int)D.a;
+    j = r / D.nx;
+    i = r - j * D.nx;
+}
+
+// ------------------------------------------------- free-surface heights
+// solitary_surface_height_at_x, CODEX.py:1165-1181
+__device__ __forceinline__ float solitary_h(const lbm_params &P, const Dom &D, float xp, float t) {
+    float Lx = (float)D.nx * P.dx;
+    float h0 = P.fs_depth_m;
+    float ks = sqrtf((float)(3.0 * (double)P.solitary_amp_m) / (4.0f * h0 * h0 * h0));
+    float center = P.solitary_x0_m + P.solitary_dir_cel * t;
+    float xrel = xp - center;
+    if (!P.x_solid) {
+        if (xrel > 0.5f * Lx) xrel -= Lx;
+        if (xrel < -0.5f * Lx) xrel += Lx;
+    }
+    float arg = ks * xrel;
+    float ep = lbm_expf(arg), em = lbm_expf(-arg);
+    float sech = 2.0f / (ep + em);
+    return P.fs_base_m + P.solitary_amp_m * sech * sech;
+}
+// gaussian_surface_height_at_x, CODEX.py:1184-1194
+__device__ __forceinline__ float gaussian_h(const lbm_params &P, const Dom &D, float xp) {
+    float Lx = (float)D.nx * P.dx;
+    float xrel = xp - P.gaussian_center_x_m;
+    if (!P.x_solid) {
+        if (xrel > 0.5f * Lx) xrel -= Lx;
+        if (xrel < -0.5f * Lx) xrel += Lx;
+    }
+    float arg = xrel / P.gaussian_sigma_m;
+    return P.fs_base_m + P.gaussian_amp_m * lbm_expf(-0.5f * arg * arg);
+}
+
+// ------------------------------------------------------------- bed (2-D)
+// update_wave_bed_and_velocities, CODEX.py:1082-1162, harmonics generalised
+__global__ void k_bed(lbm_params P, Dom D, const float *__restrict__ h_prev, float *h, float *uw, float *vw,
+                      float *ww, const float *__restrict__ piecewise, float t) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (int)D.a) return;
+    int i = a % D.nx;
+    const bool moving = P.bed_profile == LBM_BED_MOVING_SINE;
+    float a1 = 0.0f, a2 = 0.0f;
+    if (moving) {
+        if (t < P.bed_ramp_time) {
+            float s = smooth01(t / P.bed_ramp_time);
+            a1 = P.bed_amp1 * s;
+            a2 = P.bed_amp2 * s;
+        } else {
+            a1 = P.bed_amp1;
+            a2 = P.bed_amp2;
+        }
+    }
+    float x0 = (float)i * P.dx;
+    float hl = h_prev[a];
+    float eta1 = 0.0f, eta2 = 0.0f, eta = 0.0f, ph1 = 0.0f, ph2 = 0.0f;
+    if (moving) {
+        float xph1 = x0 - P.bed_c1 * t;
+        float xph2 = x0 - P.bed_c2 * t;
+        ph1 = P.bed_k1 * xph1;
+        ph2 = P.bed_k2 * xph2;
+        eta1 = a1 * lbm_sinf(ph1);
+        eta2 = a2 * lbm_sinf(ph2);
+        eta = eta1 + eta2;
+    }
+    float bh = P.bed_offset_m + eta;
+    if (P.bed_profile == LBM_BED_PIECEWISE) bh = piecewise[i];
+    h[a] = bh;
+    float us = 0.0f, vs = 0.0f, ws = 0.0f;
+    if (moving) {
+        float ex1 = a1 * P.bed_k1 * lbm_cosf(ph1);
+        float ex2 = a2 * P.bed_k2 * lbm_cosf(ph2);
+        float eta_x = ex1 + ex2;
+        float eta_y = 0.0f;
+        float eta_t = (bh - hl) / P.dt_phys_f;
+        if (P.bed_orbital_velocity) us = P.bed_c1 * eta1 / (P.bed_h0 + eta1) + P.bed_c2 * eta2 / (P.bed_h0 + eta2);
+        ws = eta_t + us * eta_x + vs * eta_y;
+    }
+    uw[a] = us / P.vel_scale;
+    vw[a] = vs / P.vel_scale;
+    ww[a] = ws / P.vel_scale;
+}
+
+// max of the bed over the 3x3 column neighbourhood (periodic): the support
+// of every link-endpoint sample of the column
+__global__ void k_hmax(Dom D, const float *__restrict__ h, float *hmax) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (int)D.a) return;
+    int j = a / D.nx, i = a - j * D.nx;
+    float m = -3.4e38f;
+    for (int dj = -1; dj <= 1; ++dj)
+        for (int di = -1; di <= 1; ++di) {
+            int jj = (j + dj + D.ny) % D.ny, ii = (i + di + D.nx) % D.nx;
+            m = fmaxf(m, h[D.col(jj, ii)]);
+        }
+    hmax[a] = m;
+}
+
+// ------------------------------------------------------- step kernels
+template <int S>
+__device__ __forceinline__ void load_cell(const StepArgs &A, int c, float f[19]) {
+    const typename Store<S>::T *src = (const typename Store<S>::T *)A.fsrc;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[q] = Store<S>::ld(src, (size_t)q * A.D.n + (size_t)c, q, A.P.rho0);
+}
+template <int S>
+__device__ __forceinline__ void store_cell(const StepArgs &A, int c, const float f[19]) {
+    typename Store<S>::T *dst = (typename Store<S>::T *)A.fdst;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) Store<S>::st(dst, (size_t)q * A.D.n + (size_t)c, f[q], q, A.P.rho0);
+}
+
+// Populations entering the collide step, then the condition and macro
+// stages on the collide step's geometry.  IN = 0: from the stored
+// post-stream state; IN = 1: stream + BC of the previous step from its
+// post-collision state.  Cells away from every wall and boundary take the
+// plain gather; the general path handles the rest.
+template <int S, int IN>
+__device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, int i, float f[19], bool &fast_c,
+                                      bool &open, int &type, float &gbf, float &r, float &vx, float &vy, float &vz) {
+    const lbm_params &P = A.P;
+    const bool water = P.fs_mode != LBM_FS_NONE;
+    if (cell_fast(A, IN == 1, true, k, j, i)) {
+        if (IN == 0) load_cell<S>(A, c, f);
+        else stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
+        fast_c = true;
+        open = true;
+        type = LBM_FS_LIQUID;
+        gbf = 0.0f;
+        macro(P, A.D, f, k, false, type, gbf, r, vx, vy, vz);
+        return;
+    }
+    if (IN == 0) {
+        load_cell<S>(A, c, f);
+    } else {
+        GeoLinks Ls;
+        Geo gs = geo_cell(P, A.slot, A.D, A.bed_s, k, j, i, Ls, true, P.use_link_wall_velocity && P.include_bed);
+        int cut = 0, fscut = 0, bridge = 0;
+        stream_bc<S>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
+    }
+    GeoLinks Lc;
+    Geo gc = geo_cell(P, A.slot, A.D, A.bed_c, k, j, i, Lc, true, P.use_link_wall_velocity && P.include_bed);
+    fast_c = gc.fast;
+    open = (gc.lo & 1u) != 0u;
+    type = LBM_FS_LIQUID;
+    float fill = 1.0f;
+    gbf = 0.0f;
+    if (water) {
+        fs_state(A, c, k, j, i, open, type, fill);
+        gbf = gbf_of(P, k, open, type);
+    }
+    condition(P, A.D, A.bed_c, gc, Lc, k, j, i, f);
+    macro(P, A.D, f, k, water, type, gbf, r, vx, vy, vz);
+}
+
+template <int S, int IN>
+__global__ void __launch_bounds__(256, 2) k_prepass(StepArgs A) {
+    int i, j, k, c;
+    if (!cell_xyz(A, i, j, k, c)) return;
+    float f[19], r, vx, vy, vz, gbf;
+    int type;
+    bool fast_c, open;
+    front<S, IN>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
+    A.u_out[c] = vx;
+    A.u_out[A.D.n + c] = vy;
+    A.u_out[2 * A.D.n + c] = vz;
+}
+
+template <int S, int IN>
+__global__ void __launch_bounds__(256, 2) k_collide(StepArgs A) {
+    int i, j, k, c;
+    if (!cell_xyz(A, i, j, k, c)) return;
+    float f[19], r, vx, vy, vz, gbf;
+    int type;
+    bool fast_c, open;
+    front<S, IN>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
+    const lbm_params &P = A.P;
+    const bool water = P.fs_mode != LBM_FS_NONE;
+    const bool gas = water && type == LBM_FS_GAS;
+    if (A.flags & F_WRITE_MACRO) {
+        A.rho[c] = r; A.ux[c] = vx; A.uy[c] = vy; A.uz[c] = vz;
+    }
+    if (!(r == r) || fabsf(r) > 3.0e38f) atomicOr(A.status, 1u);
+    float om;
+    if (P.use_les) {
+        if (open && !gas) {
+            om = les_omega(A, k, j, i, c, vx, vy, vz);
+            if ((A.flags & F_WRITE_ALL_OMEGA) || !fast_c) A.omega[c] = om;
+        } else {
+            om = A.omega[c];
+        }
+    } else {
+        om = P.omega0;
+    }
+    collide(A, c, k, !open, water, gas, gbf, r, vx, vy, vz, om, f);
+    store_cell<S>(A, c, f);
+}
+
+template <int S>
+__global__ void __launch_bounds__(256, 2) k_stream(StepArgs A) {
+    int i, j, k, c;
+    int cut = 0, fscut = 0, bridge = 0;
+    if (cell_xyz(A, i, j, k, c)) {
+        float f[19];
+        if (cell_fast(A, true, false, k, j, i)) {
+            stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
+            store_cell<S>(A, c, f);
+        } else {
+            GeoLinks Ls;
+            Geo gs = geo_cell(A.P, A.slot, A.D, A.bed_s, k, j, i, Ls, true, A.P.use_link_wall_velocity && A.P.include_bed);
+            stream_bc<S>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
+            store_cell<S>(A, c, f);
+            if (A.P.fs_mode != LBM_FS_NONE) {
+                // post-stream macro_step of the water path, CODEX.py:3897
+                int type;
+                float fill;
+                bool open = (gs.lo & 1u) != 0u;
+                fs_state(A, c, k, j, i, open, type, fill);
+                float gbf = gbf_of(A.P, k, open, type);
+                float r, vx, vy, vz;
+                macro(A.P, A.D, f, k, true, type, gbf, r, vx, vy, vz);
+                A.rho[c] = r; A.ux[c] = vx; A.uy[c] = vy; A.uz[c] = vz;
+            }
+        }
+    }
+    if (A.flags & F_COUNT) {
+        unsigned m = __activemask();
+        int s0 = __reduce_add_sync(m, cut), s1 = __reduce_add_sync(m, fscut), s2 = __reduce_add_sync(m, bridge);
+        if ((threadIdx.x & 31) == 0) {
+            if (s0) atomicAdd(A.counters + 0, s0);
+            if (s1) atomicAdd(A.counters + 1, s1);
+            if (s2) atomicAdd(A.counters + 2, s2);
+        }
+    }
+}
+
+// -------------------------------------------- height-function free surface
+// compute_free_surface_column_flux, CODEX.py:2376-2388 (sequential in k)
+__global__ void k_column_flux(StepArgs A, float *qx_out, float *qy_out) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (int)A.D.a) return;
+    const Dom &D = A.D;
+    int j = a / D.nx, i = a - j * D.nx;
+    float h = A.fs_h[a];
+    float qx = 0.0f, qy = 0.0f;
+    for (int k = 0; k < D.nz; ++k) {
+        int c = D.cell(k, j, i);
+        int type;
+        float fill;
+        classify_height(A.P, h, k, true, type, fill);
+        if (type == LBM_FS_GAS) continue;
+        if (!cell_open(A.P, A.slot, D, A.bed_s, k, j, i)) continue;
+        qx += fill * A.ux[c] * A.P.vel_scale * A.P.dx;
+        qy += fill * A.uy[c] * A.P.vel_scale * A.P.dx;
+    }
+    qx_out[a] = qx;
+    qy_out[a] = qy;
+}
+
+// advect_free_surface_height, CODEX.py:2391-2429
+__global__ void k_advect(lbm_params P, Dom D, const float *__restrict__ bed_h, const float *__restrict__ qx,
+                         const float *__restrict__ qy, const float *h_in, float *h_out, float *h_last, float t) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (int)D.a) return;
+    int j = a / D.nx, i = a - j * D.nx;
+    float Lz = (float)D.nz * P.dx;
+    float ho = h_in[a];
+    float h = ho;
+    if (P.fs_mode == LBM_FS_PRESCRIBED_SOLITARY) {
+        float x = ((float)i + 0.5f) * P.dx;
+        h = solitary_h(P, D, x, t);
+    } else if (P.fs_mode == LBM_FS_HEIGHT_KINEMATIC) {
+        float dqdx;
+        if (P.x_solid) {
+            float fl = 0.0f, fr = 0.0f;
+            if (i > 0) fl = 0.5f * (qx[D.col(j, i - 1)] + qx[a]);
+            if (i < D.nx - 1) fr = 0.5f * (qx[a] + qx[D.col(j, i + 1)]);
+            dqdx = (fr - fl) / P.dx;
+        } else {
+            int ip = (i + 1) % D.nx, im = (i - 1 + D.nx) % D.nx;
+            dqdx = (qx[D.col(j, ip)] - qx[D.col(j, im)]) * P.half_inv_dx;
+        }
+        int jp = (j + 1) % D.ny, jm = (j - 1 + D.ny) % D.ny;
+        float dqdy = (qy[D.col(jp, i)] - qy[D.col(jm, i)]) * P.half_inv_dx;
+        float dhdt = -(dqdx + dqdy);
+        h = ho + P.dt_phys_f * dhdt;
+        float mn = bed_h[a] + 0.5f * P.dx;
+        float mx = Lz - 0.5f * P.dx;
+        if (h < mn) h = mn;
+        if (h > mx) h = mx;
+    }
+    h_last[a] = ho;
+    h_out[a] = h;
+}
+
+// refill_new_free_surface_cells, CODEX.py:2163-2316.  Height path: the
+// before/after states come from h_last/h; VOF path: from the stored
+// type_prev/type (F_VOF_STATE).
+template <int S>
+__global__ void __launch_bounds__(256) k_refill(StepArgs A, const int8_t *type_prev_v, int *count) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int did = 0;
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    const bool vofm = (A.flags & F_VOF_STATE) != 0;
+    if (c < (int)D.n) {
+        int k, j, i;
+        cell_of(D, c, k, j, i);
+        int tp, tn;
+        float fl;
+        if (vofm) {
+            tp = type_prev_v[c];
+            tn = A.fs_type[c];
+        } else {
+            classify_height(P, A.fs_h_last[D.col(j, i)], k, true, tp, fl);
+            classify_height(P, A.fs_h[D.col(j, i)], k, true, tn, fl);
+        }
+        bool cand = tp == LBM_FS_GAS && tn != LBM_FS_GAS;
+        if (cand && cell_open(P, A.slot, D, A.bed_s, k, j, i)) {
+            typename Store<S>::T *fb = (typename Store<S>::T *)A.fdst;
+            float ws = 0.0f, fws = 0.0f, ra = 0.0f, xa = 0.0f, ya = 0.0f, za = 0.0f;
+            float fra = 0.0f, fxa = 0.0f, fya = 0.0f, fza = 0.0f;
+            float na[19], nfa[19];
+#pragma unroll
+            for (int q = 0; q < 19; ++q) { na[q] = 0.0f; nfa[q] = 0.0f; }
+#pragma unroll
+            for (int qn = 1; qn < 19; ++qn) {
+                int nir = i + cxq(qn);
+                int nj = pymod(j + cyq(qn) + D.ny, D.ny);
+                int nk = k + czq(qn);
+                int ni = nir;
+                bool valid = true;
+                if (!P.x_solid) ni = pymod(nir + D.nx, D.nx);
+                else if (nir < 0 || nir >= D.nx) valid = false;
+                if (nk < 0 || nk >= D.nz) valid = false;
+                if (!valid) continue;
+                int nb = D.cell(nk, nj, ni);
+                int ntp, ntn;
+                float nfl;
+                if (vofm) {
+                    ntp = type_prev_v[nb];
+                    ntn = A.fs_type[nb];
+                    nfl = A.fs_fill[nb];
+                } else {
+                    float dummy;
+                    classify_height(P, A.fs_h_last[D.col(nj, ni)], nk, true, ntp, dummy);
+                    classify_height(P, A.fs_h[D.col(nj, ni)], nk, true, ntn, nfl);
+                }
+                if (!(ntp != LBM_FS_GAS && ntn != LBM_FS_GAS)) continue;
+                if (!cell_open(P, A.slot, D, A.bed_s, nk, nj, ni)) continue;
+                float wn = wq(qn);
+                float rn = A.rho[nb], uxn = A.ux[nb], uyn = A.uy[nb], uzn = A.uz[nb];
+                fws += wn;
+                fra += wn * rn; fxa += wn * uxn; fya += wn * uyn; fza += wn * uzn;
+                float lw = wn * nfl;
+                ws += lw;
+                ra += lw * rn; xa += lw * uxn; ya += lw * uyn; za += lw * uzn;
+                if (P.fs_refill == LBM_REFILL_NONEQ) {
+                    float u2n = usq(uxn, uyn, uzn);
+#pragma unroll
+                    for (int qq = 0; qq < 19; ++qq) {
+                        float fe = 0.0f;
+                        switch (qq) {
+#define FQ(Q) case Q: fe = feq<Q>(rn, uxn, uyn, uzn, u2n); break;
+                            FQ(0) FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13)
+                            FQ(14) FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+                        }
+                        float fneq = Store<S>::ld_rw(fb, (size_t)qq * D.n + nb, qq, P.rho0) - fe;
+                        na[qq] += lw * fneq;
+                        nfa[qq] += wn * fneq;
+                    }
+                }
+            }
+            float rr = P.rho0;
+            if (!vofm) {
+                // gravity fraction of the state at the start of the step
+                float gbf = gbf_of(P, k, true, tp);
+                rr = fs_density_cell(P, A.fs_h[D.col(j, i)], k, gbf);
+            }
+            float urx = P.u_current_lb, ury = 0.0f, urz = 0.0f;
+            if (ws > 0.0f) {
+                float iw = 1.0f / ws;
+                if (vofm) rr = ra * iw;
+                urx = xa * iw; ury = ya * iw; urz = za * iw;
+            } else if (fws > 0.0f) {
+                float iw = 1.0f / fws;
+                if (vofm) rr = fra * iw;
+                urx = fxa * iw; ury = fya * iw; urz = fza * iw;
+            } else if (vofm) {
+                rr = P.rho0;
+            }
+            float fr[19];
+            float rp = 0.0f;
+            float u2r = usq(urx, ury, urz);
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                float v = 0.0f;
+                switch (q) {
+#define FQ(Q) case Q: v = feq<Q>(rr, urx, ury, urz, u2r); break;
+                    FQ(0) FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+                    FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+                }
+                if (P.fs_refill == LBM_REFILL_NONEQ) {
+                    if (ws > 0.0f) v += na[q] / ws;
+                    else if (fws > 0.0f) v += nfa[q] / fws;
+                } else if (P.fs_refill == LBM_REFILL_DIRECTIONAL) {
+                    int sir = i - cxq(q);
+                    int si = sir;
+                    int sj = pymod(j - cyq(q) + D.ny, D.ny);
+                    int sk = k - czq(q);
+                    bool sv = true;
+                    if (!P.x_solid) si = pymod(sir + D.nx, D.nx);
+                    else if (sir < 0 || sir >= D.nx) sv = false;
+                    if (sk < 0 || sk >= D.nz) sv = false;
+                    if (sv) {
+                        int s = D.cell(sk, sj, si);
+                        int stp, stn;
+                        float sfl;
+                        if (vofm) {
+                            stp = type_prev_v[s];
+                            stn = A.fs_type[s];
+                        } else {
+                            classify_height(P, A.fs_h_last[D.col(sj, si)], sk, true, stp, sfl);
+                            classify_height(P, A.fs_h[D.col(sj, si)], sk, true, stn, sfl);
+                        }
+                        if (stp != LBM_FS_GAS && stn != LBM_FS_GAS && cell_open(P, A.slot, D, A.bed_s, sk, sj, si))
+                            v = Store<S>::ld_rw(fb, (size_t)q * D.n + s, q, P.rho0);
+                    }
+                }
+                fr[q] = v;
+                rp += v;
+            }
+            if (P.fs_refill == LBM_REFILL_DIRECTIONAL) {
+                float scale = 1.0f;
+                if (rp > 1.0e-8f) scale = rr / rp;
+                rp = 0.0f;
+                float mx = 0.0f, my = 0.0f, mz = 0.0f;
+#pragma unroll
+                for (int q = 0; q < 19; ++q) {
+                    float fv = fr[q] * scale;
+                    fr[q] = fv;
+                    rp += fv;
+                    if (cxq(q) > 0) mx += fv; else if (cxq(q) < 0) mx += -fv;
+                    if (cyq(q) > 0) my += fv; else if (cyq(q) < 0) my += -fv;
+                    if (czq(q) > 0) mz += fv; else if (czq(q) < 0) mz += -fv;
+                }
+                A.rho[c] = rp;
+                if (rp > 1.0e-8f) { A.ux[c] = mx / rp; A.uy[c] = my / rp; A.uz[c] = mz / rp; }
+                else { A.ux[c] = urx; A.uy[c] = ury; A.uz[c] = urz; }
+            } else {
+                A.rho[c] = rr; A.ux[c] = urx; A.uy[c] = ury; A.uz[c] = urz;
+            }
+            // a refilled cell is never a source for another refilled cell
+            // (sources need type_prev != GAS), so writing in place is safe
+            store_cell<S>(A, c, fr);
+            did = 1;
+        }
+    }
+    unsigned m = __activemask();
+    int s = __reduce_add_sync(m, did);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(count, s);
+}
+
+// free-surface fields of the height path after a call: fill and type from
+// the new height, type_prev from the height before advection
+__global__ void k_height_types(StepArgs A, float *fill, int8_t *type, int8_t *type_prev) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int)A.D.n) return;
+    int k, j, i;
+    cell_of(A.D, c, k, j, i);
+    bool open = cell_open(A.P, A.slot, A.D, A.bed_s, k, j, i);
+    int tp, tn;
+    float fp, fn;
+    classify_height(A.P, A.fs_h_last[A.D.col(j, i)], k, open, tp, fp);
+    classify_height(A.P, A.fs_h[A.D.col(j, i)], k, open, tn, fn);
+    fill[c] = fn;
+    type[c] = (int8_t)tn;
+    type_prev[c] = (int8_t)tp;
+}
+
+// ======================================================== initialisation
+// init_constants, CODEX.py:1022-1080
+__global__ void k_init_constants(InitArgs I) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const Dom &D = I.D;
+    const lbm_params &P = I.P;
+    if (c < (int)D.n) {
+        I.rho[c] = P.rho0; I.ux[c] = 0.0f; I.uy[c] = 0.0f; I.uz[c] = 0.0f;
+        I.omega[c] = P.omega0;
+        I.fs_fill[c] = 1.0f;
+        I.fs_type[c] = LBM_FS_LIQUID;
+        I.fs_type_prev[c] = LBM_FS_LIQUID;
+        I.fs_mass[c] = P.rho0;
+        I.fs_mass_excess[c] = 0.0f;
+        I.fs_excess_dir[c] = 0;
+    }
+    if (c < (int)D.a) {
+        int i = c % D.nx;
+        float bh = P.bed_offset_m;
+        if (P.bed_profile == LBM_BED_PIECEWISE) bh = I.piecewise[i];
+        I.water_h[c] = bh;
+        I.water_h_last[c] = bh;
+        I.u_wave[c] = 0.0f; I.v_wave[c] = 0.0f; I.w_wave[c] = 0.0f;
+        I.fs_h[c] = P.fs_base_m;
+        I.fs_h_last[c] = P.fs_base_m;
+        I.fs_flux_x[c] = 0.0f;
+        I.fs_flux_y[c] = 0.0f;
+    }
+}
+
+// initialize_free_surface_height, CODEX.py:1197-1207
+__global__ void k_fs_height_init(InitArgs I) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (int)I.D.a) return;
+    const lbm_params &P = I.P;
+    int i = a % I.D.nx;
+    float x = ((float)i + 0.5f) * P.dx;
+    float h = P.fs_base_m;
+    if (P.fs_initial == LBM_FSINIT_SOLITARY || P.fs_mode == LBM_FS_PRESCRIBED_SOLITARY) h = solitary_h(P, I.D, x, 0.0f);
+    else if (P.fs_initial == LBM_FSINIT_GAUSSIAN) h = gaussian_h(P, I.D, x);
+    I.fs_h[a] = h;
+    I.fs_h_last[a] = h;
+}
+
+// classify_free_surface_cells, CODEX.py:1210-1235 (stored form)
+__global__ void k_classify_store(InitArgs I) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int)I.D.n) return;
+    int k, j, i;
+    cell_of(I.D, c, k, j, i);
+    int8_t old = I.fs_type[c];
+    float fl = 1.0f;
+    int ct = LBM_FS_LIQUID;
+    if (I.P.fs_mode != LBM_FS_NONE) {
+        bool open = cell_open(I.P, I.slot, I.D, I.bed, k, j, i);
+        classify_height(I.P, I.fs_h[I.D.col(j, i)], k, open, ct, fl);
+    }
+    I.fs_fill[c] = fl;
+    I.fs_type_prev[c] = old;
+    I.fs_type[c] = (int8_t)ct;
+}
+
+__device__ __forceinline__ float overlap(float cmin, float cmax, float bmin, float bmax) {
+    float lo = cmin;
+    if (bmin > lo) lo = bmin;
+    float hi = cmax;
+    if (bmax < hi) hi = bmax;
+    float ov = hi - lo;
+    if (ov < 0.0f) ov = 0.0f;
+    return ov / (cmax - cmin);
+}
+// apply_vof_initial_disconnected_shape, CODEX.py:1253-1286
+__global__ void k_vof_block(InitArgs I) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int)I.D.n) return;
+    const lbm_params &P = I.P;
+    int k, j, i;
+    cell_of(I.D, c, k, j, i);
+    if (!cell_open(P, I.slot, I.D, I.bed, k, j, i)) return;
+    float dx = P.dx;
+    float x0 = (float)i * dx, x1 = x0 + dx, y0 = (float)j * dx, y1 = y0 + dx, z0 = (float)k * dx, z1 = z0 + dx;
+    float fx = overlap(x0, x1, P.vof_block_xmin, P.vof_block_xmax);
+    float fy = overlap(y0, y1, P.vof_block_ymin, P.vof_block_ymax);
+    float fz = overlap(z0, z1, P.vof_block_zmin, P.vof_block_zmax);
+    float bf = fx * fy * fz;
+    if (bf > 1e-4f) {
+        int8_t old = I.fs_type[c];
+        float fl = I.fs_fill[c];
+        if (bf > fl) fl = bf;
+        int ct = LBM_FS_INTERFACE;
+        if (fl >= (float)(1.0 - 1e-4)) { fl = 1.0f; ct = LBM_FS_LIQUID; }
+        I.fs_fill[c] = fl;
+        I.fs_type_prev[c] = old;
+        I.fs_type[c] = (int8_t)ct;
+    }
+}
+
+// log-law inlet profile of init_fields, CODEX.py:2718-2742 (sequential)
+__global__ void k_profile(InitArgs I) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const lbm_params &P = I.P;
+    const int nz = I.D.nz;
+    float B = 5.0f;
+    float u_tau = P.u_tau_init;
+    float nu_lbm = P.nu_lbm_init;
+    for (int k = 0; k < nz; ++k) {
+        float y = (float)k;
+        float yp = y * u_tau / nu_lbm;
+        if (yp <= 1.0f) yp = 1.0f;
+        I.u_inlet_profile[k] = P.inv_kappa * lbm_logf(yp) + B;
+    }
+    float top = I.u_inlet_profile[nz - 1];
+    if (top == 0.0f) top = 1.0f;
+    for (int k = 0; k < nz; ++k) I.u_inlet_profile[k] = I.u_inlet_profile[k] / top * P.u_top_lb;
+}
+
+// velocity and equilibrium populations of init_fields, CODEX.py:2744-2825
+template <int S>
+__global__ void k_init_fields(InitArgs I) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int)I.D.n) return;
+    const lbm_params &P = I.P;
+    const Dom &D = I.D;
+    int k, j, i;
+    cell_of(D, c, k, j, i);
+    GeoLinks L;
+    Geo g = geo_cell(P, I.slot, D, I.bed, k, j, i, L);
+    bool open = (g.lo & 1u) != 0u;
+    const bool water = P.fs_mode != LBM_FS_NONE;
+    float r = I.rho[c], vx, vy, vz;
+    if (P.init_velocity_mode == LBM_INITVEL_UNIFORM) {
+        float amp = P.init_noise_amp;
+        vx = P.init_u0x + I.noise[c] * amp;
+        vy = P.init_u0y + I.noise[D.n + c] * amp;
+        vz = P.init_u0z + I.noise[2 * D.n + c] * amp;
+    } else {
+        float kick = I.noise[c];
+        vx = I.u_inlet_profile[k] * (1.0f + kick * P.ti_kick);
+        vy = 0.0f;
+        vz = 0.0f;
+    }
+    int type = water ? I.fs_type[c] : LBM_FS_LIQUID;
+    if (water) {
+        if (type == LBM_FS_GAS) {
+            r = P.rho0; vx = 0.0f; vy = 0.0f; vz = 0.0f;
+        } else {
+            r = I.rho_initial[c];
+            vx = P.u_current_lb;
+            if (P.fs_initial == LBM_FSINIT_SOLITARY && P.solitary_velocity_mode != LBM_SOLVEL_NONE) {
+                float eta_fs = I.fs_h[D.col(j, i)] - P.fs_base_m;
+                if (eta_fs < 0.0f) eta_fs = 0.0f;
+                float hd = P.fs_depth_m;
+                float usol = P.solitary_direction * P.solitary_celerity * eta_fs / (hd + eta_fs);
+                vx += usol / P.vel_scale;
+                if (P.solitary_velocity_mode == LBM_SOLVEL_SHALLOW_DIVFREE) {
+                    float xc = ((float)i + 0.5f) * P.dx;
+                    float Lxs = (float)D.nx * P.dx;
+                    float xrel = xc - P.solitary_x0_m;
+                    if (!P.x_solid) {
+                        if (xrel > 0.5f * Lxs) xrel -= Lxs;
+                        if (xrel < -0.5f * Lxs) xrel += Lxs;
+                    }
+                    float arg = P.solitary_kappa_inv * xrel;
+                    float ep = lbm_expf(arg), em = lbm_expf(-arg);
+                    float den = ep + em;
+                    float sech = 2.0f / den;
+                    float th = (ep - em) / den;
+                    float eta_x = -2.0f * P.solitary_amp_m * P.solitary_kappa_inv * sech * sech * th;
+                    float dudx = P.solitary_direction * P.solitary_celerity * hd * eta_x / ((hd + eta_fs) * (hd + eta_fs));
+                    float zc = ((float)k + 0.5f) * P.dx;
+                    float zrel = zc - I.bed.h[D.col(j, i)];
+                    if (zrel < 0.0f) zrel = 0.0f;
+                    vz += (-zrel * dudx) / P.vel_scale;
+                }
+            }
+        }
+    }
+    if (!open) {
+        vx = 0.0f; vy = 0.0f; vz = 0.0f;
+        r = P.rho0;
+        if (L.wt[0] == LBM_WALL_BED) {
+            int a = D.col(j, i);
+            vx = I.bed.uw[a]; vy = I.bed.vw[a]; vz = I.bed.ww[a];
+        }
+    }
+    I.rho[c] = r; I.ux[c] = vx; I.uy[c] = vy; I.uz[c] = vz;
+    float ez = vz;
+    if (water && open && type != LBM_FS_GAS) ez += 0.5f * g_local(P, gbf_of(P, k, open, type));
+    float u2 = usq(vx, vy, ez);
+    typename Store<S>::T *dst = (typename Store<S>::T *)I.f_cur;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        float v = 0.0f;
+        switch (q) {
+#define FQ(Q) case Q: v = feq<Q>(r, vx, vy, ez, u2); break;
+            FQ(0) FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14) FQ(15)
+            FQ(16) FQ(17) FQ(18)
+#undef FQ
+        }
+        Store<S>::st(dst, (size_t)q * D.n + c, v, q, P.rho0);
+    }
+}
+
+// initialize_free_surface_boundary_populations, CODEX.py:2828-2875:
+// f_other = f_cur, plus the atmospheric projection when enabled
+template <int S>
+__global__ void k_fs_boundary_pop(InitArgs I) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int)I.D.n) return;
+    const lbm_params &P = I.P;
+    const Dom &D = I.D;
+    typedef typename Store<S>::T ST;
+    const ST *fo = (const ST *)I.f_cur;
+    ST *fn = (ST *)I.f_other;
+    float f[19], out[19];
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        f[q] = Store<S>::ld_rw(fo, (size_t)q * D.n + c, q, P.rho0);
+        out[q] = f[q];
+    }
+    if (P.fs_mode != LBM_FS_NONE && P.init_fs_populations) {
+        int k, j, i;
+        cell_of(D, c, k, j, i);
+        bool open = cell_open(P, I.slot, D, I.bed, k, j, i);
+        int type = I.fs_type[c];
+        if (open && type != LBM_FS_GAS) {
+            float vx = I.ux[c], vy = I.uy[c], vz = I.uz[c];
+            float u2 = usq(vx, vy, vz);
+            float gbf = gbf_of(P, k, open, type);
+            float hcol = I.fs_h[D.col(j, i)];
+#pragma unroll
+            for (int q = 1; q < 19; ++q) {
+                int sir = i - cxq(q);
+                int si = sir;
+                bool sf = true;
+                if (!P.x_solid) si = pymod(sir + D.nx, D.nx);
+                else if (sir < 0) { si = 0; sf = false; }
+                else if (sir >= D.nx) { si = D.nx - 1; sf = false; }
+                int sj = pymod(j - cyq(q) + D.ny, D.ny);
+                int sk = k - czq(q);
+                bool src_gas = false;
+                if (!sf) src_gas = false;
+                else if (sk >= D.nz) src_gas = true;
+                else if (sk >= 0) {
+                    int s = D.cell(sk, sj, si);
+                    if (I.fs_type[s] == LBM_FS_GAS && cell_open(P, I.slot, D, I.bed, sk, sj, si)) src_gas = true;
+                }
+                if (src_gas) {
+                    float rfs = P.rho0;
+                    if (P.use_hydrostatic_balanced_pressure || P.fs_boundary == LBM_FSB_HYDROSTATIC)
+                        rfs = fs_density_link(P, hcol, k, czq(q), gbf);
+                    switch (q) {
+#define FQ(Q) case Q: out[q] = feq<Q>(rfs, vx, vy, vz, u2) + feq<oppq(Q)>(rfs, vx, vy, vz, u2) - f[oppq(Q)]; break;
+                        FQ(1) FQ(2) FQ(3) FQ(4) FQ(5) FQ(6) FQ(7) FQ(8) FQ(9) FQ(10) FQ(11) FQ(12) FQ(13) FQ(14)
+                        FQ(15) FQ(16) FQ(17) FQ(18)
+#undef FQ
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 19; ++q) Store<S>::st(fn, (size_t)q * D.n + c, out[q], q, P.rho0);
+}
+
+// initialize_vof_mass_from_fill, CODEX.py:1289-1302
+__global__ void k_vof_mass_init(InitArgs I) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int)I.D.n) return;
+    int k, j, i;
+    cell_of(I.D, c, k, j, i);
+    bool open = cell_open(I.P, I.slot, I.D, I.bed, k, j, i);
+    if (open && I.fs_type[c] != LBM_FS_GAS) {
+        I.fs_mass[c] = I.fs_fill[c] * I.rho[c];
+    } else {
+        I.fs_mass[c] = 0.0f;
+        I.fs_fill[c] = 0.0f;
+        I.fs_type[c] = LBM_FS_GAS;
+    }
+    I.fs_type_prev[c] = I.fs_type[c];
+    I.fs_mass_excess[c] = 0.0f;
+    I.fs_excess_dir[c] = 0;
+}
+
+// ------------------------------------------------------------------ export
+__global__ void k_export(InitArgs I, ExportArgs E) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int)I.D.n) return;
+    const lbm_params &P = I.P;
+    const Dom &D = I.D;
+    int k, j, i;
+    cell_of(D, c, k, j, i);
+    GeoLinks L;
+    Geo g = geo_cell(P, I.slot, D, I.bed, k, j, i, L, false);
+    bool open = (g.lo & 1u) != 0u;
+    if (E.phi) E.phi[c] = phi_cell(P, D, I.bed.h, k, j, i);
+    if (E.obstacle) E.obstacle[c] = open ? 0 : 1;
+    if (E.near_obstacle) E.near_obstacle[c] = g.near ? 1 : 0;
+    for (int q = 0; q < 19; ++q) {
+        if (E.lattice_open) E.lattice_open[(size_t)q * D.n + c] = (int8_t)((g.lo >> q) & 1u);
+        if (E.lattice_open_frac) E.lattice_open_frac[(size_t)q * D.n + c] = L.lf[q];
+        if (E.lattice_wall_type) E.lattice_wall_type[(size_t)q * D.n + c] = (int8_t)L.wt[q];
+    }
+    // update_pressure_reference_fields ran at the start of the last step
+    // (types of that moment = fs_type_prev now) or, before any step, at init
+    int tp = E.types_are_prev ? I.fs_type_prev[c] : I.fs_type[c];
+    if (E.prh) E.prh[c] = prh_of(P, k, open, tp);
+    if (E.gbf) E.gbf[c] = gbf_of(P, k, open, tp);
+}
+
+// ---------------------------------------------------------------- launchers
+void launch_bed(const lbm_params &P, const Dom &D, const float *h_prev, float *h, float *hmax, float *uw, float *vw,
+                float *ww, const float *piecewise, float t, cudaStream_t st) {
+    k_bed<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, h_prev, h, uw, vw, ww, piecewise, t);
+    k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax);
+}
+void launch_hmax(const Dom &D, const float *h, float *hmax, cudaStream_t st) {
+    k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax);
+}
+
+template <int S>
+static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) {
+    dim3 g = grid3(A);
+    const int ni = A.zi1 - A.zi0 + 1;
+    const bool tile_kernel = which >= KER_TILE_CANON;
+    if (!tile_kernel && g.z == 0) return;
+    if (tile_kernel && (ni <= 0 || A.chunk <= 0)) return;
+    const unsigned tz = tile_kernel ? (unsigned)((ni + A.chunk - 1) / A.chunk) : 0u;
+    dim3 gt(A.D.nx / LBM_TILE, A.D.ny / LBM_TILE, tz);
+    dim3 gs(A.D.nx / LBM_TILE, A.D.ny / LBM_TILE, tile_kernel ? (unsigned)ni : 0u);
+    const bool les = A.P.use_les != 0;
+    switch (which) {
+        case KER_PREPASS_CANON: k_prepass<S, 0><<<g, kBlock3, 0, st>>>(A); break;
+        case KER_PREPASS_FUSED: k_prepass<S, 1><<<g, kBlock3, 0, st>>>(A); break;
+        case KER_COLLIDE_CANON: k_collide<S, 0><<<g, kBlock3, 0, st>>>(A); break;
+        case KER_COLLIDE_FUSED: k_collide<S, 1><<<g, kBlock3, 0, st>>>(A); break;
+        case KER_STREAM: k_stream<S><<<g, kBlock3, 0, st>>>(A); break;
+        case KER_TILE_CANON:
+            if (les) k_tile<S, 0, true><<<gt, 256, 0, st>>>(A);
+            else k_tile<S, 0, false><<<gt, 256, 0, st>>>(A);
+            break;
+        case KER_TILE_FUSED:
+            if (les) k_tile<S, 1, true><<<gt, 256, 0, st>>>(A);
+            else k_tile<S, 1, false><<<gt, 256, 0, st>>>(A);
+            break;
+        case KER_STREAM_INTERIOR: k_stream_interior<S><<<gs, 256, 0, st>>>(A); break;
+        default: break;
+    }
+}
+void launch_step_kernel(int which, const StepArgs &A, cudaStream_t st) {
+    switch (A.P.pop_storage) {
+        case LBM_STORE_F16S: launch_step_kernel_s<LBM_STORE_F16S>(which, A, st); break;
+        case LBM_STORE_BF16S: launch_step_kernel_s<LBM_STORE_BF16S>(which, A, st); break;
+        default: launch_step_kernel_s<LBM_STORE_F32>(which, A, st); break;
+    }
+}
+void launch_column_flux(const StepArgs &A, float *qx, float *qy, cudaStream_t st) {
+    k_column_flux<<<blocks_for(A.D.a, 128), 128, 0, st>>>(A, qx, qy);
+}
+void launch_advect(const lbm_params &P, const Dom &D, const float *bed_h, const float *qx, const float *qy,
+                   const float *h_in, float *h_out, float *h_last, float t, cudaStream_t st) {
+    k_advect<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, bed_h, qx, qy, h_in, h_out, h_last, t);
+}
+void launch_refill(const StepArgs &A, const int8_t *type_prev, int *count, cudaStream_t st) {
+    unsigned g = blocks_for(A.D.n, 256);
+    switch (A.P.pop_storage) {
+        case LBM_STORE_F16S: k_refill<LBM_STORE_F16S><<<g, 256, 0, st>>>(A, type_prev, count); break;
+        case LBM_STORE_BF16S: k_refill<LBM_STORE_BF16S><<<g, 256, 0, st>>>(A, type_prev, count); break;
+        default: k_refill<LBM_STORE_F32><<<g, 256, 0, st>>>(A, type_prev, count); break;
+    }
+}
+void launch_height_types(const StepArgs &A, float *fill, int8_t *type, int8_t *type_prev, cudaStream_t st) {
+    k_height_types<<<blocks_for(A.D.n, 256), 256, 0, st>>>(A, fill, type, type_prev);
+}
+
+void launch_init_constants(const InitArgs &I, cudaStream_t st) {
+    size_t n = I.D.n > I.D.a ? I.D.n : I.D.a;
+    k_init_constants<<<blocks_for(n, 256), 256, 0, st>>>(I);
+}
+void launch_fs_height_init(const InitArgs &I, cudaStream_t st) {
+    k_fs_height_init<<<blocks_for(I.D.a, 256), 256, 0, st>>>(I);
+}
+void launch_classify_store(const InitArgs &I, cudaStream_t st) {
+    k_classify_store<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I);
+}
+void launch_vof_block(const InitArgs &I, cudaStream_t st) {
+    k_vof_block<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I);
+}
+void launch_init_fields(const InitArgs &I, cudaStream_t st) {
+    k_profile<<<1, 1, 0, st>>>(I);
+    unsigned g = blocks_for(I.D.n, 256);
+    switch (I.P.pop_storage) {
+        case LBM_STORE_F16S:
+            k_init_fields<LBM_STORE_F16S><<<g, 256, 0, st>>>(I);
+            k_fs_boundary_pop<LBM_STORE_F16S><<<g, 256, 0, st>>>(I);
+            break;
+        case LBM_STORE_BF16S:
+            k_init_fields<LBM_STORE_BF16S><<<g, 256, 0, st>>>(I);
+            k_fs_boundary_pop<LBM_STORE_BF16S><<<g, 256, 0, st>>>(I);
+            break;
+        default:
+            k_init_fields<LBM_STORE_F32><<<g, 256, 0, st>>>(I);
+            k_fs_boundary_pop<LBM_STORE_F32><<<g, 256, 0, st>>>(I);
+            break;
+    }
+}
+void launch_vof_mass_init(const InitArgs &I, cudaStream_t st) {
+    k_vof_mass_init<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I);
+}
+void launch_export(const InitArgs &I, const ExportArgs &E, cudaStream_t st) {
+    k_export<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I, E);
+}
+
+}  // namespace lbm

@@ -8,6 +8,12 @@
 // every link endpoint is more than half a cell above the bed and outside
 // the cube takes a fast path (all links open, fraction 1): the test is
 // conservative, so the fast and full paths give identical results.
+//
+// Link endpoints x_c + c_q dx/2 take only three x and three y positions per
+// cell, so the full path sets up the periodic bilinear interpolation once
+// per axis position and evaluates the bed (and, when needed, the wall
+// velocity) once per (x, y) endpoint: the same arithmetic as sampling link
+// by link, with a ninth of the divisions.
 #pragma once
 
 #include "lbm_dev.cuh"
@@ -20,34 +26,34 @@ struct Geo {
     bool near;       // near_obstacle
     bool fast;       // all links open with fraction 1 (links below not written)
 };
-// per-link fractions and wall sources; written only for cells off the fast
-// path (the fast path reads neither)
+// per-link fractions and wall sources, and the wall velocity at the nine
+// link endpoints; written only for cells off the fast path (the fast path
+// reads none of it)
 struct GeoLinks {
     float lf[19];
     uint8_t wt[19];
+    float uw[9][3];   // [3*(cx+1) + (cy+1)][component], valid when has_uw
+    bool has_uw;
 };
+__host__ __device__ constexpr int endpoint_index(int q) { return 3 * (cxq(q) + 1) + (cyq(q) + 1); }
 
-// periodic bilinear sampling setup (CODEX.py:665-683, 2570-2588, 941-957)
+// one axis of the periodic bilinear sampling setup (CODEX.py:665-683,
+// 2570-2588, 941-957): position -> (i0, i1, fraction)
+LBM_DEV void bl_axis(float p, float dx, int n, int &i0, int &i1, float &f) {
+    float L = (float)n * dx, Nf = (float)n;
+    float w = p - floorf(p / L) * L;
+    float u = w / dx - 0.5f;
+    u = u - floorf(u / Nf) * Nf;
+    i0 = (int)floorf(u);
+    f = u - (float)i0;
+    if (i0 >= n) i0 -= n;
+    if (i0 < 0) i0 += n;
+    i1 = (i0 + 1) % n;
+}
 LBM_DEV void bl_setup(const lbm_params &P, const Dom &D, float xp, float yp, int &i0, int &j0, int &i1, int &j1,
                       float &fx, float &fy) {
-    const float dx = P.dx;
-    float Lx = (float)D.nx * dx, Ly = (float)D.ny * dx, Nxf = (float)D.nx, Nyf = (float)D.ny;
-    float xw = xp - floorf(xp / Lx) * Lx;
-    float yw = yp - floorf(yp / Ly) * Ly;
-    float u = xw / dx - 0.5f;
-    float v = yw / dx - 0.5f;
-    u = u - floorf(u / Nxf) * Nxf;
-    v = v - floorf(v / Nyf) * Nyf;
-    i0 = (int)floorf(u);
-    j0 = (int)floorf(v);
-    fx = u - (float)i0;
-    fy = v - (float)j0;
-    if (i0 >= D.nx) i0 -= D.nx;
-    if (j0 >= D.ny) j0 -= D.ny;
-    if (i0 < 0) i0 += D.nx;
-    if (j0 < 0) j0 += D.ny;
-    i1 = (i0 + 1) % D.nx;
-    j1 = (j0 + 1) % D.ny;
+    bl_axis(xp, P.dx, D.nx, i0, i1, fx);
+    bl_axis(yp, P.dx, D.ny, j0, j1, fy);
 }
 LBM_DEV float bl_sample(const float *a, const Dom &D, int i0, int j0, int i1, int j1, float fx, float fy) {
     float v00 = __ldg(a + D.col(j0, i0)), v10 = __ldg(a + D.col(j0, i1));
@@ -128,7 +134,8 @@ LBM_DEV float phi_cell(const lbm_params &P, const Dom &D, const float *h, int k,
 }
 
 // sample_phi_periodic, CODEX.py:661-707 (phi evaluated on the fly)
-static __device__ __noinline__ float sample_phi(const lbm_params &P, const Dom &D, const float *h, float xp, float yp, float zp) {
+static __device__ __noinline__ float sample_phi(int slot, Dom D, const float *h, float xp, float yp, float zp) {
+    const lbm_params &P = c_params[slot];
     int i0, j0, i1, j1;
     float fx, fy;
     bl_setup(P, D, xp, yp, i0, j0, i1, j1, fx, fy);
@@ -177,14 +184,39 @@ LBM_DEV bool geo_far(const lbm_params &P, const Dom &D, const BedView &B, int k,
     return true;
 }
 
-// build_lattice_open_from_free_surface_periodic for one cell (full path)
-static __device__ __noinline__ Geo geo_slow(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i,
-                                     GeoLinks *L) {
+// build_lattice_open_from_free_surface_periodic for one cell (full path);
+// with want_uw, also the wall velocity at the nine link endpoints
+static __device__ __noinline__ Geo geo_slow(int slot, Dom D, BedView B, int k, int j, int i, GeoLinks *L,
+                                            bool want_uw) {
+    const lbm_params &P = c_params[slot];
     Geo g;
     g.fast = false;
     const float dx = P.dx, hdx = 0.5f * dx;
     float xc = ((float)i + 0.5f) * dx, yc = ((float)j + 0.5f) * dx, zc = ((float)k + 0.5f) * dx;
-    float eta_c = sample_h(P, D, B.h, xc, yc);
+    // bilinear setups of the three endpoint positions per axis
+    int xi0[3], xi1[3], yj0[3], yj1[3];
+    float xf[3], yf[3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        bl_axis(xc + hdx * (float)(s - 1), dx, D.nx, xi0[s], xi1[s], xf[s]);
+        bl_axis(yc + hdx * (float)(s - 1), dx, D.ny, yj0[s], yj1[s], yf[s]);
+    }
+    float eta9[9];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+            eta9[3 * a + b] = bl_sample(B.h, D, xi0[a], yj0[b], xi1[a], yj1[b], xf[a], yf[b]);
+    L->has_uw = want_uw;
+    if (want_uw) {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) {
+                L->uw[3 * a + b][0] = bl_sample(B.uw, D, xi0[a], yj0[b], xi1[a], yj1[b], xf[a], yf[b]);
+                L->uw[3 * a + b][1] = bl_sample(B.vw, D, xi0[a], yj0[b], xi1[a], yj1[b], xf[a], yf[b]);
+                L->uw[3 * a + b][2] = bl_sample(B.ww, D, xi0[a], yj0[b], xi1[a], yj1[b], xf[a], yf[b]);
+            }
+    }
+    float eta_c = eta9[4];
     float gap_c = zc - eta_c;
     float ggc = 1.0e6f;
     int wtc = LBM_WALL_NONE;
@@ -201,11 +233,12 @@ static __device__ __noinline__ Geo geo_slow(const lbm_params &P, const Dom &D, c
     L->lf[0] = frc;
     L->wt[0] = (uint8_t)wtc;
     uint32_t lo = 0u;
+#pragma unroll
     for (int q = 1; q < 19; ++q) {
         float xq = xc + hdx * (float)cxq(q);
         float yq = yc + hdx * (float)cyq(q);
         float zq = zc + hdx * (float)czq(q);
-        float eta = sample_h(P, D, B.h, xq, yq);
+        float eta = eta9[endpoint_index(q)];
         float gap = zq - eta;
         float gg = 1.0e6f;
         int wq_ = LBM_WALL_NONE;
@@ -215,7 +248,7 @@ static __device__ __noinline__ Geo geo_slow(const lbm_params &P, const Dom &D, c
             if (cg < gg) { gg = cg; wq_ = LBM_WALL_CUBE; }
         }
         float sg = gg;
-        if (P.use_phi_open_fraction) sg = sample_phi(P, D, B.h, xq, yq, zq);
+        if (P.use_phi_open_fraction) sg = sample_phi(slot, D, B.h, xq, yq, zq);
         float fr = 0.5f + sg / dx;
         if (fr < 0.0f) fr = 0.0f;
         if (fr > 1.0f) fr = 1.0f;
@@ -242,8 +275,8 @@ static __device__ __noinline__ Geo geo_slow(const lbm_params &P, const Dom &D, c
     return g;
 }
 
-LBM_DEV Geo geo_cell(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i, GeoLinks &L,
-                     bool allow_fast = true) {
+LBM_DEV Geo geo_cell(const lbm_params &P, int slot, const Dom &D, const BedView &B, int k, int j, int i, GeoLinks &L,
+                     bool allow_fast = true, bool want_uw = false) {
     if (allow_fast && geo_far(P, D, B, k, j, i)) {
         Geo g;
         g.lo = 0x7FFFFu;
@@ -252,18 +285,17 @@ LBM_DEV Geo geo_cell(const lbm_params &P, const Dom &D, const BedView &B, int k,
         g.fast = true;
         return g;
     }
-    return geo_slow(P, D, B, k, j, i, &L);
+    return geo_slow(slot, D, B, k, j, i, &L, want_uw);
 }
 
-static __device__ __noinline__ bool cell_open_slow(const lbm_params &P, const Dom &D, const BedView &B, int k, int j,
-                                            int i) {
+static __device__ __noinline__ bool cell_open_slow(int slot, Dom D, BedView B, int k, int j, int i) {
     GeoLinks L;
-    return (geo_slow(P, D, B, k, j, i, &L).lo & 1u) != 0u;
+    return (geo_slow(slot, D, B, k, j, i, &L, false).lo & 1u) != 0u;
 }
 // lattice_open[0] only (cheap when far from walls)
-LBM_DEV bool cell_open(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i) {
+LBM_DEV bool cell_open(const lbm_params &P, int slot, const Dom &D, const BedView &B, int k, int j, int i) {
     if (geo_far(P, D, B, k, j, i)) return true;
-    return cell_open_slow(P, D, B, k, j, i);
+    return cell_open_slow(slot, D, B, k, j, i);
 }
 
 }  // namespace lbm

@@ -1,5 +1,5 @@
-// lbm_launch.h - argument structs and launchers shared by the kernel files
-// and the host API of the B200 D3Q19 step engine.
+// lbm_launch.h - argument structs and launchers shared by the device
+// translation unit (lbm_device.cu) and the host API (lbm_api.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -8,12 +8,47 @@
 
 namespace lbm {
 
-struct StepArgs;
+enum : int {
+    F_WRITE_MACRO = 1,      // store rho/ux/uy/uz of this collide
+    F_WRITE_ALL_OMEGA = 2,  // store omega for every active cell (else near-wall band only)
+    F_COUNT = 4,            // count cut / free-surface / bridge links in stream
+    F_VOF_STATE = 8,        // free-surface state from stored type/fill (else from column height)
+};
 
-enum { KER_PREPASS_CANON = 0, KER_PREPASS_FUSED = 1, KER_COLLIDE_CANON = 2, KER_COLLIDE_FUSED = 3, KER_STREAM = 4 };
+enum {
+    KER_PREPASS_CANON = 0, KER_PREPASS_FUSED = 1, KER_COLLIDE_CANON = 2, KER_COLLIDE_FUSED = 3, KER_STREAM = 4,
+    KER_TILE_CANON = 5, KER_TILE_FUSED = 6, KER_STREAM_INTERIOR = 7
+};
+#define LBM_TILE 16   // interior tile edge (x and y); the tile path needs nx, ny multiples of it
+
+struct StepArgs {
+    lbm_params P;
+    int slot;
+    Dom D;
+    const void *fsrc;  // populations read
+    void *fdst;        // populations written
+    BedView bed_s;     // geometry of the stream stage
+    BedView bed_c;     // geometry of the condition/collide stage
+    float *rho, *ux, *uy, *uz, *omega;
+    const float *u_les;  // [3][n] velocities for the LES stencil
+    float *u_out;        // [3][n] pre-pass output
+    const float *fs_h, *fs_h_last;
+    const float *fs_fill;
+    const int8_t *fs_type;
+    const float *u_inlet_profile;
+    int *counters;       // [0] cut, [1] fs cut, [2] bridge
+    unsigned *status;    // bit 0: non-finite density
+    uint64_t step;       // 1-based step number of the collide stage (RNG key)
+    int flags;
+    // z planes covered by a launch: up to 3 ranges [zlo, zlo + zcnt), grid.z = sum of zcnt
+    int zlo[3], zcnt[3];
+    // interior planes [zi0, zi1] handled by the tile kernel (chunk planes per block)
+    int zi0, zi1, chunk;
+};
 
 struct InitArgs {
     lbm_params P;
+    int slot;
     Dom D;
     BedView bed;
     void *f_cur, *f_other;
@@ -34,35 +69,10 @@ struct ExportArgs {
     float *lattice_open_frac;
     int8_t *lattice_wall_type;
     float *prh, *gbf;
+    int types_are_prev;  // pressure reference from fs_type_prev (after a step) or fs_type (after init)
 };
 
-// solitary_surface_height_at_x, CODEX.py:1165-1181
-LBM_DEV float solitary_h(const lbm_params &P, const Dom &D, float xp, float t) {
-    float Lx = (float)D.nx * P.dx;
-    float h0 = P.fs_depth_m;
-    float ks = sqrtf((float)(3.0 * (double)P.solitary_amp_m) / (4.0f * h0 * h0 * h0));
-    float center = P.solitary_x0_m + P.solitary_dir_cel * t;
-    float xrel = xp - center;
-    if (!P.x_solid) {
-        if (xrel > 0.5f * Lx) xrel -= Lx;
-        if (xrel < -0.5f * Lx) xrel += Lx;
-    }
-    float arg = ks * xrel;
-    float ep = lbm_expf(arg), em = lbm_expf(-arg);
-    float sech = 2.0f / (ep + em);
-    return P.fs_base_m + P.solitary_amp_m * sech * sech;
-}
-// gaussian_surface_height_at_x, CODEX.py:1184-1194
-LBM_DEV float gaussian_h(const lbm_params &P, const Dom &D, float xp) {
-    float Lx = (float)D.nx * P.dx;
-    float xrel = xp - P.gaussian_center_x_m;
-    if (!P.x_solid) {
-        if (xrel > 0.5f * Lx) xrel -= Lx;
-        if (xrel < -0.5f * Lx) xrel += Lx;
-    }
-    float arg = xrel / P.gaussian_sigma_m;
-    return P.fs_base_m + P.gaussian_amp_m * lbm_expf(-0.5f * arg * arg);
-}
+cudaError_t upload_params(int slot, const lbm_params &P);
 
 void launch_bed(const lbm_params &P, const Dom &D, const float *h_prev, float *h, float *hmax, float *uw, float *vw,
                 float *ww, const float *piecewise, float t, cudaStream_t st);

@@ -1,0 +1,234 @@
+// lbm_tile.cuh - the interior step kernel: one pass per step over the
+// planes that are provably away from every wall.
+//
+// A block owns a 16x16 column tile and marches up a chunk of z planes.  For
+// every plane it gathers the post-stream populations of its 256 cells
+// (pull from the previous step's post-collision state, or the stored
+// post-stream state for the first step of a call), takes the moments, and
+// publishes the velocity of the cells and of the 64-cell ring around the
+// tile (recomputed by 64 threads) to shared memory.  Once plane p is
+// published, plane p-1 has its full 7-point velocity stencil: LES, then
+// collision, then the post-collision populations go to HBM.  So each step
+// reads every population once and writes it once (plus the ring re-reads,
+// served by L2); the velocity never round-trips through HBM.
+//
+// Preconditions, established by the host: air mode without free surface,
+// periodic x without the x fringe, nx and ny multiples of 16, and every
+// plane in [zi0, zi1] far from the bed (the bed amplitude bounds the bed
+// height) so no link there is cut and no cell below is solid.  The kernel
+// re-checks the geometry of its cells and sets status bit 1 if a
+// precondition fails.
+#pragma once
+
+#include "lbm_stages.cuh"
+
+namespace lbm {
+
+// compute_LES without the wall model (the cell below is fluid by the
+// preconditions), from a 7-point stencil
+LBM_DEV float les_interior(const lbm_params &P, float uxp, float uxm, float uyp, float uym, float uzp, float uzm,
+                           float vxp, float vxm, float vyp, float vym, float vzp, float vzm, float wxp, float wxm,
+                           float wyp, float wym, float wzp, float wzm) {
+    float du_dx = 0.5f * (uxp - uxm);
+    float du_dy = 0.5f * (uyp - uym);
+    float du_dz = 0.5f * (uzp - uzm);
+    float dv_dx = 0.5f * (vxp - vxm);
+    float dv_dy = 0.5f * (vyp - vym);
+    float dv_dz = 0.5f * (vzp - vzm);
+    float dw_dx = 0.5f * (wxp - wxm);
+    float dw_dy = 0.5f * (wyp - wym);
+    float dw_dz = 0.5f * (wzp - wzm);
+    float Sxx = du_dx, Syy = dv_dy, Szz = dw_dz;
+    float Sxy = 0.5f * (du_dy + dv_dx);
+    float Sxz = 0.5f * (du_dz + dw_dx);
+    float Syz = 0.5f * (dv_dz + dw_dy);
+    float Sc = (Sxx * Sxx + Syy * Syy + Szz * Szz + 2.0f * (Sxy * Sxy + Sxz * Sxz + Syz * Syz));
+    float Smag = sqrtf(2.0f * Sc + 1e-6f);
+    float nu_t = P.cs_delta_sq * Smag;
+    if (nu_t > P.nu_t_max) nu_t = P.nu_t_max;
+    float nu_eff = P.nu0 + nu_t;
+    float tau_eff = 0.5f + 3.0f * nu_eff;
+    if (tau_eff > 2.0f) tau_eff = 2.0f;
+    return 1.0f / tau_eff;
+}
+
+// populations entering the collide step for an interior cell
+template <int S, int IN>
+LBM_DEV void interior_front(const StepArgs &A, int k, int j, int i, float f[19]) {
+    const int c = A.D.cell(k, j, i);
+    if (IN == 0) {
+        const typename Store<S>::T *src = (const typename Store<S>::T *)A.fsrc;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) f[q] = Store<S>::ld(src, (size_t)q * A.D.n + (size_t)c, q, A.P.rho0);
+    } else {
+        stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
+    }
+}
+
+__constant__ int c_tile_cx[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0};
+__constant__ int c_tile_cy[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, -1, 1};
+__constant__ int c_tile_cz[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+
+// ring cell r (0..63) around a 16x16 tile: rows below/above, columns left/right
+LBM_DEV void ring_cell(int r, int &rx, int &ry) {
+    if (r < 16) { rx = r; ry = -1; }
+    else if (r < 32) { rx = r - 16; ry = LBM_TILE; }
+    else if (r < 48) { rx = -1; ry = r - 32; }
+    else { rx = LBM_TILE; ry = r - 48; }
+}
+
+// populations entering the collide step for the 64 ring cells of plane p,
+// gathered by all 256 threads (item m = (q, r) with q = m / 64) into
+// ringf[q][r]
+template <int S, int IN>
+LBM_DEV void ring_gather(const StepArgs &A, int p, int t, float (*ringf)[64]) {
+    const Dom &D = A.D;
+    const typename Store<S>::T *src = (const typename Store<S>::T *)A.fsrc;
+#pragma unroll
+    for (int u = 0; u < 5; ++u) {
+        const int m = t + 256 * u;
+        if (m < 64 * 19) {
+            const int r = m & 63, q = m >> 6;
+            int rx, ry;
+            ring_cell(r, rx, ry);
+            int si = blockIdx.x * LBM_TILE + rx, sj = blockIdx.y * LBM_TILE + ry, sk = p;
+            if (IN == 1) {
+                si -= c_tile_cx[q];
+                sj -= c_tile_cy[q];
+                sk -= c_tile_cz[q];
+            }
+            si = (si + 2 * D.nx) % D.nx;
+            sj = (sj + 2 * D.ny) % D.ny;
+            const size_t idx = (size_t)q * D.n + (size_t)D.cell(sk, sj, si);
+            float v;
+            if (S == LBM_STORE_F32) v = __ldg((const float *)src + idx);
+            else v = Store<S>::ld(src, idx, q, A.P.rho0);
+            ringf[q][r] = v;
+        }
+    }
+}
+
+LBM_DEV void check_far(const StepArgs &A, bool stream_geo, int k, int j, int i) {
+    bool ok = geo_far(A.P, A.D, A.bed_c, k, j, i);
+    if (stream_geo) ok = ok && geo_far(A.P, A.D, A.bed_s, k, j, i);
+    if (!ok) atomicOr(A.status, 2u);
+}
+
+template <int S, int IN, bool LES>
+__global__ void __launch_bounds__(256, 2) k_tile(StepArgs A) {
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    const int i = blockIdx.x * LBM_TILE + tx, j = blockIdx.y * LBM_TILE + ty;
+    const int z0 = A.zi0 + blockIdx.z * A.chunk;
+    const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
+    __shared__ float su[3][3][LBM_TILE + 2][LBM_TILE + 2];  // [plane slot][component][y][x]
+    __shared__ float ringf[LES ? 19 : 1][64];               // ring populations of the current plane
+
+    // ring cell whose moments this thread takes (threads 0..63)
+    int rx = 0, ry = 0;
+    ring_cell(t & 63, rx, ry);
+    const int ri = (blockIdx.x * LBM_TILE + rx + D.nx) % D.nx;
+    const int rj = (blockIdx.y * LBM_TILE + ry + D.ny) % D.ny;
+    const bool ring = LES && t < 64;
+
+    float fp[19];
+    float rp = 0.0f, vxp = 0.0f, vyp = 0.0f, vzp = 0.0f;
+    const size_t n = D.n;
+    for (int p = z0 - 1; p <= z1; ++p) {
+        const int sl = p % 3;
+        const bool interior = p >= A.zi0 && p <= A.zi1;
+        float fc[19];
+        float r = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
+        if (interior) {
+            interior_front<S, IN>(A, p, j, i, fc);
+            macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
+            if (LES) {
+                su[sl][0][ty + 1][tx + 1] = vx;
+                su[sl][1][ty + 1][tx + 1] = vy;
+                su[sl][2][ty + 1][tx + 1] = vz;
+            }
+            if (LES) ring_gather<S, IN>(A, p, t, ringf);
+        } else if (LES) {
+            // plane handled by the general kernels: velocity from their pre-pass
+            const int c = D.cell(p, j, i);
+            su[sl][0][ty + 1][tx + 1] = __ldg(A.u_les + c);
+            su[sl][1][ty + 1][tx + 1] = __ldg(A.u_les + n + c);
+            su[sl][2][ty + 1][tx + 1] = __ldg(A.u_les + 2 * n + c);
+            if (ring) {
+                const int cr = D.cell(p, rj, ri);
+                su[sl][0][ry + 1][rx + 1] = __ldg(A.u_les + cr);
+                su[sl][1][ry + 1][rx + 1] = __ldg(A.u_les + n + cr);
+                su[sl][2][ry + 1][rx + 1] = __ldg(A.u_les + 2 * n + cr);
+            }
+        }
+        if (LES) __syncthreads();
+        if (LES && interior) {
+            // moments of the ring cells from the cooperatively gathered populations
+            if (ring) {
+                float fr[19], rr, a, b, d;
+#pragma unroll
+                for (int q = 0; q < 19; ++q) fr[q] = ringf[q][t];
+                macro(P, D, fr, p, false, LBM_FS_LIQUID, 0.0f, rr, a, b, d);
+                su[sl][0][ry + 1][rx + 1] = a;
+                su[sl][1][ry + 1][rx + 1] = b;
+                su[sl][2][ry + 1][rx + 1] = d;
+            }
+            __syncthreads();
+        }
+        const int k = p - 1;
+        if (k >= z0 && k < z1) {
+            const int c = D.cell(k, j, i);
+            check_far(A, IN == 1, k, j, i);
+            if (k == A.zi0) check_far(A, IN == 1, k - 1, j, i);
+            float om = P.omega0;
+            if (LES) {
+                const int sm = (p + 1) % 3, s0 = (p + 2) % 3, sp = sl;  // planes k-1, k, k+1
+                const int y = ty + 1, x = tx + 1;
+                om = les_interior(P, su[s0][0][y][x + 1], su[s0][0][y][x - 1], su[s0][0][y + 1][x],
+                                  su[s0][0][y - 1][x], su[sp][0][y][x], su[sm][0][y][x], su[s0][1][y][x + 1],
+                                  su[s0][1][y][x - 1], su[s0][1][y + 1][x], su[s0][1][y - 1][x], su[sp][1][y][x],
+                                  su[sm][1][y][x], su[s0][2][y][x + 1], su[s0][2][y][x - 1], su[s0][2][y + 1][x],
+                                  su[s0][2][y - 1][x], su[sp][2][y][x], su[sm][2][y][x]);
+                if (A.flags & F_WRITE_ALL_OMEGA) A.omega[c] = om;
+                if (k == A.zi0 || k == A.zi1) {
+                    // velocity of the interior planes next to the general ones,
+                    // for the general kernels' stencils
+                    A.u_out[c] = vxp;
+                    A.u_out[n + c] = vyp;
+                    A.u_out[2 * n + c] = vzp;
+                }
+            }
+            if (A.flags & F_WRITE_MACRO) {
+                A.rho[c] = rp; A.ux[c] = vxp; A.uy[c] = vyp; A.uz[c] = vzp;
+            }
+            if (!(rp == rp) || fabsf(rp) > 3.0e38f) atomicOr(A.status, 1u);
+            collide(A, c, k, false, false, false, 0.0f, rp, vxp, vyp, vzp, om, fp);
+            typename Store<S>::T *dst = (typename Store<S>::T *)A.fdst;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) Store<S>::st(dst, (size_t)q * n + (size_t)c, fp[q], q, P.rho0);
+        }
+#pragma unroll
+        for (int q = 0; q < 19; ++q) fp[q] = fc[q];
+        rp = r; vxp = vx; vyp = vy; vzp = vz;
+        if (LES) __syncthreads();
+    }
+}
+
+// stream only (the last pass of a call) for interior cells
+template <int S>
+__global__ void __launch_bounds__(256) k_stream_interior(StepArgs A) {
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    const int i = blockIdx.x * LBM_TILE + tx, j = blockIdx.y * LBM_TILE + ty;
+    const int k = A.zi0 + blockIdx.z;
+    if (k > A.zi1) return;
+    const int c = A.D.cell(k, j, i);
+    check_far(A, true, k, j, i);
+    float f[19];
+    stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
+    typename Store<S>::T *dst = (typename Store<S>::T *)A.fdst;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) Store<S>::st(dst, (size_t)q * A.D.n + (size_t)c, f[q], q, A.P.rho0);
+}
+
+}  // namespace lbm

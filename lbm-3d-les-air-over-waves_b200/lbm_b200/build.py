@@ -20,8 +20,8 @@ REPO = os.path.dirname(SRC_ROOT)
 INCLUDE = os.path.join(REPO, "include")
 OUT_DIR = os.path.join(PKG, "_native")
 LIB = os.path.join(OUT_DIR, "liblbm_b200.so")
-SOURCES = ["lbm_api.cu", "lbm_kernels.cu", "lbm_init.cu"]
-HEADERS = ["lbm_dev.cuh", "lbm_geom.cuh", "lbm_step.cuh", "lbm_launch.h"]
+SOURCES = ["lbm_api.cu", "lbm_device.cu"]
+HEADERS = ["lbm_dev.cuh", "lbm_geom.cuh", "lbm_stages.cuh", "lbm_tile.cuh", "lbm_launch.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

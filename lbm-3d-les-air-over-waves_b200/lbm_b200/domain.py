@@ -79,6 +79,15 @@ class Domain:
         self._check(self.lib.lbm_read_counters(self.ctx, C.byref(c)), "lbm_read_counters")
         return c.as_dict()
 
+    def set_kernel_timing(self, enable: bool):
+        self._check(self.lib.lbm_set_kernel_timing(self.ctx, 1 if enable else 0), "lbm_set_kernel_timing")
+
+    def kernel_timing(self):
+        """(summed ms, launches, cells per launch) of the interior kernel."""
+        ms, n, cells = C.c_double(), C.c_int64(), C.c_int64()
+        self._check(self.lib.lbm_kernel_timing(self.ctx, C.byref(ms), C.byref(n), C.byref(cells)), "lbm_kernel_timing")
+        return ms.value, n.value, cells.value
+
     def synchronize(self):
         self.stream.synchronize()
 

@@ -747,6 +747,14 @@ int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out) {
     *out = ctx->impl->ctr;
     return LBM_OK;
 }
+int lbm_set_kernel_timing(lbm_ctx *ctx, int32_t) { return ctx ? LBM_OK : LBM_ERR_BAD_ARG; }
+int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t *cells) {
+    if (!ctx || !total_ms || !launches || !cells) return LBM_ERR_BAD_ARG;
+    *total_ms = 0.0;
+    *launches = 0;
+    *cells = 0;
+    return LBM_OK;
+}
 int lbm_destroy(lbm_ctx *ctx) {
     if (!ctx) return LBM_ERR_BAD_ARG;
     delete ctx->impl;

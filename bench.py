@@ -1,0 +1,395 @@
+"""Throughput of the D3Q19 air-over-moving-wave step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step is one time step of the whole domain: bed update, pull-stream with
+the moving-wall link fractions, Smagorinsky LES and regularized collision.
+Workload: air over a moving sinusoidal bed, 512x256x256 cells, FP32
+populations (A-B buffers, 5.1 GB, larger than L2), regularized collision,
+Smagorinsky Cs = 0.16, tau0 = 0.52, bed z = 8 + 4 sin(2 pi (x - 0.02 t)/64),
+seeded synthetic initial state.  Steps run through the public C ABI in
+chunks of 100 (the reference's health-report cadence).
+
+Printed (rank 0, one JSON line): MLUPS over all ranks (replicas, weak
+scaling; device time, max over ranks), the roofline of the dominant kernel
+(the interior one-pass step kernel, timed live with CUDA events on its
+stream), the end-to-end figure through the API with host buffers, the SM
+clocks sampled during the timed region, and the CPU oracle timed on a
+bounded sample of the same workload.
+
+--impl reference times the reference algorithm's CPU implementation (the
+FP32 C++ restatement in oracle/, OpenMP over all host cores) on a bounded
+sample of the same workload; the reference itself needs Taichi, which is
+not installed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.join(ROOT, "lbm-3d-les-air-over-waves_b200")
+TESTS = os.path.join(ROOT, "tests")
+if PKG_ROOT not in sys.path:
+    sys.path.insert(0, PKG_ROOT)
+
+NX, NY, NZ = 512, 256, 256
+CHUNK = 100                 # steps per API call (health-report cadence of the reference loop)
+B_ALG = 152                 # algorithmic bytes per cell update, FP32 populations read + written once
+WORKLOAD = "air over moving wave, LES regularized, 512x256x256, FP32 populations"
+METRIC, UNIT = "MLUPS", "MLUPS"
+# bounded CPU samples: periodic sub-blocks of the workload with its full height
+# (same bed, same vertical structure), largest first
+CPU_SAMPLES = [(128, 64, 256), (64, 64, 256), (64, 32, 256), (64, 16, 256)]
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_tile_air_interior.md")
+
+
+def workload_env(nx=NX, ny=NY, nz=NZ, seed=12345):
+    from lbm_b200.config import air_wave_env
+
+    return air_wave_env(nx, ny, nz, storage="f32", seed=seed)
+
+
+def base_config():
+    return {
+        "workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "cells": NX * NY * NZ, "collision": "regularized",
+        "les": "smagorinsky Cs=0.16", "tau0": 0.52, "storage": "f32", "steps_per_call": CHUNK,
+        "l2": "inputs larger than L2 (5.1 GB of populations, A-B)", "parallelism": "replicas",
+    }
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        import tempfile
+
+        fd, self.path = tempfile.mkstemp(prefix="lbm_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        # samples under load: the upper half of the clock readings, the
+        # timed region being most of the sampling window
+        load = sorted(sm)[len(sm) // 4:] if sm else []
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU oracle
+def oracle_sample_rate(budget_s: float, max_steps: int):
+    """Time the CPU oracle on a bounded sample; returns (MLUPS, sample text)."""
+    if TESTS not in sys.path:
+        sys.path.insert(0, TESTS)
+    from oracle_runner import OracleSim
+
+    shape = CPU_SAMPLES[0]
+    sim = OracleSim(workload_env(*shape))
+    t0 = time.perf_counter()
+    sim.step(1)
+    t1 = time.perf_counter() - t0
+    n = shape[0] * shape[1] * shape[2]
+    steps = max(1, min(max_steps, int(budget_s / max(t1, 1e-3))))
+    t0 = time.perf_counter()
+    sim.step(steps)
+    dt = time.perf_counter() - t0
+    sim.close()
+    rate = n * steps / dt / 1e6
+    sample = (f"{shape[0]}x{shape[1]}x{shape[2]} periodic sub-block of the workload (full height, same bed), "
+              f"{steps} steps after 1 warm-up step, {dt:.1f} s")
+    return rate, sample
+
+
+def reference_arm(args):
+    """Reference CPU implementation of the path on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    if TESTS not in sys.path:
+        sys.path.insert(0, TESTS)
+    from oracle_runner import OracleSim
+
+    cores = host_cores()
+    K, W = args.steps, max(args.warmup, 0)
+    budget = 150.0   # seconds for the whole run
+    # pick the largest sample whose K + W steps fit the budget, from one probe step
+    probe_shape = CPU_SAMPLES[0]
+    sim = OracleSim(workload_env(*probe_shape))
+    t0 = time.perf_counter()
+    sim.step(1)
+    t_probe = time.perf_counter() - t0
+    per_cell = t_probe / (probe_shape[0] * probe_shape[1] * probe_shape[2])
+    shape = CPU_SAMPLES[-1]
+    for s in CPU_SAMPLES:
+        if per_cell * s[0] * s[1] * s[2] * (K + W) <= budget:
+            shape = s
+            break
+    if shape != probe_shape:
+        sim.close()
+        sim = OracleSim(workload_env(*shape))
+    n = shape[0] * shape[1] * shape[2]
+    if W:
+        sim.step(W)
+    t0 = time.perf_counter()
+    sim.step(K)
+    dt = time.perf_counter() - t0
+    sim.close()
+    value = n * K / dt / 1e6
+    sample = f"{shape[0]}x{shape[1]}x{shape[2]} periodic sub-block of the workload (full height, same bed) per step"
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": K, "warmup": W,
+        "ms_per_step": dt / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": base_config(), "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's own solver needs Taichi (absent); timed: the FP32 C++ restatement of its "
+                "kernels (oracle), OpenMP over all host cores",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def profile_traffic_per_cell():
+    """DRAM bytes per cell update of the interior kernel from the committed
+    ncu summary (a line 'dram_bytes_per_cell: X')."""
+    try:
+        with open(PROFILE_SUMMARY) as fh:
+            for line in fh:
+                m = re.match(r"\s*[-*]?\s*dram_bytes_per_cell:\s*([0-9.]+)", line)
+                if m:
+                    return float(m.group(1))
+    except OSError:
+        pass
+    return None
+
+
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def run_steps(dom, k):
+    done = 0
+    while done < k:
+        n = min(CHUNK, k - done)
+        dom.step(n)
+        done += n
+
+
+def ours(args):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(vals):
+        t = torch.tensor(vals, dtype=torch.float64, device=dev)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.tolist()
+
+    from lbm_b200.domain import Domain
+
+    K, W = args.steps, max(args.warmup, 3)
+    env = workload_env(seed=12345 + rank)
+    dom = Domain(env, device=dev, with_diag=False)
+    lib = dom.lib
+    s = dom.stream
+    ncell = NX * NY * NZ
+
+    # ---- warm-up
+    run_steps(dom, W)
+    dom.synchronize()
+    if dom.counters()["status_flags"]:
+        raise SystemExit("non-finite state after warm-up")
+
+    # ---- device-resident throughput (+ live timing of the dominant kernel)
+    dom.set_kernel_timing(True)
+    l0 = C.c_int64()
+    lib.lbm_launch_count(C.byref(l0))
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    run_steps(dom, K)
+    e1.record(s)
+    e1.synchronize()
+    torch.cuda.synchronize(dev)
+    barrier()
+    clk = clocks.stop()
+    l1 = C.c_int64()
+    lib.lbm_launch_count(C.byref(l1))
+    ms = e0.elapsed_time(e1)
+    k_ms, k_launches, k_cells = dom.kernel_timing()
+    dom.set_kernel_timing(False)
+    if dom.counters()["status_flags"]:
+        raise SystemExit("non-finite state in the timed region")
+
+    # ---- end to end through the API with host buffers: the reference's main
+    # loop (initial state from the host, steps in chunks of 100, the health
+    # report's velocity fields read back after every chunk)
+    noise_h = torch.from_numpy(np.ascontiguousarray(dom.arrays["init_noise"].cpu().numpy())).pin_memory()
+    rho_h = torch.from_numpy(np.ascontiguousarray(dom.arrays["rho_initial"].cpu().numpy())).pin_memory()
+    vel_h = [torch.empty(ncell, dtype=torch.float32).pin_memory() for _ in range(3)]
+    h2d = noise_h.numel() * 4 + rho_h.numel() * 4
+    d2h = 0
+    barrier()
+    torch.cuda.synchronize(dev)
+    x0, x1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    x0.record(s)
+    with torch.cuda.stream(s):
+        dom.arrays["init_noise"].copy_(noise_h, non_blocking=True)
+        dom.arrays["rho_initial"].copy_(rho_h, non_blocking=True)
+    sp = C.c_void_p(s.cuda_stream)
+    dom._check(lib.lbm_init_geometry(dom.ctx, sp), "lbm_init_geometry")
+    dom._check(lib.lbm_init_fields(dom.ctx, sp), "lbm_init_fields")
+    done = 0
+    while done < K:
+        n = min(CHUNK, K - done)
+        dom.step(n)
+        done += n
+        with torch.cuda.stream(s):
+            for h, name in zip(vel_h, ("ux", "uy", "uz")):
+                h.copy_(dom.arrays[name].view(-1), non_blocking=True)
+        d2h += 3 * ncell * 4
+        ctr = dom.counters()     # health report: status and link counters
+        if ctr["status_flags"]:
+            raise SystemExit("non-finite state in the end-to-end run")
+    x1.record(s)
+    x1.synchronize()
+    barrier()
+    e2e_ms = x0.elapsed_time(x1)
+
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms])
+    value = world * ncell * K / (ms * 1e-3) / 1e6
+    e2e = world * ncell * K / (e2e_ms * 1e-3) / 1e6
+
+    out = None
+    if rank == 0:
+        peak, peak_kind = measured_hbm_peak()
+        roof = None
+        if k_launches > 0 and k_ms > 0:
+            per_launch_s = k_ms / k_launches * 1e-3
+            achieved = B_ALG * k_cells / per_launch_s / 1e9
+            tpc = profile_traffic_per_cell()
+            roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": (tpc * k_cells) if tpc else None, "peak_kind": peak_kind,
+                    "kernel": "k_tile (interior one-pass stream+LES+collide)", "cells_per_launch": k_cells,
+                    "bytes_per_cell": B_ALG, "launch_ms": per_launch_s * 1e3,
+                    "step_frac": B_ALG * value * 1e6 / world / (peak * 1e9)}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            rate, sample = oracle_sample_rate(budget_s=12.0, max_steps=20)
+            cpu = {"value": rate, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": sample}
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": base_config(),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K},
+            "gpu_launches": int(l1.value - l0.value),
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+        }
+    dom.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed CPU oracle sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -296,6 +296,10 @@ int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out);
    reports zeros. */
 int lbm_set_kernel_timing(lbm_ctx *ctx, int32_t enable);
 int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t *cells_per_launch);
+/* Measurement hook (no counterpart in the reference): number of kernels the
+   library has launched in this process, over all contexts.  The CPU oracle
+   reports 0. */
+int lbm_launch_count(int64_t *count);
 
 int lbm_destroy(lbm_ctx *ctx);
 const char *lbm_last_error(lbm_ctx *ctx);

@@ -620,6 +620,12 @@ int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t
     return LBM_OK;
 }
 
+int lbm_launch_count(int64_t *count) {
+    if (!count) return LBM_ERR_BAD_ARG;
+    *count = (int64_t)lbm::launch_count();
+    return LBM_OK;
+}
+
 int lbm_destroy(lbm_ctx *ctx) {
     if (!ctx) return LBM_ERR_BAD_ARG;
     for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);

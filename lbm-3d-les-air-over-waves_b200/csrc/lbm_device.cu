@@ -20,6 +20,8 @@
 #define LBM_DEVICE_TU
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "lbm_launch.h"
 #include "lbm_stages.cuh"
 #include "lbm_tile.cuh"
@@ -32,6 +34,11 @@ cudaError_t upload_params(int slot, const lbm_params &P) {
 }
 
 static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// kernels launched by this library since the process started
+static std::atomic<long long> g_launches{0};
+long long launch_count() { return g_launches.load(); }
+#define LAUNCHED(n) g_launches.fetch_add((n), std::memory_order_relaxed)
 
 // 3-D launch of the general kernels: block (32, 8), grid (ceil(nx/32),
 // ceil(ny/8), planes), blockIdx.z walking the launch's z ranges
@@ -849,11 +856,11 @@ __global__ void k_export(InitArgs I, ExportArgs E) {
 // ---------------------------------------------------------------- launchers
 void launch_bed(const lbm_params &P, const Dom &D, const float *h_prev, float *h, float *hmax, float *uw, float *vw,
                 float *ww, const float *piecewise, float t, cudaStream_t st) {
-    k_bed<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, h_prev, h, uw, vw, ww, piecewise, t);
-    k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax);
+    k_bed<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, h_prev, h, uw, vw, ww, piecewise, t); LAUNCHED(1);
+    k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax); LAUNCHED(1);
 }
 void launch_hmax(const Dom &D, const float *h, float *hmax, cudaStream_t st) {
-    k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax);
+    k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax); LAUNCHED(1);
 }
 
 template <int S>
@@ -868,20 +875,20 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
     dim3 gs(A.D.nx / LBM_TILE, A.D.ny / LBM_TILE, tile_kernel ? (unsigned)ni : 0u);
     const bool les = A.P.use_les != 0;
     switch (which) {
-        case KER_PREPASS_CANON: k_prepass<S, 0><<<g, kBlock3, 0, st>>>(A); break;
-        case KER_PREPASS_FUSED: k_prepass<S, 1><<<g, kBlock3, 0, st>>>(A); break;
-        case KER_COLLIDE_CANON: k_collide<S, 0><<<g, kBlock3, 0, st>>>(A); break;
-        case KER_COLLIDE_FUSED: k_collide<S, 1><<<g, kBlock3, 0, st>>>(A); break;
-        case KER_STREAM: k_stream<S><<<g, kBlock3, 0, st>>>(A); break;
+        case KER_PREPASS_CANON: { k_prepass<S, 0><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
+        case KER_PREPASS_FUSED: { k_prepass<S, 1><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
+        case KER_COLLIDE_CANON: { k_collide<S, 0><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
+        case KER_COLLIDE_FUSED: { k_collide<S, 1><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
+        case KER_STREAM: { k_stream<S><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
         case KER_TILE_CANON:
-            if (les) k_tile<S, 0, true><<<gt, 256, 0, st>>>(A);
-            else k_tile<S, 0, false><<<gt, 256, 0, st>>>(A);
+            if (les) { k_tile<S, 0, true><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }
+            else { k_tile<S, 0, false><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }
             break;
         case KER_TILE_FUSED:
-            if (les) k_tile<S, 1, true><<<gt, 256, 0, st>>>(A);
-            else k_tile<S, 1, false><<<gt, 256, 0, st>>>(A);
+            if (les) { k_tile<S, 1, true><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }
+            else { k_tile<S, 1, false><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }
             break;
-        case KER_STREAM_INTERIOR: k_stream_interior<S><<<gs, 256, 0, st>>>(A); break;
+        case KER_STREAM_INTERIOR: { k_stream_interior<S><<<gs, 256, 0, st>>>(A); LAUNCHED(1); } break;
         default: break;
     }
 }
@@ -893,60 +900,60 @@ void launch_step_kernel(int which, const StepArgs &A, cudaStream_t st) {
     }
 }
 void launch_column_flux(const StepArgs &A, float *qx, float *qy, cudaStream_t st) {
-    k_column_flux<<<blocks_for(A.D.a, 128), 128, 0, st>>>(A, qx, qy);
+    k_column_flux<<<blocks_for(A.D.a, 128), 128, 0, st>>>(A, qx, qy); LAUNCHED(1);
 }
 void launch_advect(const lbm_params &P, const Dom &D, const float *bed_h, const float *qx, const float *qy,
                    const float *h_in, float *h_out, float *h_last, float t, cudaStream_t st) {
-    k_advect<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, bed_h, qx, qy, h_in, h_out, h_last, t);
+    k_advect<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, bed_h, qx, qy, h_in, h_out, h_last, t); LAUNCHED(1);
 }
 void launch_refill(const StepArgs &A, const int8_t *type_prev, int *count, cudaStream_t st) {
     unsigned g = blocks_for(A.D.n, 256);
     switch (A.P.pop_storage) {
-        case LBM_STORE_F16S: k_refill<LBM_STORE_F16S><<<g, 256, 0, st>>>(A, type_prev, count); break;
-        case LBM_STORE_BF16S: k_refill<LBM_STORE_BF16S><<<g, 256, 0, st>>>(A, type_prev, count); break;
-        default: k_refill<LBM_STORE_F32><<<g, 256, 0, st>>>(A, type_prev, count); break;
+        case LBM_STORE_F16S: { k_refill<LBM_STORE_F16S><<<g, 256, 0, st>>>(A, type_prev, count); LAUNCHED(1); } break;
+        case LBM_STORE_BF16S: { k_refill<LBM_STORE_BF16S><<<g, 256, 0, st>>>(A, type_prev, count); LAUNCHED(1); } break;
+        default: k_refill<LBM_STORE_F32><<<g, 256, 0, st>>>(A, type_prev, count); LAUNCHED(1); break;
     }
 }
 void launch_height_types(const StepArgs &A, float *fill, int8_t *type, int8_t *type_prev, cudaStream_t st) {
-    k_height_types<<<blocks_for(A.D.n, 256), 256, 0, st>>>(A, fill, type, type_prev);
+    k_height_types<<<blocks_for(A.D.n, 256), 256, 0, st>>>(A, fill, type, type_prev); LAUNCHED(1);
 }
 
 void launch_init_constants(const InitArgs &I, cudaStream_t st) {
     size_t n = I.D.n > I.D.a ? I.D.n : I.D.a;
-    k_init_constants<<<blocks_for(n, 256), 256, 0, st>>>(I);
+    k_init_constants<<<blocks_for(n, 256), 256, 0, st>>>(I); LAUNCHED(1);
 }
 void launch_fs_height_init(const InitArgs &I, cudaStream_t st) {
-    k_fs_height_init<<<blocks_for(I.D.a, 256), 256, 0, st>>>(I);
+    k_fs_height_init<<<blocks_for(I.D.a, 256), 256, 0, st>>>(I); LAUNCHED(1);
 }
 void launch_classify_store(const InitArgs &I, cudaStream_t st) {
-    k_classify_store<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I);
+    k_classify_store<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I); LAUNCHED(1);
 }
 void launch_vof_block(const InitArgs &I, cudaStream_t st) {
-    k_vof_block<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I);
+    k_vof_block<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I); LAUNCHED(1);
 }
 void launch_init_fields(const InitArgs &I, cudaStream_t st) {
-    k_profile<<<1, 1, 0, st>>>(I);
+    k_profile<<<1, 1, 0, st>>>(I); LAUNCHED(1);
     unsigned g = blocks_for(I.D.n, 256);
     switch (I.P.pop_storage) {
         case LBM_STORE_F16S:
-            k_init_fields<LBM_STORE_F16S><<<g, 256, 0, st>>>(I);
-            k_fs_boundary_pop<LBM_STORE_F16S><<<g, 256, 0, st>>>(I);
+            k_init_fields<LBM_STORE_F16S><<<g, 256, 0, st>>>(I); LAUNCHED(1);
+            k_fs_boundary_pop<LBM_STORE_F16S><<<g, 256, 0, st>>>(I); LAUNCHED(1);
             break;
         case LBM_STORE_BF16S:
-            k_init_fields<LBM_STORE_BF16S><<<g, 256, 0, st>>>(I);
-            k_fs_boundary_pop<LBM_STORE_BF16S><<<g, 256, 0, st>>>(I);
+            k_init_fields<LBM_STORE_BF16S><<<g, 256, 0, st>>>(I); LAUNCHED(1);
+            k_fs_boundary_pop<LBM_STORE_BF16S><<<g, 256, 0, st>>>(I); LAUNCHED(1);
             break;
         default:
-            k_init_fields<LBM_STORE_F32><<<g, 256, 0, st>>>(I);
-            k_fs_boundary_pop<LBM_STORE_F32><<<g, 256, 0, st>>>(I);
+            k_init_fields<LBM_STORE_F32><<<g, 256, 0, st>>>(I); LAUNCHED(1);
+            k_fs_boundary_pop<LBM_STORE_F32><<<g, 256, 0, st>>>(I); LAUNCHED(1);
             break;
     }
 }
 void launch_vof_mass_init(const InitArgs &I, cudaStream_t st) {
-    k_vof_mass_init<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I);
+    k_vof_mass_init<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I); LAUNCHED(1);
 }
 void launch_export(const InitArgs &I, const ExportArgs &E, cudaStream_t st) {
-    k_export<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I, E);
+    k_export<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I, E); LAUNCHED(1);
 }
 
 }  // namespace lbm

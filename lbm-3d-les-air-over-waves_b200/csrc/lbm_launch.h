@@ -73,6 +73,7 @@ struct ExportArgs {
 };
 
 cudaError_t upload_params(int slot, const lbm_params &P);
+long long launch_count();
 
 void launch_bed(const lbm_params &P, const Dom &D, const float *h_prev, float *h, float *hmax, float *uw, float *vw,
                 float *ww, const float *piecewise, float t, cudaStream_t st);

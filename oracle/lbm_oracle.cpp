@@ -747,6 +747,11 @@ int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out) {
     *out = ctx->impl->ctr;
     return LBM_OK;
 }
+int lbm_launch_count(int64_t *count) {
+    if (!count) return LBM_ERR_BAD_ARG;
+    *count = 0;
+    return LBM_OK;
+}
 int lbm_set_kernel_timing(lbm_ctx *ctx, int32_t) { return ctx ? LBM_OK : LBM_ERR_BAD_ARG; }
 int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t *cells) {
     if (!ctx || !total_ms || !launches || !cells) return LBM_ERR_BAD_ARG;

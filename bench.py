@@ -50,17 +50,19 @@ CPU_SAMPLES = [(128, 64, 256), (64, 64, 256), (64, 32, 256), (64, 16, 256)]
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_tile_air_interior.md")
 
 
-def workload_env(nx=NX, ny=NY, nz=NZ, seed=12345):
+def workload_env(nx=None, ny=None, nz=None, seed=12345):
     from lbm_b200.config import air_wave_env
 
-    return air_wave_env(nx, ny, nz, storage="f32", seed=seed)
+    return air_wave_env(nx or NX, ny or NY, nz or NZ, storage="f32", seed=seed)
 
 
 def base_config():
     return {
         "workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "cells": NX * NY * NZ, "collision": "regularized",
         "les": "smagorinsky Cs=0.16", "tau0": 0.52, "storage": "f32", "steps_per_call": CHUNK,
-        "l2": "inputs larger than L2 (5.1 GB of populations, A-B)", "parallelism": "replicas",
+        "l2": (f"inputs larger than L2 ({NX * NY * NZ * B_ALG / 1e9:.2f} GB of populations, A-B)"
+               if NX * NY * NZ * B_ALG > 126e6 else "inputs fit in L2 (small profiling case)"),
+        "parallelism": "replicas",
     }
 
 
@@ -385,7 +387,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed CPU oracle sample")
+    ap.add_argument("--size", type=str, default=None,
+                    help="NXxNYxNZ: another domain size of the same workload (profiling of small cases)")
     args = ap.parse_args()
+    if args.size:
+        global NX, NY, NZ, WORKLOAD
+        NX, NY, NZ = (int(v) for v in args.size.lower().split("x"))
+        WORKLOAD = f"air over moving wave, LES regularized, {NX}x{NY}x{NZ}, FP32 populations"
     if args.impl == "reference":
         return reference_arm(args)
     return ours(args)

@@ -71,6 +71,8 @@ struct lbm_ctx {
     // scratch owned by the library
     float *bed_h[2] = {nullptr, nullptr}, *bed_hmax[2] = {nullptr, nullptr};
     float *bed_uw[2] = {nullptr, nullptr}, *bed_vw[2] = {nullptr, nullptr}, *bed_ww[2] = {nullptr, nullptr};
+    float *bed_cg[2] = {nullptr, nullptr};  // per-column link-endpoint cache (bed-only geometry)
+    bool use_cg = false;
     float *u_les = nullptr;
     int *dcount = nullptr;
     unsigned *dstatus = nullptr;
@@ -118,7 +120,20 @@ static BedView slot_view(const lbm_ctx *ctx, int s) {
     v.uw = ctx->bed_uw[s];
     v.vw = ctx->bed_vw[s];
     v.ww = ctx->bed_ww[s];
+    v.cg = ctx->use_cg ? ctx->bed_cg[s] : nullptr;
     return v;
+}
+
+// the column cache serves bed-only geometry: no cube, no phi geometry,
+// periodic x
+static bool wants_column_cache(const lbm_params &P) {
+    return P.include_bed && !P.include_cube && !P.use_phi_open_fraction && !P.use_phi_open_flags && !P.x_solid;
+}
+static int refresh_column_cache(lbm_ctx *ctx, int s, cudaStream_t st) {
+    if (!ctx->use_cg) return LBM_OK;
+    launch_colgeo(ctx->P, ctx->D, slot_view(ctx, s), ctx->bed_cg[s], st);
+    CK_LAUNCH("column cache");
+    return LBM_OK;
 }
 
 static float step_time(const lbm_ctx *ctx, int64_t step) {
@@ -133,6 +148,7 @@ static InitArgs init_args(lbm_ctx *ctx, int slot) {
     I.slot = ctx->slot;
     I.D = ctx->D;
     I.bed = slot_view(ctx, slot);
+    I.bed.cg = nullptr;   // setup kernels take the per-link path
     I.f_cur = b.f[ctx->cur];
     I.f_other = b.f[1 - ctx->cur];
     I.rho = b.rho; I.ux = b.ux; I.uy = b.uy; I.uz = b.uz; I.omega = b.omega;
@@ -180,7 +196,7 @@ static int load_bed_slot(lbm_ctx *ctx, int s, cudaStream_t st) {
     CK(cudaMemcpyAsync(ctx->bed_ww[s], ctx->b.w_wave, bytes, cudaMemcpyDeviceToDevice, st), "bed copy");
     launch_hmax(ctx->D, ctx->bed_h[s], ctx->bed_hmax[s], st);
     CK_LAUNCH("hmax");
-    return LBM_OK;
+    return refresh_column_cache(ctx, s, st);
 }
 // copy slot s (and the previous height) back to the bound buffers
 static int store_bed_slot(lbm_ctx *ctx, int s, const float *h_prev, cudaStream_t st) {
@@ -198,7 +214,7 @@ static int bed_step(lbm_ctx *ctx, int64_t m, cudaStream_t st) {
     launch_bed(ctx->P, ctx->D, ctx->bed_h[sp], ctx->bed_h[s], ctx->bed_hmax[s], ctx->bed_uw[s], ctx->bed_vw[s],
                ctx->bed_ww[s], ctx->b.piecewise_bed_z, step_time(ctx, m), st);
     CK_LAUNCH("bed");
-    return LBM_OK;
+    return refresh_column_cache(ctx, s, st);
 }
 
 // Split of the planes between the interior tile kernel and the general
@@ -449,6 +465,11 @@ int lbm_bind(lbm_ctx *ctx, const lbm_buffers *bufs) {
                 return s;
         }
         if (ctx->P.use_les && (s = alloc(ctx, (void **)&ctx->u_les, 3 * ctx->D.n * sizeof(float)))) return s;
+        if (wants_column_cache(ctx->P)) {
+            for (int i = 0; i < 2; ++i)
+                if ((s = alloc(ctx, (void **)&ctx->bed_cg[i], (size_t)CG_N * A))) return s;
+            ctx->use_cg = true;
+        }
         if ((s = alloc(ctx, (void **)&ctx->dcount, CNT_N * sizeof(int))) ||
             (s = alloc(ctx, (void **)&ctx->dstatus, sizeof(unsigned))) ||
             (s = alloc(ctx, (void **)&ctx->dfcount, 8 * sizeof(float))))

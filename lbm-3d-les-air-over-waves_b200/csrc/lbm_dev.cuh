@@ -141,7 +141,10 @@ struct BedView {
     const float *h;      // water_h (bed height)
     const float *hmax;   // max of h over the 3x3 column neighbourhood
     const float *uw, *vw, *ww;
+    const float *cg;     // per-column link-endpoint cache (bed-only geometry), or null
 };
+// components of the column cache, [component][column]
+enum { CG_ETA = 0, CG_UW = 9, CG_DEN = 36, CG_N = 37 };
 
 // free-surface view (height path derives cell states from the column height)
 struct FsView {

@@ -159,7 +159,20 @@ __global__ void k_hmax(Dom D, const float *__restrict__ h, float *hmax) {
     hmax[a] = m;
 }
 
+// per-column link-endpoint cache of one bed state (bed-only geometry)
+__global__ void k_colgeo(lbm_params P, Dom D, BedView B, float *cg) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (int)D.a) return;
+    const int j = a / D.nx, i = a - j * D.nx;
+    colgeo_column(P, D, B, j, i, cg);
+}
+
 // ------------------------------------------------------- step kernels
+// resident blocks per SM requested for the general (near-wall) kernels:
+// one, so that their long near-wall paths run without register spills
+#ifndef LBM_GEN_MINB
+#define LBM_GEN_MINB 1
+#endif
 template <int S>
 __device__ __forceinline__ void load_cell(const StepArgs &A, int c, float f[19]) {
     const typename Store<S>::T *src = (const typename Store<S>::T *)A.fsrc;
@@ -178,7 +191,7 @@ __device__ __forceinline__ void store_cell(const StepArgs &A, int c, const float
 // post-stream state; IN = 1: stream + BC of the previous step from its
 // post-collision state.  Cells away from every wall and boundary take the
 // plain gather; the general path handles the rest.
-template <int S, int IN>
+template <int S, int IN, bool CG>
 __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, int i, float f[19], bool &fast_c,
                                       bool &open, int &type, float &gbf, float &r, float &vx, float &vy, float &vz) {
     const lbm_params &P = A.P;
@@ -197,12 +210,12 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
         load_cell<S>(A, c, f);
     } else {
         GeoLinks Ls;
-        Geo gs = geo_cell(P, A.slot, A.D, A.bed_s, k, j, i, Ls, true, P.use_link_wall_velocity && P.include_bed);
+        Geo gs = geo_cell<CG>(P, A.slot, A.D, A.bed_s, k, j, i, Ls, true, P.use_link_wall_velocity && P.include_bed);
         int cut = 0, fscut = 0, bridge = 0;
         stream_bc<S>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
     }
     GeoLinks Lc;
-    Geo gc = geo_cell(P, A.slot, A.D, A.bed_c, k, j, i, Lc, true, P.use_link_wall_velocity && P.include_bed);
+    Geo gc = geo_cell<CG>(P, A.slot, A.D, A.bed_c, k, j, i, Lc, true, P.use_link_wall_velocity && P.include_bed);
     fast_c = gc.fast;
     open = (gc.lo & 1u) != 0u;
     type = LBM_FS_LIQUID;
@@ -216,27 +229,27 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
     macro(P, A.D, f, k, water, type, gbf, r, vx, vy, vz);
 }
 
-template <int S, int IN>
-__global__ void __launch_bounds__(256, 2) k_prepass(StepArgs A) {
+template <int S, int IN, bool CG>
+__global__ void __launch_bounds__(256, LBM_GEN_MINB) k_prepass(StepArgs A) {
     int i, j, k, c;
     if (!cell_xyz(A, i, j, k, c)) return;
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
-    front<S, IN>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
+    front<S, IN, CG>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
     A.u_out[c] = vx;
     A.u_out[A.D.n + c] = vy;
     A.u_out[2 * A.D.n + c] = vz;
 }
 
-template <int S, int IN>
-__global__ void __launch_bounds__(256, 2) k_collide(StepArgs A) {
+template <int S, int IN, bool CG>
+__global__ void __launch_bounds__(256, LBM_GEN_MINB) k_collide(StepArgs A) {
     int i, j, k, c;
     if (!cell_xyz(A, i, j, k, c)) return;
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
-    front<S, IN>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
+    front<S, IN, CG>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
     const lbm_params &P = A.P;
     const bool water = P.fs_mode != LBM_FS_NONE;
     const bool gas = water && type == LBM_FS_GAS;
@@ -259,8 +272,8 @@ __global__ void __launch_bounds__(256, 2) k_collide(StepArgs A) {
     store_cell<S>(A, c, f);
 }
 
-template <int S>
-__global__ void __launch_bounds__(256, 2) k_stream(StepArgs A) {
+template <int S, bool CG>
+__global__ void __launch_bounds__(256, LBM_GEN_MINB) k_stream(StepArgs A) {
     int i, j, k, c;
     int cut = 0, fscut = 0, bridge = 0;
     if (cell_xyz(A, i, j, k, c)) {
@@ -270,7 +283,7 @@ __global__ void __launch_bounds__(256, 2) k_stream(StepArgs A) {
             store_cell<S>(A, c, f);
         } else {
             GeoLinks Ls;
-            Geo gs = geo_cell(A.P, A.slot, A.D, A.bed_s, k, j, i, Ls, true, A.P.use_link_wall_velocity && A.P.include_bed);
+            Geo gs = geo_cell<CG>(A.P, A.slot, A.D, A.bed_s, k, j, i, Ls, true, A.P.use_link_wall_velocity && A.P.include_bed);
             stream_bc<S>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
             store_cell<S>(A, c, f);
             if (A.P.fs_mode != LBM_FS_NONE) {
@@ -859,6 +872,9 @@ void launch_bed(const lbm_params &P, const Dom &D, const float *h_prev, float *h
     k_bed<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, h_prev, h, uw, vw, ww, piecewise, t); LAUNCHED(1);
     k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax); LAUNCHED(1);
 }
+void launch_colgeo(const lbm_params &P, const Dom &D, const BedView &B, float *cg, cudaStream_t st) {
+    k_colgeo<<<blocks_for(D.a, 128), 128, 0, st>>>(P, D, B, cg); LAUNCHED(1);
+}
 void launch_hmax(const Dom &D, const float *h, float *hmax, cudaStream_t st) {
     k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax); LAUNCHED(1);
 }
@@ -874,12 +890,34 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
     dim3 gt(A.D.nx / LBM_TILE, A.D.ny / LBM_TILE, tz);
     dim3 gs(A.D.nx / LBM_TILE, A.D.ny / LBM_TILE, tile_kernel ? (unsigned)ni : 0u);
     const bool les = A.P.use_les != 0;
+    // the column cache is set on both bed views or on neither
+    const bool cg = A.bed_s.cg != nullptr && A.bed_c.cg != nullptr;
     switch (which) {
-        case KER_PREPASS_CANON: { k_prepass<S, 0><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
-        case KER_PREPASS_FUSED: { k_prepass<S, 1><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
-        case KER_COLLIDE_CANON: { k_collide<S, 0><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
-        case KER_COLLIDE_FUSED: { k_collide<S, 1><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
-        case KER_STREAM: { k_stream<S><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); } break;
+        case KER_PREPASS_CANON:
+            if (cg) k_prepass<S, 0, true><<<g, kBlock3, 0, st>>>(A);
+            else k_prepass<S, 0, false><<<g, kBlock3, 0, st>>>(A);
+            LAUNCHED(1);
+            break;
+        case KER_PREPASS_FUSED:
+            if (cg) k_prepass<S, 1, true><<<g, kBlock3, 0, st>>>(A);
+            else k_prepass<S, 1, false><<<g, kBlock3, 0, st>>>(A);
+            LAUNCHED(1);
+            break;
+        case KER_COLLIDE_CANON:
+            if (cg) k_collide<S, 0, true><<<g, kBlock3, 0, st>>>(A);
+            else k_collide<S, 0, false><<<g, kBlock3, 0, st>>>(A);
+            LAUNCHED(1);
+            break;
+        case KER_COLLIDE_FUSED:
+            if (cg) k_collide<S, 1, true><<<g, kBlock3, 0, st>>>(A);
+            else k_collide<S, 1, false><<<g, kBlock3, 0, st>>>(A);
+            LAUNCHED(1);
+            break;
+        case KER_STREAM:
+            if (cg) k_stream<S, true><<<g, kBlock3, 0, st>>>(A);
+            else k_stream<S, false><<<g, kBlock3, 0, st>>>(A);
+            LAUNCHED(1);
+            break;
         case KER_TILE_CANON:
             if (les) { k_tile<S, 0, true><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }
             else { k_tile<S, 0, false><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }

@@ -275,6 +275,101 @@ static __device__ __noinline__ Geo geo_slow(int slot, Dom D, BedView B, int k, i
     return g;
 }
 
+// Per-column cache of the bed at the link endpoints.  With bed-only
+// geometry (no cube, no phi geometry, periodic x) a cell's link endpoints
+// sit at nine (x, y) positions that do not depend on k, so the bed height
+// and wall velocity there are sampled once per column per bed state, with
+// the arithmetic of the per-link path.  Layout [component][column]:
+// 0..8 bed height at endpoint e = endpoint_index(q), 9..35 wall velocity
+// (e, component), 36 slope denominator of compute_phi_slope_corrected.
+LBM_DEV void colgeo_column(const lbm_params &P, const Dom &D, const BedView &B, int j, int i, float *cg) {
+    const float dx = P.dx, hdx = 0.5f * dx;
+    const size_t A = D.a;
+    const int a = D.col(j, i);
+    float xc = ((float)i + 0.5f) * dx, yc = ((float)j + 0.5f) * dx;
+    int xi0[3], xi1[3], yj0[3], yj1[3];
+    float xf[3], yf[3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        bl_axis(xc + hdx * (float)(s - 1), dx, D.nx, xi0[s], xi1[s], xf[s]);
+        bl_axis(yc + hdx * (float)(s - 1), dx, D.ny, yj0[s], yj1[s], yf[s]);
+    }
+#pragma unroll
+    for (int xa = 0; xa < 3; ++xa)
+#pragma unroll
+        for (int yb = 0; yb < 3; ++yb) {
+            const int e = 3 * xa + yb;
+            cg[(size_t)(CG_ETA + e) * A + a] = bl_sample(B.h, D, xi0[xa], yj0[yb], xi1[xa], yj1[yb], xf[xa], yf[yb]);
+            cg[(size_t)(CG_UW + 3 * e) * A + a] = bl_sample(B.uw, D, xi0[xa], yj0[yb], xi1[xa], yj1[yb], xf[xa], yf[yb]);
+            cg[(size_t)(CG_UW + 3 * e + 1) * A + a] =
+                bl_sample(B.vw, D, xi0[xa], yj0[yb], xi1[xa], yj1[yb], xf[xa], yf[yb]);
+            cg[(size_t)(CG_UW + 3 * e + 2) * A + a] =
+                bl_sample(B.ww, D, xi0[xa], yj0[yb], xi1[xa], yj1[yb], xf[xa], yf[yb]);
+        }
+    // slope denominator of phi_cell (periodic x)
+    int ip = (i + 1) % D.nx, im = (i - 1 + D.nx) % D.nx, jp = (j + 1) % D.ny, jm = (j - 1 + D.ny) % D.ny;
+    float dhdx = (__ldg(B.h + D.col(j, ip)) - __ldg(B.h + D.col(j, im))) * P.half_inv_dx;
+    float dhdy = (__ldg(B.h + D.col(jp, i)) - __ldg(B.h + D.col(jm, i))) * P.half_inv_dx;
+    float denom = sqrtf(1.0f + dhdx * dhdx + dhdy * dhdy);
+    if (denom < 1e-6f) denom = 1.0f;
+    cg[(size_t)CG_DEN * A + a] = denom;
+}
+
+// geo_slow for bed-only geometry from the column cache (same arithmetic)
+LBM_DEV Geo geo_cached(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i, GeoLinks &L) {
+    const size_t A = D.a;
+    const int a = D.col(j, i);
+    const float dx = P.dx, hdx = 0.5f * dx;
+    float zc = ((float)k + 0.5f) * dx;
+    float eta9[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) eta9[e] = __ldg(B.cg + (size_t)(CG_ETA + e) * A + a);
+    Geo g;
+    g.fast = false;
+    const int wtb = P.include_bed ? LBM_WALL_BED : LBM_WALL_NONE;
+    float ggc = P.include_bed ? zc - eta9[4] : 1.0e6f;
+    float frc = 0.5f + ggc / dx;
+    if (frc < 0.0f) frc = 0.0f;
+    if (frc > 1.0f) frc = 1.0f;
+    L.lf[0] = frc;
+    L.wt[0] = (uint8_t)wtb;
+    uint32_t lo = 0u;
+#pragma unroll
+    for (int q = 1; q < 19; ++q) {
+        float zq = zc + hdx * (float)czq(q);
+        float gg = P.include_bed ? zq - eta9[endpoint_index(q)] : 1.0e6f;
+        float fr = 0.5f + gg / dx;
+        if (fr < 0.0f) fr = 0.0f;
+        if (fr > 1.0f) fr = 1.0f;
+        L.lf[q] = fr;
+        L.wt[q] = (uint8_t)wtb;
+        if (!(gg < 0.0f)) lo |= (1u << q);
+    }
+    if (lo) lo |= 1u;
+    g.near = (lo & 0x7FFFEu) != 0x7FFFEu;
+    uint32_t part = 0u;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        if (q > 0 && !(lo & 1u)) L.lf[q] = 0.0f;
+        if (L.lf[q] < 1.0f) part |= (1u << q);
+    }
+    g.part = part;
+    g.lo = lo;
+    L.has_uw = false;
+    return g;
+}
+// wall velocity at endpoint e from the column cache
+LBM_DEV void cached_wall(const Dom &D, const BedView &B, int j, int i, int e, float &wx, float &wy, float &wz) {
+    const size_t A = D.a;
+    const int a = D.col(j, i);
+    wx = __ldg(B.cg + (size_t)(CG_UW + 3 * e) * A + a);
+    wy = __ldg(B.cg + (size_t)(CG_UW + 3 * e + 1) * A + a);
+    wz = __ldg(B.cg + (size_t)(CG_UW + 3 * e + 2) * A + a);
+}
+
+// CG: the bed view carries the column cache (bed-only geometry); the link
+// data then never goes through an out-of-line call
+template <bool CG = false>
 LBM_DEV Geo geo_cell(const lbm_params &P, int slot, const Dom &D, const BedView &B, int k, int j, int i, GeoLinks &L,
                      bool allow_fast = true, bool want_uw = false) {
     if (allow_fast && geo_far(P, D, B, k, j, i)) {
@@ -285,11 +380,13 @@ LBM_DEV Geo geo_cell(const lbm_params &P, int slot, const Dom &D, const BedView 
         g.fast = true;
         return g;
     }
+    if (CG) return geo_cached(P, D, B, k, j, i, L);
     return geo_slow(slot, D, B, k, j, i, &L, want_uw);
 }
 
 static __device__ __noinline__ bool cell_open_slow(int slot, Dom D, BedView B, int k, int j, int i) {
     GeoLinks L;
+    if (B.cg) return (geo_cached(c_params[slot], D, B, k, j, i, L).lo & 1u) != 0u;
     return (geo_slow(slot, D, B, k, j, i, &L, false).lo & 1u) != 0u;
 }
 // lattice_open[0] only (cheap when far from walls)

@@ -78,6 +78,7 @@ long long launch_count();
 void launch_bed(const lbm_params &P, const Dom &D, const float *h_prev, float *h, float *hmax, float *uw, float *vw,
                 float *ww, const float *piecewise, float t, cudaStream_t st);
 void launch_hmax(const Dom &D, const float *h, float *hmax, cudaStream_t st);
+void launch_colgeo(const lbm_params &P, const Dom &D, const BedView &B, float *cg, cudaStream_t st);
 void launch_step_kernel(int which, const StepArgs &A, cudaStream_t st);
 void launch_column_flux(const StepArgs &A, float *qx, float *qy, cudaStream_t st);
 void launch_advect(const lbm_params &P, const Dom &D, const float *bed_h, const float *qx, const float *qy,

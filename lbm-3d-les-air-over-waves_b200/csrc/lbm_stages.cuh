@@ -360,6 +360,8 @@ LBM_DEV void stream_bc(const StepArgs &A, const typename Store<S>::T *__restrict
                     if (L.has_uw) {
                         const int e = endpoint_index(q);
                         wx = L.uw[e][0]; wy = L.uw[e][1]; wz = L.uw[e][2];
+                    } else if (B.cg) {
+                        cached_wall(D, B, j, i, endpoint_index(q), wx, wy, wz);
                     } else {
                         sample_wall(P, D, B, xc + hdx * (float)cxq(q), yc + hdx * (float)cyq(q), wx, wy, wz);
                     }
@@ -402,6 +404,8 @@ LBM_DEV void condition(const lbm_params &P, const Dom &D, const BedView &B, cons
             if (L.has_uw) {
                 const int e = endpoint_index(q);
                 vx = L.uw[e][0]; vy = L.uw[e][1]; vz = L.uw[e][2];
+            } else if (B.cg) {
+                cached_wall(D, B, j, i, endpoint_index(q), vx, vy, vz);
             } else {
                 sample_wall(P, D, B, xc + hdx * (float)cxq(q), yc + hdx * (float)cyq(q), vx, vy, vz);
             }
@@ -459,9 +463,20 @@ static __device__ __noinline__ float wall_model_nu(int slot, Dom D, BedView bed,
                                                    float vy, float nu_t) {
     const lbm_params &P = c_params[slot];
     GeoLinks Lb;
-    Geo gb = geo_slow(slot, D, bed, k - 1, j, i, &Lb, false);
-    if (gb.lo & 1u) return nu_t;
-    float phi = phi_cell(P, D, bed.h, k, j, i);
+    float phi;
+    if (bed.cg) {
+        Geo gb = geo_cached(P, D, bed, k - 1, j, i, Lb);
+        if (gb.lo & 1u) return nu_t;
+        // phi_cell with bed-only geometry
+        phi = 1.0e6f;
+        if (P.include_bed)
+            phi = (((float)k + 0.5f) * P.dx - __ldg(bed.h + D.col(j, i))) /
+                  __ldg(bed.cg + (size_t)CG_DEN * D.a + D.col(j, i));
+    } else {
+        Geo gb = geo_slow(slot, D, bed, k - 1, j, i, &Lb, false);
+        if (gb.lo & 1u) return nu_t;
+        phi = phi_cell(P, D, bed.h, k, j, i);
+    }
     float dist = fmaxf(phi, P.wall_dist_floor);
     float lv = lbm_logf(dist / P.z0_phys);
     if (lv < 2.0f) lv = 2.0f;

@@ -27,6 +27,7 @@
 #ifndef LBM_B200_H
 #define LBM_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -300,6 +301,37 @@ int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t
    library has launched in this process, over all contexts.  The CPU oracle
    reports 0. */
 int lbm_launch_count(int64_t *count);
+
+/* Allocation-free link geometry (no counterpart in the reference).
+   Writes, for the bed height field bed_h ([ny][nx], device) and the grid
+   and geometry options in params, the same per-cell link geometry that
+   lbm_export_diagnostics writes after a step: phi, obstacle, near_obstacle
+   ([nz][ny][nx]) and lattice_open, lattice_open_frac, lattice_wall_type
+   ([19][nz][ny][nx]).  Any output pointer may be NULL.  It needs no
+   context and allocates nothing.  It is meant for callers that must not
+   call cudaMalloc but still want the open flags and fractions of a bed
+   shape (a visualisation or analysis hook).  Examples: a serving process
+   whose device memory is fully committed to population buffers by its
+   admission budget; a host framework that owns all device memory through
+   its own caching allocator, where a raw cudaMalloc would synchronise the
+   device and fragment the pool.
+   Scratch is a fixed device array of 9 floats per column, sized for at
+   most LBM_NOALLOC_MAX_COLUMNS columns (nx*ny; 2.25 MiB, held by every
+   GPU that loads the library until the process exits); larger grids are
+   rejected with LBM_ERR_BAD_ARG.  Bed geometry only (no cube, no phi
+   geometry, periodic x), else LBM_ERR_UNSUPPORTED.  Runs on the calling
+   thread's current device, asynchronously on stream (which must belong to
+   that device).  The first call on a device looks up the array's device
+   address; make that first call before any stream capture.  All calls
+   share the one array: calls that overlap on the GPU (other streams, other
+   threads) race and must be serialised by the caller.  Each call rewrites
+   every entry it reads, so nothing needs clearing between calls.  err (may
+   be NULL) receives a message of at most err_len bytes on failure.  The
+   CPU oracle returns LBM_ERR_UNSUPPORTED. */
+#define LBM_NOALLOC_MAX_COLUMNS 65536
+int lbm_link_geometry_noalloc(const lbm_params *params, const float *bed_h, float *phi, int32_t *obstacle,
+                              int32_t *near_obstacle, int8_t *lattice_open, float *lattice_open_frac,
+                              int8_t *lattice_wall_type, void *stream, char *err, size_t err_len);
 
 int lbm_destroy(lbm_ctx *ctx);
 const char *lbm_last_error(lbm_ctx *ctx);

@@ -21,6 +21,9 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
 
 #include "lbm_launch.h"
 #include "lbm_stages.cuh"
@@ -995,3 +998,156 @@ void launch_export(const InitArgs &I, const ExportArgs &E, cudaStream_t st) {
 }
 
 }  // namespace lbm
+
+// ------------------------------------------- allocation-free link geometry
+// lbm_link_geometry_noalloc: the link geometry that lbm_export_diagnostics
+// writes (phi, obstacle, near_obstacle, lattice_open, lattice_open_frac,
+// lattice_wall_type), for a bed height field the caller passes, without any
+// context or allocation.  The bed heights at the nine link-endpoint (x, y)
+// positions of each column are sampled once into a fixed device array, and
+// the per-cell pass reads them from there (the bed-only path of the step
+// kernels, same arithmetic as the per-link path of k_export).
+namespace lbm {
+
+#define LBM_MAX_DEVICES 64
+
+// [9][columns]: bed height at endpoint e of each column, stride nx*ny.
+// Every call overwrites the entries it reads, so nothing needs clearing.
+static __device__ __align__(256) float g_noalloc_endpoints[9 * LBM_NOALLOC_MAX_COLUMNS];
+
+__global__ void k_noalloc_endpoints(lbm_params P, Dom D, const float *__restrict__ bed_h, float *cache) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (int)D.a) return;
+    const int j = a / D.nx, i = a - j * D.nx;
+    const float dx = P.dx, hdx = 0.5f * dx;
+    float xc = ((float)i + 0.5f) * dx, yc = ((float)j + 0.5f) * dx;
+    int xi0[3], xi1[3], yj0[3], yj1[3];
+    float xf[3], yf[3];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        bl_axis(xc + hdx * (float)(s - 1), dx, D.nx, xi0[s], xi1[s], xf[s]);
+        bl_axis(yc + hdx * (float)(s - 1), dx, D.ny, yj0[s], yj1[s], yf[s]);
+    }
+#pragma unroll
+    for (int xa = 0; xa < 3; ++xa)
+#pragma unroll
+        for (int yb = 0; yb < 3; ++yb)
+            cache[(size_t)(CG_ETA + 3 * xa + yb) * D.a + a] =
+                bl_sample(bed_h, D, xi0[xa], yj0[yb], xi1[xa], yj1[yb], xf[xa], yf[yb]);
+}
+
+__global__ void k_noalloc_links(lbm_params P, Dom D, const float *__restrict__ bed_h, const float *cache,
+                                ExportArgs E) {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int)D.n) return;
+    int k, j, i;
+    cell_of(D, c, k, j, i);
+    BedView B;
+    B.h = bed_h;
+    B.hmax = nullptr;
+    B.uw = B.vw = B.ww = nullptr;
+    B.cg = cache;
+    GeoLinks L;
+    Geo g = geo_cached(P, D, B, k, j, i, L);
+    bool open = (g.lo & 1u) != 0u;
+    if (E.phi) E.phi[c] = phi_cell(P, D, bed_h, k, j, i);
+    if (E.obstacle) E.obstacle[c] = open ? 0 : 1;
+    if (E.near_obstacle) E.near_obstacle[c] = g.near ? 1 : 0;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) {
+        if (E.lattice_open) E.lattice_open[(size_t)q * D.n + c] = (int8_t)((g.lo >> q) & 1u);
+        if (E.lattice_open_frac) E.lattice_open_frac[(size_t)q * D.n + c] = L.lf[q];
+        if (E.lattice_wall_type) E.lattice_wall_type[(size_t)q * D.n + c] = (int8_t)L.wt[q];
+    }
+}
+
+// Device address of g_noalloc_endpoints on the current device.  In host
+// code the array's name is only a host-side stand-in, so the address is
+// looked up once per device (with that device current) and kept.
+static std::mutex g_noalloc_mutex;
+static float *g_noalloc_address[LBM_MAX_DEVICES] = {};
+
+static cudaError_t noalloc_endpoints_address(float **out) {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= LBM_MAX_DEVICES) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_address[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_endpoints);
+        if (e != cudaSuccess) return e;
+        g_noalloc_address[dev] = (float *)p;
+    }
+    *out = g_noalloc_address[dev];
+    return cudaSuccess;
+}
+
+static int noalloc_fail(char *err, size_t err_len, int code, const char *msg) {
+    if (err && err_len) snprintf(err, err_len, "%s", msg);
+    return code;
+}
+
+}  // namespace lbm
+
+extern "C" int lbm_link_geometry_noalloc(const lbm_params *params, const float *bed_h, float *phi, int32_t *obstacle,
+                                         int32_t *near_obstacle, int8_t *lattice_open, float *lattice_open_frac,
+                                         int8_t *lattice_wall_type, void *stream, char *err, size_t err_len) {
+    using namespace lbm;
+    if (err && err_len) err[0] = '\0';
+    if (!params || !bed_h)
+        return noalloc_fail(err, err_len, LBM_ERR_BAD_ARG, "lbm_link_geometry_noalloc: params and bed_h are required");
+    const lbm_params &P = *params;
+    if (P.abi_version != LBM_ABI_VERSION || P.magic_end != LBM_PARAMS_MAGIC)
+        return noalloc_fail(err, err_len, LBM_ERR_BAD_ARG,
+                            "lbm_link_geometry_noalloc: lbm_params layout or ABI version mismatch");
+    if (P.nx < 1 || P.ny < 1 || P.nz < 2)
+        return noalloc_fail(err, err_len, LBM_ERR_BAD_ARG, "lbm_link_geometry_noalloc: grid must be nx, ny >= 1, nz >= 2");
+    const size_t cols = (size_t)P.nx * (size_t)P.ny;
+    if (cols > (size_t)LBM_NOALLOC_MAX_COLUMNS) {
+        char msg[200];
+        snprintf(msg, sizeof msg,
+                 "lbm_link_geometry_noalloc: nx*ny = %zu columns exceeds the fixed maximum of %d; "
+                 "use lbm_export_diagnostics on a context instead",
+                 cols, (int)LBM_NOALLOC_MAX_COLUMNS);
+        return noalloc_fail(err, err_len, LBM_ERR_BAD_ARG, msg);
+    }
+    if (cols * (size_t)P.nz > 0x7fffffffULL)
+        return noalloc_fail(err, err_len, LBM_ERR_BAD_ARG, "lbm_link_geometry_noalloc: more than 2^31-1 cells");
+    if (P.include_cube || P.use_phi_open_fraction || P.use_phi_open_flags || P.x_solid)
+        return noalloc_fail(err, err_len, LBM_ERR_UNSUPPORTED,
+                            "lbm_link_geometry_noalloc: only bed geometry with periodic x is supported "
+                            "(no cube, no phi geometry, no solid x walls)");
+    float *cache = nullptr;
+    cudaError_t e = noalloc_endpoints_address(&cache);
+    if (e != cudaSuccess) {
+        char msg[200];
+        snprintf(msg, sizeof msg, "lbm_link_geometry_noalloc: device address of the fixed array: %s",
+                 cudaGetErrorString(e));
+        return noalloc_fail(err, err_len, LBM_ERR_CUDA, msg);
+    }
+    Dom D;
+    D.nx = P.nx;
+    D.ny = P.ny;
+    D.nz = P.nz;
+    D.a = cols;
+    D.n = cols * (size_t)P.nz;
+    ExportArgs E;
+    memset(&E, 0, sizeof E);
+    E.phi = phi;
+    E.obstacle = obstacle;
+    E.near_obstacle = near_obstacle;
+    E.lattice_open = lattice_open;
+    E.lattice_open_frac = lattice_open_frac;
+    E.lattice_wall_type = lattice_wall_type;
+    cudaStream_t st = (cudaStream_t)stream;
+    k_noalloc_endpoints<<<blocks_for(D.a, 128), 128, 0, st>>>(P, D, bed_h, cache); LAUNCHED(1);
+    k_noalloc_links<<<blocks_for(D.n, 256), 256, 0, st>>>(P, D, bed_h, cache, E); LAUNCHED(1);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        char msg[200];
+        snprintf(msg, sizeof msg, "lbm_link_geometry_noalloc: launch: %s", cudaGetErrorString(e));
+        return noalloc_fail(err, err_len, LBM_ERR_CUDA, msg);
+    }
+    return LBM_OK;
+}

@@ -15,6 +15,12 @@ LBM_ABI_VERSION = 1
 LBM_PARAMS_MAGIC = 0x1B200D19
 
 LBM_OK = 0
+LBM_ERR_BAD_ARG = -1
+LBM_ERR_CUDA = -2
+LBM_ERR_NOT_CONVERGED = -3
+LBM_ERR_NONFINITE = -4
+LBM_ERR_UNSUPPORTED = -5
+LBM_ERR_NOT_BOUND = -6
 ERRORS = {
     -1: "bad argument", -2: "CUDA error", -3: "not converged", -4: "non-finite value",
     -5: "unsupported configuration", -6: "buffers not bound",
@@ -263,13 +269,16 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.lbm_kernel_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.lbm_launch_count.restype = C.c_int
     lib.lbm_launch_count.argtypes = [C.POINTER(C.c_int64)]
+    lib.lbm_link_geometry_noalloc.restype = C.c_int
+    lib.lbm_link_geometry_noalloc.argtypes = [C.POINTER(LbmParams), vp, vp, vp, vp, vp, vp, vp, vp, C.c_char_p,
+                                              C.c_size_t]
     return lib
 
 
 ABI_SYMBOLS = (
     "lbm_backend_name", "lbm_abi_version", "lbm_struct_size", "lbm_create", "lbm_bind", "lbm_init_geometry",
     "lbm_init_fields", "lbm_step", "lbm_export_diagnostics", "lbm_read_counters", "lbm_destroy", "lbm_last_error",
-    "lbm_set_kernel_timing", "lbm_kernel_timing", "lbm_launch_count",
+    "lbm_set_kernel_timing", "lbm_kernel_timing", "lbm_launch_count", "lbm_link_geometry_noalloc",
 )
 
 

@@ -747,6 +747,11 @@ int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out) {
     *out = ctx->impl->ctr;
     return LBM_OK;
 }
+int lbm_link_geometry_noalloc(const lbm_params *, const float *, float *, int32_t *, int32_t *, int8_t *, float *,
+                              int8_t *, void *, char *err, size_t err_len) {
+    if (err && err_len) snprintf(err, err_len, "%s", "the CPU oracle has no allocation-free variant");
+    return LBM_ERR_UNSUPPORTED;
+}
 int lbm_launch_count(int64_t *count) {
     if (!count) return LBM_ERR_BAD_ARG;
     *count = 0;

@@ -209,7 +209,22 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
         macro(P, A.D, f, k, false, type, gbf, r, vx, vy, vz);
         return;
     }
-    if (IN == 0) {
+    GeoLinks Lc;
+    Geo gc = geo_cell<CG>(P, A.slot, A.D, A.bed_c, k, j, i, Lc, true, P.use_link_wall_velocity && P.include_bed);
+    // A cell with every link closed in the collide geometry (air): the
+    // condition stage sets f_q = frac_q f_q + (1 - frac_q) feq_q on every
+    // link, with frac_q = 0 for q >= 1, so only the rest population of the
+    // stream stage survives (the others enter multiplied by zero).  The
+    // stream stage leaves f_0 local here (no fringe, no top drive at this
+    // cell), so the gather and the stream geometry are skipped.
+    const bool solid_c = gc.lo == 0u && !water && !P.physics_water &&
+                         !(P.enable_x_fringe && i < 5 && k > A.D.nz / 2) &&
+                         !(P.enable_top_drive && k == A.D.nz - 1);
+    if (solid_c) {
+        f[0] = Store<S>::ld((const typename Store<S>::T *)A.fsrc, (size_t)c, 0, P.rho0);
+#pragma unroll
+        for (int q = 1; q < 19; ++q) f[q] = 0.0f;
+    } else if (IN == 0) {
         load_cell<S>(A, c, f);
     } else {
         GeoLinks Ls;
@@ -217,8 +232,6 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
         int cut = 0, fscut = 0, bridge = 0;
         stream_bc<S>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
     }
-    GeoLinks Lc;
-    Geo gc = geo_cell<CG>(P, A.slot, A.D, A.bed_c, k, j, i, Lc, true, P.use_link_wall_velocity && P.include_bed);
     fast_c = gc.fast;
     open = (gc.lo & 1u) != 0u;
     type = LBM_FS_LIQUID;

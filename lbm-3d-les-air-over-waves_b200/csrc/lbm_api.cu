@@ -124,10 +124,12 @@ static BedView slot_view(const lbm_ctx *ctx, int s) {
     return v;
 }
 
-// the column cache serves bed-only geometry: no cube, no phi geometry,
-// periodic x
+// the column cache serves bed-only geometry in air mode: no cube, no phi
+// geometry, periodic x, no free surface (the kernels that use it carry no
+// free-surface code)
 static bool wants_column_cache(const lbm_params &P) {
-    return P.include_bed && !P.include_cube && !P.use_phi_open_fraction && !P.use_phi_open_flags && !P.x_solid;
+    return P.include_bed && !P.include_cube && !P.use_phi_open_fraction && !P.use_phi_open_flags && !P.x_solid &&
+           !P.physics_water && P.fs_mode == LBM_FS_NONE;
 }
 static int refresh_column_cache(lbm_ctx *ctx, int s, cudaStream_t st) {
     if (!ctx->use_cg) return LBM_OK;

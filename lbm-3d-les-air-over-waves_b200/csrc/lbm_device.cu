@@ -176,6 +176,9 @@ __global__ void k_colgeo(lbm_params P, Dom D, BedView B, float *cg) {
 #ifndef LBM_GEN_MINB
 #define LBM_GEN_MINB 1
 #endif
+#ifndef LBM_CG_MINB
+#define LBM_CG_MINB 2
+#endif
 template <int S>
 __device__ __forceinline__ void load_cell(const StepArgs &A, int c, float f[19]) {
     const typename Store<S>::T *src = (const typename Store<S>::T *)A.fsrc;
@@ -198,7 +201,9 @@ template <int S, int IN, bool CG>
 __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, int i, float f[19], bool &fast_c,
                                       bool &open, int &type, float &gbf, float &r, float &vx, float &vy, float &vz) {
     const lbm_params &P = A.P;
-    const bool water = P.fs_mode != LBM_FS_NONE;
+    // the column cache is used in air mode only: CG kernels carry no
+    // free-surface code
+    const bool water = !CG && P.fs_mode != LBM_FS_NONE;
     if (cell_fast(A, IN == 1, true, k, j, i)) {
         if (IN == 0) load_cell<S>(A, c, f);
         else stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
@@ -230,7 +235,7 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
         GeoLinks Ls;
         Geo gs = geo_cell<CG>(P, A.slot, A.D, A.bed_s, k, j, i, Ls, true, P.use_link_wall_velocity && P.include_bed);
         int cut = 0, fscut = 0, bridge = 0;
-        stream_bc<S>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
+        stream_bc<S, CG>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
     }
     fast_c = gc.fast;
     open = (gc.lo & 1u) != 0u;
@@ -246,7 +251,7 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
 }
 
 template <int S, int IN, bool CG>
-__global__ void __launch_bounds__(256, LBM_GEN_MINB) k_prepass(StepArgs A) {
+__global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_prepass(StepArgs A) {
     int i, j, k, c;
     if (!cell_xyz(A, i, j, k, c)) return;
     float f[19], r, vx, vy, vz, gbf;
@@ -259,7 +264,7 @@ __global__ void __launch_bounds__(256, LBM_GEN_MINB) k_prepass(StepArgs A) {
 }
 
 template <int S, int IN, bool CG>
-__global__ void __launch_bounds__(256, LBM_GEN_MINB) k_collide(StepArgs A) {
+__global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collide(StepArgs A) {
     int i, j, k, c;
     if (!cell_xyz(A, i, j, k, c)) return;
     float f[19], r, vx, vy, vz, gbf;
@@ -267,7 +272,7 @@ __global__ void __launch_bounds__(256, LBM_GEN_MINB) k_collide(StepArgs A) {
     bool fast_c, open;
     front<S, IN, CG>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
     const lbm_params &P = A.P;
-    const bool water = P.fs_mode != LBM_FS_NONE;
+    const bool water = !CG && P.fs_mode != LBM_FS_NONE;
     const bool gas = water && type == LBM_FS_GAS;
     if (A.flags & F_WRITE_MACRO) {
         A.rho[c] = r; A.ux[c] = vx; A.uy[c] = vy; A.uz[c] = vz;
@@ -289,7 +294,7 @@ __global__ void __launch_bounds__(256, LBM_GEN_MINB) k_collide(StepArgs A) {
 }
 
 template <int S, bool CG>
-__global__ void __launch_bounds__(256, LBM_GEN_MINB) k_stream(StepArgs A) {
+__global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream(StepArgs A) {
     int i, j, k, c;
     int cut = 0, fscut = 0, bridge = 0;
     if (cell_xyz(A, i, j, k, c)) {
@@ -300,9 +305,9 @@ __global__ void __launch_bounds__(256, LBM_GEN_MINB) k_stream(StepArgs A) {
         } else {
             GeoLinks Ls;
             Geo gs = geo_cell<CG>(A.P, A.slot, A.D, A.bed_s, k, j, i, Ls, true, A.P.use_link_wall_velocity && A.P.include_bed);
-            stream_bc<S>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
+            stream_bc<S, CG>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
             store_cell<S>(A, c, f);
-            if (A.P.fs_mode != LBM_FS_NONE) {
+            if (!CG && A.P.fs_mode != LBM_FS_NONE) {
                 // post-stream macro_step of the water path, CODEX.py:3897
                 int type;
                 float fill;

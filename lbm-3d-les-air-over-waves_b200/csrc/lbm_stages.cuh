@@ -138,14 +138,15 @@ LBM_DEV void stream_fast(const StepArgs &A, const typename Store<S>::T *__restri
 
 // ------------------------------------------------------------ stream + BC
 // post-stream populations of cell (k,j,i) from post-collision fs[]
-template <int S>
+// AIR: compiled for air mode only (no free-surface code in the kernel)
+template <int S, bool AIR = false>
 LBM_DEV void stream_bc(const StepArgs &A, const typename Store<S>::T *__restrict__ fs, const Geo &g,
                        const GeoLinks &L, int k, int j, int i, int c, float out[19], int &cut, int &fscut,
                        int &bridge) {
     const lbm_params &P = A.P;
     const Dom &D = A.D;
     const size_t n = D.n;
-    const bool water = P.fs_mode != LBM_FS_NONE;
+    const bool water = !AIR && P.fs_mode != LBM_FS_NONE;
     const bool vof = water && P.fs_tracking == LBM_TRACK_VOF;
     const float rho0 = P.rho0;
     const bool open_c = (g.lo & 1u) != 0u;

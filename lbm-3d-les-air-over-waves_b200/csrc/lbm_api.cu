@@ -227,6 +227,7 @@ static int bed_step(lbm_ctx *ctx, int64_t m, cudaStream_t st) {
 // cell below is fluid) and end below the top row.
 struct Plan {
     bool tile = false;
+    bool classic = false;   // unpipelined interior kernel even for FP32 (LBM_B200_TILE_KERNEL=classic)
     int zi0 = 0, zi1 = -1, chunk = 64;
     int zlo[3] = {0, 0, 0}, zcnt[3] = {0, 0, 0};
 };
@@ -252,6 +253,8 @@ static Plan plan_planes(const lbm_ctx *ctx) {
     if (zi0 < 1) zi0 = 1;
     if (zi1 < zi0) return R;
     R.tile = true;
+    const char *tk = getenv("LBM_B200_TILE_KERNEL");
+    R.classic = tk && strcmp(tk, "classic") == 0;
     R.zi0 = zi0;
     R.zi1 = zi1;
     // planes per block: enough blocks for ~4 waves of 2 blocks per SM, at
@@ -296,7 +299,8 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     A.bed_c = slot_view(ctx, (int)((n + 1) & 1));
     A.bed_s = A.bed_c;
     A.step = (uint64_t)(n + 1);
-    A.flags = (K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0;
+    const int tflag = R.classic ? F_TILE_CLASSIC : 0;
+    A.flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
     if (les) {
         launch_step_kernel(KER_PREPASS_CANON, A, st);
         CK_LAUNCH("prepass");
@@ -315,7 +319,7 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
         A.bed_s = slot_view(ctx, (int)(m & 1));
         A.bed_c = slot_view(ctx, (int)((m + 1) & 1));
         A.step = (uint64_t)(m + 1);
-        A.flags = (m + 1 == n + K) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0;
+        A.flags = ((m + 1 == n + K) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
         if (les) {
             launch_step_kernel(KER_PREPASS_FUSED, A, st);
             CK_LAUNCH("prepass fused");

@@ -900,6 +900,26 @@ void launch_hmax(const Dom &D, const float *h, float *hmax, cudaStream_t st) {
     k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax); LAUNCHED(1);
 }
 
+// the pipelined interior kernel takes more than 48 KB of shared memory:
+// raise the per-kernel limit once per device
+static bool pipe_smem_ready() {
+    static bool done[64] = {false}, ok[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    if (!done[dev]) {
+        done[dev] = true;
+        ok[dev] = cudaFuncSetAttribute(k_tile_pipe<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       PIPE_SMEM_BYTES) == cudaSuccess &&
+                  cudaFuncSetAttribute(k_tile_pipe<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       PIPE_SMEM_BYTES) == cudaSuccess &&
+                  cudaFuncSetAttribute(k_tile_pipe<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       PIPE_SMEM_BYTES) == cudaSuccess &&
+                  cudaFuncSetAttribute(k_tile_pipe<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       PIPE_SMEM_BYTES) == cudaSuccess;
+    }
+    return ok[dev];
+}
+
 template <int S>
 static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) {
     dim3 g = grid3(A);
@@ -913,6 +933,9 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
     const bool les = A.P.use_les != 0;
     // the column cache is set on both bed views or on neither
     const bool cg = A.bed_s.cg != nullptr && A.bed_c.cg != nullptr;
+    // pipelined interior kernel: FP32 populations, 32-bit population indices
+    const bool pipe = tile_kernel && S == LBM_STORE_F32 && !(A.flags & F_TILE_CLASSIC) &&
+                      19.0 * (double)A.D.n < 2147483647.0 && pipe_smem_ready();
     switch (which) {
         case KER_PREPASS_CANON:
             if (cg) k_prepass<S, 0, true><<<g, kBlock3, 0, st>>>(A);
@@ -940,12 +963,24 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
             LAUNCHED(1);
             break;
         case KER_TILE_CANON:
-            if (les) { k_tile<S, 0, true><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }
-            else { k_tile<S, 0, false><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }
+            if (pipe) {
+                if (les) k_tile_pipe<0, true><<<gt, 256, PIPE_SMEM_BYTES, st>>>(A);
+                else k_tile_pipe<0, false><<<gt, 256, PIPE_SMEM_BYTES, st>>>(A);
+            } else {
+                if (les) k_tile<S, 0, true><<<gt, 256, 0, st>>>(A);
+                else k_tile<S, 0, false><<<gt, 256, 0, st>>>(A);
+            }
+            LAUNCHED(1);
             break;
         case KER_TILE_FUSED:
-            if (les) { k_tile<S, 1, true><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }
-            else { k_tile<S, 1, false><<<gt, 256, 0, st>>>(A); LAUNCHED(1); }
+            if (pipe) {
+                if (les) k_tile_pipe<1, true><<<gt, 256, PIPE_SMEM_BYTES, st>>>(A);
+                else k_tile_pipe<1, false><<<gt, 256, PIPE_SMEM_BYTES, st>>>(A);
+            } else {
+                if (les) k_tile<S, 1, true><<<gt, 256, 0, st>>>(A);
+                else k_tile<S, 1, false><<<gt, 256, 0, st>>>(A);
+            }
+            LAUNCHED(1);
             break;
         case KER_STREAM_INTERIOR: { k_stream_interior<S><<<gs, 256, 0, st>>>(A); LAUNCHED(1); } break;
         default: break;

@@ -13,6 +13,7 @@ enum : int {
     F_WRITE_ALL_OMEGA = 2,  // store omega for every active cell (else near-wall band only)
     F_COUNT = 4,            // count cut / free-surface / bridge links in stream
     F_VOF_STATE = 8,        // free-surface state from stored type/fill (else from column height)
+    F_TILE_CLASSIC = 16,    // interior planes: the unpipelined tile kernel even for FP32
 };
 
 enum {

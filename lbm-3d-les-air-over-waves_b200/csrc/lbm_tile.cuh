@@ -215,6 +215,192 @@ __global__ void __launch_bounds__(256, 2) k_tile(StepArgs A) {
     }
 }
 
+// ------------------------------------------------- pipelined interior kernel
+// k_tile_pipe: k_tile for FP32 populations with the gathers of plane p + 2
+// in flight while plane p is worked on.  Each thread copies its own cell's
+// 19 pulled populations (and 4-5 ring items) straight into shared memory
+// with cp.async (4-byte copies, no registers held), in a ring of 3 plane
+// slots; a commit group per plane keeps the waits in order.  Per-column
+// work is hoisted out of the z loop: source offsets, the ring items'
+// addresses, and the far-from-the-bed check (monotone in k, so the lowest
+// plane of the chunk decides).  Arithmetic, and so every result, is that of
+// k_tile.
+constexpr int PIPE_SLOTS = 3;
+constexpr int PIPE_SMEM_FLOATS =
+    PIPE_SLOTS * 19 * 256 + PIPE_SLOTS * 19 * 64 + 3 * 3 * (LBM_TILE + 2) * (LBM_TILE + 2);
+constexpr int PIPE_SMEM_BYTES = PIPE_SMEM_FLOATS * 4;
+
+LBM_DEV void cp_async4(float *smem, const float *gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+LBM_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+LBM_DEV void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int IN, bool LES>
+__global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
+    extern __shared__ __align__(16) float smem[];
+    float *sf = smem;                                   // [slot][q][256] own-cell populations
+    float *sr = smem + PIPE_SLOTS * 19 * 256;           // [slot][q][64] ring populations
+    float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =        // [plane slot][component][y][x]
+        (float (*)[3][LBM_TILE + 2][LBM_TILE + 2])(sr + PIPE_SLOTS * 19 * 64);
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    const int i = blockIdx.x * LBM_TILE + tx, j = blockIdx.y * LBM_TILE + ty;
+    const int z0 = A.zi0 + blockIdx.z * A.chunk;
+    const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
+    const int n = (int)D.n, nxy = D.nx * D.ny;
+    const float *fsrc = (const float *)A.fsrc;
+    float *fdst = (float *)A.fdst;
+
+    // far-from-the-bed precondition of this column (status bit 1)
+    {
+        const int kc = max(z0, A.zi0);
+        bool ok = geo_far(P, D, A.bed_c, kc, j, i) && (IN == 0 || geo_far(P, D, A.bed_s, kc, j, i));
+        if (z0 == A.zi0)
+            ok = ok && geo_far(P, D, A.bed_c, z0 - 1, j, i) && (IN == 0 || geo_far(P, D, A.bed_s, z0 - 1, j, i));
+        if (!ok) atomicOr(A.status, 2u);
+    }
+    // neighbour offsets of the pull gather (periodic x and y)
+    const int col = j * D.nx + i;
+    const int xm = (i == 0) ? D.nx - 1 : -1, xp = (i + 1 == D.nx) ? 1 - D.nx : 1;
+    const int ym = (j == 0) ? (D.ny - 1) * D.nx : -D.nx, yp = (j + 1 == D.ny) ? (1 - D.ny) * D.nx : D.nx;
+    // ring items of this thread: ring cell r = t & 63, q = (t >> 6) + 4u
+    int rx = 0, ry = 0;
+    ring_cell(t & 63, rx, ry);
+    const int ri = (blockIdx.x * LBM_TILE + rx + D.nx) % D.nx;
+    const int rj = (blockIdx.y * LBM_TILE + ry + D.ny) % D.ny;
+    int roff[5];
+#pragma unroll
+    for (int u = 0; u < 5; ++u) {
+        const int q = (t >> 6) + 4 * u;
+        int si = ri, sj = rj, dz = 0;
+        if (q < 19) {
+            if (IN == 1) {
+                si -= c_tile_cx[q];
+                sj -= c_tile_cy[q];
+                dz = -c_tile_cz[q];
+            }
+            si = si < 0 ? si + D.nx : (si >= D.nx ? si - D.nx : si);
+            sj = sj < 0 ? sj + D.ny : (sj >= D.ny ? sj - D.ny : sj);
+        }
+        roff[u] = q * n + dz * nxy + sj * D.nx + si;
+    }
+    const bool ring = LES && t < 64;
+
+    // copies of plane p into slot p % 3 (own cell, and the ring with LES)
+    auto issue = [&](int p) {
+        if (p >= A.zi0 && p <= A.zi1 && p <= z1) {
+            const int slot = p % PIPE_SLOTS;
+            const int base = p * nxy + col;
+            float *dst = sf + slot * 19 * 256 + t;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                int off = 0;
+                if (IN == 1) {
+                    if (cxq(q) > 0) off += xm; else if (cxq(q) < 0) off += xp;
+                    if (cyq(q) > 0) off += ym; else if (cyq(q) < 0) off += yp;
+                    if (czq(q) > 0) off -= nxy; else if (czq(q) < 0) off += nxy;
+                }
+                cp_async4(dst + q * 256, fsrc + (q * n + base + off));
+            }
+            if (LES) {
+                float *rdst = sr + slot * 19 * 64 + (t & 63);
+#pragma unroll
+                for (int u = 0; u < 5; ++u) {
+                    const int q = (t >> 6) + 4 * u;
+                    if (q < 19) cp_async4(rdst + q * 64, fsrc + (roff[u] + p * nxy));
+                }
+            }
+        }
+        cp_async_commit();
+    };
+
+    issue(z0 - 1);
+    issue(z0);
+    float fp[19];
+    float rp = 0.0f, vxp = 0.0f, vyp = 0.0f, vzp = 0.0f;
+    for (int p = z0 - 1; p <= z1; ++p) {
+        const int sl = p % 3;
+        const bool interior = p >= A.zi0 && p <= A.zi1;
+        cp_async_wait1();       // plane p has landed (p + 1 may still be in flight)
+        __syncthreads();        // ring items of plane p come from other threads
+        float fc[19];
+        float r = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
+        if (interior) {
+            const float *src = sf + sl * 19 * 256 + t;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) fc[q] = src[q * 256];
+        }
+        issue(p + 2);           // into the slot consumed before the barrier above
+        if (interior) {
+            macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
+            if (LES) {
+                su[sl][0][ty + 1][tx + 1] = vx;
+                su[sl][1][ty + 1][tx + 1] = vy;
+                su[sl][2][ty + 1][tx + 1] = vz;
+                if (ring) {
+                    const float *rs = sr + sl * 19 * 64 + t;
+                    float fr[19], rr, a, b, d;
+#pragma unroll
+                    for (int q = 0; q < 19; ++q) fr[q] = rs[q * 64];
+                    macro(P, D, fr, p, false, LBM_FS_LIQUID, 0.0f, rr, a, b, d);
+                    su[sl][0][ry + 1][rx + 1] = a;
+                    su[sl][1][ry + 1][rx + 1] = b;
+                    su[sl][2][ry + 1][rx + 1] = d;
+                }
+            }
+        } else if (LES) {
+            // plane handled by the general kernels: velocity from their pre-pass
+            const int c = p * nxy + col;
+            su[sl][0][ty + 1][tx + 1] = __ldg(A.u_les + c);
+            su[sl][1][ty + 1][tx + 1] = __ldg(A.u_les + n + c);
+            su[sl][2][ty + 1][tx + 1] = __ldg(A.u_les + 2 * n + c);
+            if (ring) {
+                const int cr = (p * D.ny + rj) * D.nx + ri;
+                su[sl][0][ry + 1][rx + 1] = __ldg(A.u_les + cr);
+                su[sl][1][ry + 1][rx + 1] = __ldg(A.u_les + n + cr);
+                su[sl][2][ry + 1][rx + 1] = __ldg(A.u_les + 2 * n + cr);
+            }
+        }
+        if (LES) __syncthreads();
+        const int k = p - 1;
+        if (k >= z0 && k < z1) {
+            const int c = k * nxy + col;
+            float om = P.omega0;
+            if (LES) {
+                const int sm = (p + 1) % 3, s0 = (p + 2) % 3, sp = sl;  // planes k-1, k, k+1
+                const int y = ty + 1, x = tx + 1;
+                om = les_interior(P, su[s0][0][y][x + 1], su[s0][0][y][x - 1], su[s0][0][y + 1][x],
+                                  su[s0][0][y - 1][x], su[sp][0][y][x], su[sm][0][y][x], su[s0][1][y][x + 1],
+                                  su[s0][1][y][x - 1], su[s0][1][y + 1][x], su[s0][1][y - 1][x], su[sp][1][y][x],
+                                  su[sm][1][y][x], su[s0][2][y][x + 1], su[s0][2][y][x - 1], su[s0][2][y + 1][x],
+                                  su[s0][2][y - 1][x], su[sp][2][y][x], su[sm][2][y][x]);
+                if (A.flags & F_WRITE_ALL_OMEGA) A.omega[c] = om;
+                if (k == A.zi0 || k == A.zi1) {
+                    // velocity of the interior planes next to the general ones,
+                    // for the general kernels' stencils
+                    A.u_out[c] = vxp;
+                    A.u_out[n + c] = vyp;
+                    A.u_out[2 * n + c] = vzp;
+                }
+            }
+            if (A.flags & F_WRITE_MACRO) {
+                A.rho[c] = rp; A.ux[c] = vxp; A.uy[c] = vyp; A.uz[c] = vzp;
+            }
+            if (!(rp == rp) || fabsf(rp) > 3.0e38f) atomicOr(A.status, 1u);
+            collide(A, c, k, false, false, false, 0.0f, rp, vxp, vyp, vzp, om, fp);
+#pragma unroll
+            for (int q = 0; q < 19; ++q) fdst[q * n + c] = fp[q];
+        }
+#pragma unroll
+        for (int q = 0; q < 19; ++q) fp[q] = fc[q];
+        rp = r; vxp = vx; vyp = vy; vzp = vz;
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // stream only (the last pass of a call) for interior cells
 template <int S>
 __global__ void __launch_bounds__(256) k_stream_interior(StepArgs A) {

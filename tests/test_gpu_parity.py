@@ -55,11 +55,11 @@ def test_gpu_matches_oracle_water_gaussian_benchmark_shape():
     assert not problems, "\n".join(problems[:20])
 
 
-@pytest.mark.parametrize("variant", ["les", "no_les", "kbc", "small_chunks"])
+@pytest.mark.parametrize("variant", ["les", "no_les", "kbc", "small_chunks", "classic", "classic_no_les"])
 def test_gpu_tile_path_matches_oracle(variant, monkeypatch):
     """nx, ny multiples of 16 and periodic x: interior planes run on the
-    tile kernel, the planes next to the bed and the top on the general
-    kernels."""
+    tile kernel (the pipelined one for FP32, or the classic one), the planes
+    next to the bed and the top on the general kernels."""
     env = air_wave_env(64, 32, 48, amp=3.0, level=6.0, wavelength=32.0)
     if variant == "no_les":
         env["LBM_USE_LES"] = "0"
@@ -67,6 +67,10 @@ def test_gpu_tile_path_matches_oracle(variant, monkeypatch):
         env["LBM_COLLISION"] = "kbc"
     elif variant == "small_chunks":
         monkeypatch.setenv("LBM_B200_TILE_CHUNK", "7")
+    if variant.startswith("classic"):
+        monkeypatch.setenv("LBM_B200_TILE_KERNEL", "classic")
+        if variant == "classic_no_les":
+            env["LBM_USE_LES"] = "0"
     problems = _run_pair(env, chunks=(1, 2, 6))
     assert not problems, "\n".join(problems[:20])
 

@@ -35,8 +35,6 @@ using namespace lbm;
 
 namespace {
 
-enum { CNT_CUT = 0, CNT_FSCUT = 1, CNT_BRIDGE = 2, CNT_FS_REFILL = 3, CNT_COALESCE = 4, CNT_VOF_EXCESS = 5,
-       CNT_ORPHAN = 6, CNT_COLLAPSE = 7, CNT_DET = 8, CNT_CMP = 9, CNT_SWEEPS = 10, CNT_N = 16 };
 
 // constant-memory parameter slots (LBM_MAX_SLOTS live contexts at a time)
 std::mutex g_slot_mutex;
@@ -73,6 +71,11 @@ struct lbm_ctx {
     float *bed_uw[2] = {nullptr, nullptr}, *bed_vw[2] = {nullptr, nullptr}, *bed_ww[2] = {nullptr, nullptr};
     float *bed_cg[2] = {nullptr, nullptr};  // per-column link-endpoint cache (bed-only geometry)
     bool use_cg = false;
+    // VOF scratch (VOF contexts only)
+    int8_t *v_open = nullptr, *v_t0 = nullptr, *v_ba = nullptr;
+    float *v_lf0 = nullptr, *v_m0 = nullptr, *v_x0 = nullptr, *v_fa = nullptr;
+    double *v_dd = nullptr, *v_tree = nullptr;
+    int *v_dist = nullptr;
     float *u_les = nullptr;
     int *dcount = nullptr;
     unsigned *dstatus = nullptr;
@@ -164,6 +167,30 @@ static InitArgs init_args(lbm_ctx *ctx, int slot) {
     I.fs_fill = b.fs_fill; I.fs_mass = b.fs_mass; I.fs_mass_excess = b.fs_mass_excess;
     I.fs_type = b.fs_type; I.fs_type_prev = b.fs_type_prev; I.fs_excess_dir = b.fs_excess_dir;
     return I;
+}
+
+static bool is_vof(const lbm_params &P) { return P.fs_mode != LBM_FS_NONE && P.fs_tracking == LBM_TRACK_VOF; }
+
+static VofArgs vof_args(lbm_ctx *ctx, int slot, void *f) {
+    VofArgs V;
+    memset(&V, 0, sizeof V);
+    const lbm_buffers &b = ctx->b;
+    V.P = ctx->P;
+    V.slot = ctx->slot;
+    V.D = ctx->D;
+    V.f = f;
+    V.type = b.fs_type; V.type_prev = b.fs_type_prev; V.excess_dir = b.fs_excess_dir;
+    V.fill = b.fs_fill; V.mass = b.fs_mass; V.mass_excess = b.fs_mass_excess;
+    V.rho = b.rho; V.ux = b.ux; V.uy = b.uy; V.uz = b.uz;
+    V.bed_h = ctx->bed_h[slot];
+    V.fs_h = b.fs_h; V.fs_h_last = b.fs_h_last;
+    V.open = ctx->v_open; V.lf0 = ctx->v_lf0;
+    V.m0 = ctx->v_m0; V.x0 = ctx->v_x0; V.t0 = ctx->v_t0;
+    V.fa = ctx->v_fa; V.ba = ctx->v_ba; V.dd = ctx->v_dd;
+    V.dist = ctx->v_dist;
+    V.count = ctx->dcount;
+    V.fcount = ctx->dfcount;
+    return V;
 }
 
 static StepArgs step_args(lbm_ctx *ctx) {
@@ -399,6 +426,52 @@ static int step_height(lbm_ctx *ctx, int K, cudaStream_t st) {
     return LBM_OK;
 }
 
+// VOF path: one step per iteration, the reference's order (CODEX.py:3873-3920)
+static int step_vof(lbm_ctx *ctx, int K, cudaStream_t st) {
+    const bool les = ctx->P.use_les != 0;
+    int s;
+    for (int it = 0; it < K; ++it) {
+        int64_t m = ctx->nstep + 1;
+        if ((s = bed_step(ctx, m, st)) != LBM_OK) return s;
+        const int slot = (int)(m & 1);
+        StepArgs A = step_args(ctx);
+        A.zlo[0] = 0;
+        A.zcnt[0] = ctx->P.nz;
+        A.bed_s = slot_view(ctx, slot);
+        A.bed_c = A.bed_s;
+        A.step = (uint64_t)m;
+        A.fsrc = ctx->b.f[ctx->cur];
+        A.fdst = ctx->b.f[1 - ctx->cur];
+        A.flags = F_WRITE_MACRO | F_WRITE_ALL_OMEGA | F_VOF_STATE;
+        VofArgs V = vof_args(ctx, slot, ctx->b.f[ctx->cur]);
+        launch_vof_open(V, A.bed_s, st);
+        CK_LAUNCH("vof open mask");
+        if (les) {
+            launch_step_kernel(KER_PREPASS_CANON, A, st);
+            CK_LAUNCH("prepass");
+        }
+        launch_step_kernel(KER_COLLIDE_CANON, A, st);
+        CK_LAUNCH("collide");
+        CK(cudaMemsetAsync(ctx->dcount, 0, 4 * sizeof(int), st), "counter reset");
+        A.fsrc = ctx->b.f[1 - ctx->cur];
+        A.fdst = ctx->b.f[ctx->cur];
+        A.flags = F_COUNT | F_VOF_STATE;
+        launch_step_kernel(KER_STREAM, A, st);
+        CK_LAUNCH("stream");
+        const bool due = ctx->P.vof_collapse_enabled && (m % ctx->P.vof_collapse_interval) == 0;
+        CK(vof_sequence(V, due, ctx->v_tree, st), "vof sequence");
+        A.flags = F_VOF_STATE;
+        A.fdst = ctx->b.f[ctx->cur];
+        launch_refill(A, ctx->b.fs_type_prev, ctx->dcount + CNT_FS_REFILL, st);
+        CK_LAUNCH("refill");
+        CK(cudaMemsetAsync(ctx->dcount + CNT_COALESCE, 0, sizeof(int), st), "counter reset");
+        launch_vof_coalesce(V, st);
+        CK_LAUNCH("coalescence repair");
+        ctx->nstep = m;
+    }
+    return LBM_OK;
+}
+
 extern "C" {
 
 const char *lbm_backend_name(void) { return "cuda-sm100a"; }
@@ -458,8 +531,6 @@ int lbm_bind(lbm_ctx *ctx, const lbm_buffers *bufs) {
         !b.piecewise_bed_z || !b.u_inlet_profile || !b.rho_initial || !b.init_noise || !b.fs_fill ||
         !b.fs_type || !b.fs_type_prev || !b.fs_mass || !b.fs_mass_excess || !b.fs_excess_dir)
         return fail(ctx, LBM_ERR_BAD_ARG, "lbm_bind: a required state buffer is NULL");
-    if (ctx->P.fs_mode != LBM_FS_NONE && ctx->P.fs_tracking == LBM_TRACK_VOF)
-        return fail(ctx, LBM_ERR_UNSUPPORTED, "VOF free-surface tracking is not available in this library build");
     ctx->b = b;
     if (!ctx->bound) {
         int s;
@@ -471,6 +542,17 @@ int lbm_bind(lbm_ctx *ctx, const lbm_buffers *bufs) {
                 return s;
         }
         if (ctx->P.use_les && (s = alloc(ctx, (void **)&ctx->u_les, 3 * ctx->D.n * sizeof(float)))) return s;
+        if (is_vof(ctx->P)) {
+            const size_t n = ctx->D.n;
+            const size_t nt = 6 * (n / 256 + 2);
+            if ((s = alloc(ctx, (void **)&ctx->v_open, n)) || (s = alloc(ctx, (void **)&ctx->v_t0, n)) ||
+                (s = alloc(ctx, (void **)&ctx->v_ba, 2 * n)) || (s = alloc(ctx, (void **)&ctx->v_lf0, 4 * n)) ||
+                (s = alloc(ctx, (void **)&ctx->v_m0, 4 * n)) || (s = alloc(ctx, (void **)&ctx->v_x0, 4 * n)) ||
+                (s = alloc(ctx, (void **)&ctx->v_fa, 24 * n)) || (s = alloc(ctx, (void **)&ctx->v_dd, 8 * n)) ||
+                (s = alloc(ctx, (void **)&ctx->v_tree, 8 * nt)) || (s = alloc(ctx, (void **)&ctx->v_dist, 4 * n)))
+                return s;
+            CK(cudaMemset(ctx->v_dist, 0xff, 4 * n), "memset");
+        }
         if (wants_column_cache(ctx->P)) {
             for (int i = 0; i < 2; ++i)
                 if ((s = alloc(ctx, (void **)&ctx->bed_cg[i], (size_t)CG_N * A))) return s;
@@ -517,6 +599,8 @@ int lbm_init_geometry(lbm_ctx *ctx, void *stream) {
     CK(cudaMemsetAsync(ctx->b.f[1], 0, pop_bytes, st), "memset f");
     CK(cudaMemsetAsync(ctx->dcount, 0, CNT_N * sizeof(int), st), "memset counters");
     CK(cudaMemsetAsync(ctx->dstatus, 0, sizeof(unsigned), st), "memset status");
+    CK(cudaMemsetAsync(ctx->dfcount, 0, 8 * sizeof(float), st), "memset counters");
+    if (ctx->v_dist) CK(cudaMemsetAsync(ctx->v_dist, 0xff, ctx->D.n * sizeof(int), st), "memset exterior");
     // update_wave_bed_and_velocities(0.0): previous height = initial level
     launch_bed(ctx->P, ctx->D, ctx->b.water_h, ctx->bed_h[0], ctx->bed_hmax[0], ctx->bed_uw[0], ctx->bed_vw[0],
                ctx->bed_ww[0], ctx->b.piecewise_bed_z, 0.0f, st);
@@ -546,6 +630,18 @@ int lbm_init_fields(lbm_ctx *ctx, void *stream) {
     launch_init_fields(I, st);
     CK_LAUNCH("init fields");
     ctx->cur = 1 - ctx->cur;  // copy_post_and_swap, CODEX.py:3789
+    if (is_vof(ctx->P)) {
+        // CODEX.py:3790-3792
+        const int slot = (int)(ctx->nstep & 1);
+        VofArgs V = vof_args(ctx, slot, ctx->b.f[ctx->cur]);
+        launch_vof_open(V, slot_view(ctx, slot), st);
+        CK_LAUNCH("vof open mask");
+        launch_vof_mass_init(I, st);
+        CK_LAUNCH("vof mass");
+        CK(vof_interface_layer(V, st), "vof interface layer");
+        launch_vof_height(V, st);
+        CK_LAUNCH("vof height");
+    }
     return LBM_OK;
 }
 
@@ -559,6 +655,7 @@ int lbm_step(lbm_ctx *ctx, int32_t nsteps, void *stream) {
     int64_t n0 = ctx->nstep;
     if ((s = load_bed_slot(ctx, (int)(n0 & 1), st)) != LBM_OK) return s;
     if (ctx->P.fs_mode == LBM_FS_NONE) s = step_air(ctx, nsteps, st);
+    else if (is_vof(ctx->P)) s = step_vof(ctx, nsteps, st);
     else s = step_height(ctx, nsteps, st);
     if (s != LBM_OK) return s;
     int64_t n1 = ctx->nstep;
@@ -585,8 +682,14 @@ int lbm_export_diagnostics(lbm_ctx *ctx, void *stream) {
     E.types_are_prev = ctx->nstep > 0 ? 1 : 0;
     launch_export(I, E, st);
     CK_LAUNCH("export");
-    if (ctx->b.vof_exterior_gas)
-        CK(cudaMemsetAsync(ctx->b.vof_exterior_gas, 0, ctx->D.n * sizeof(int32_t), st), "memset exterior");
+    if (ctx->b.vof_exterior_gas) {
+        if (ctx->v_dist) {
+            launch_vof_exterior(ctx->D, ctx->v_dist, ctx->b.vof_exterior_gas, st);
+            CK_LAUNCH("exterior labels");
+        } else {
+            CK(cudaMemsetAsync(ctx->b.vof_exterior_gas, 0, ctx->D.n * sizeof(int32_t), st), "memset exterior");
+        }
+    }
     return LBM_OK;
 }
 

@@ -28,6 +28,7 @@
 #include "lbm_launch.h"
 #include "lbm_stages.cuh"
 #include "lbm_tile.cuh"
+#include "lbm_vof.cuh"
 
 namespace lbm {
 
@@ -1048,6 +1049,156 @@ void launch_vof_mass_init(const InitArgs &I, cudaStream_t st) {
 }
 void launch_export(const InitArgs &I, const ExportArgs &E, cudaStream_t st) {
     k_export<<<blocks_for(I.D.n, 256), 256, 0, st>>>(I, E); LAUNCHED(1);
+}
+
+}  // namespace lbm
+
+// ------------------------------------------------------------ VOF launchers
+namespace lbm {
+
+static inline unsigned vblocks(const VofArgs &V) { return blocks_for(V.D.n, 256); }
+
+void launch_vof_open(const VofArgs &V, const BedView &B, cudaStream_t st) {
+    k_vof_open<<<vblocks(V), 256, 0, st>>>(V, B); LAUNCHED(1);
+}
+
+// FP64 tree over len values: returns the device address of the sum
+static const double *tree_reduce(const double *in, long long len, double *ping, double *pong, cudaStream_t st) {
+    const double *cur = in;
+    double *bufs[2] = {ping, pong};
+    int b = 0;
+    while (len > 1) {
+        const long long nb = (len + 255) / 256;
+        k_tree_level<<<(unsigned)nb, 256, 0, st>>>(cur, len, bufs[b]); LAUNCHED(1);
+        cur = bufs[b];
+        b ^= 1;
+        len = nb;
+    }
+    return cur;
+}
+
+static cudaError_t vof_snapshot(const VofArgs &V, const float *a, float *a0, const float *b, float *b0, bool types,
+                                cudaStream_t st) {
+    const size_t n = V.D.n;
+    cudaError_t e = cudaSuccess;
+    if (a && e == cudaSuccess) e = cudaMemcpyAsync(a0, a, n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    if (b && e == cudaSuccess) e = cudaMemcpyAsync(b0, b, n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    if (types && e == cudaSuccess) e = cudaMemcpyAsync(V.t0, V.type, n, cudaMemcpyDeviceToDevice, st);
+    return e;
+}
+
+static cudaError_t vof_redistribute(const VofArgs &V, cudaStream_t st) {
+    cudaError_t e = vof_snapshot(V, V.mass, V.m0, V.mass_excess, V.x0, false, st);
+    if (e != cudaSuccess) return e;
+    k_vof_redist_donor<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
+    k_vof_redist_recv<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
+    return cudaGetLastError();
+}
+static void vof_finalize(const VofArgs &V, int *cnt, cudaStream_t st) {
+    k_vof_finalize<<<vblocks(V), 256, 0, st>>>(V, cnt); LAUNCHED(1);
+}
+cudaError_t vof_interface_layer(const VofArgs &V, cudaStream_t st) {
+    cudaError_t e = vof_snapshot(V, nullptr, nullptr, nullptr, nullptr, true, st);
+    if (e != cudaSuccess) return e;
+    k_vof_interface_layer<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
+    return cudaGetLastError();
+}
+void launch_vof_height(const VofArgs &V, cudaStream_t st) {
+    k_vof_height<<<blocks_for(V.D.a, 128), 128, 0, st>>>(V); LAUNCHED(1);
+}
+
+// the VOF part of one step after the stream and its macro step
+// (CODEX.py:3898-3917), up to the column height; refill and coalescence
+// repair follow in the caller
+cudaError_t vof_sequence(const VofArgs &V, bool collapse_due, double *tree, cudaStream_t st) {
+    cudaError_t e;
+    const size_t n = V.D.n;
+    int *cnt = V.count;
+    // counters of this step (the reference resets them in these kernels)
+    if ((e = cudaMemsetAsync(cnt + CNT_VOF_EXCESS, 0, 5 * sizeof(int), st)) != cudaSuccess) return e;  // excess..cmp
+    if ((e = cudaMemsetAsync(V.fcount, 0, 7 * sizeof(float), st)) != cudaSuccess) return e;
+    switch (V.P.pop_storage) {
+        case LBM_STORE_F16S: k_vof_exchange<LBM_STORE_F16S><<<vblocks(V), 256, 0, st>>>(V); break;
+        case LBM_STORE_BF16S: k_vof_exchange<LBM_STORE_BF16S><<<vblocks(V), 256, 0, st>>>(V); break;
+        default: k_vof_exchange<LBM_STORE_F32><<<vblocks(V), 256, 0, st>>>(V); break;
+    }
+    LAUNCHED(1);
+    k_vof_apply<<<vblocks(V), 256, 0, st>>>(V, cnt + CNT_VOF_EXCESS); LAUNCHED(1);
+    for (int r = 0; r < 3; ++r) {
+        if ((e = vof_redistribute(V, st)) != cudaSuccess) return e;
+        vof_finalize(V, cnt + CNT_VOF_EXCESS, st);
+    }
+    if ((e = vof_interface_layer(V, st)) != cudaSuccess) return e;
+    // orphans: snapshots of mass, fill and type
+    if ((e = vof_snapshot(V, V.mass, V.m0, V.fill, V.x0, true, st)) != cudaSuccess) return e;
+    k_vof_orphan_donor<<<vblocks(V), 256, 0, st>>>(V, cnt + CNT_ORPHAN); LAUNCHED(1);
+    k_vof_orphan_recv<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
+    double *ping = tree, *pong = tree + (n / 256 + 2);
+    if (V.P.vof_detached_advection) {
+        k_vof_detached_donor<<<vblocks(V), 256, 0, st>>>(V, 0, cnt + CNT_DET); LAUNCHED(1);
+        k_vof_detached_apply<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
+        k_store_sum<<<1, 1, 0, st>>>(tree_reduce(V.dd, (long long)n, ping, pong, st), V.fcount + 5); LAUNCHED(1);
+    }
+    vof_finalize(V, cnt + CNT_VOF_EXCESS, st);
+    if (V.P.vof_detached_advection && V.P.vof_detached_residual_fill_threshold > 0.0f) {
+        k_vof_detached_donor<<<vblocks(V), 256, 0, st>>>(V, 1, cnt + CNT_CMP); LAUNCHED(1);
+        k_vof_detached_apply<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
+        k_store_sum<<<1, 1, 0, st>>>(tree_reduce(V.dd, (long long)n, ping, pong, st), V.fcount + 6); LAUNCHED(1);
+    }
+    vof_finalize(V, cnt + CNT_VOF_EXCESS, st);
+    if ((e = vof_redistribute(V, st)) != cudaSuccess) return e;
+    vof_finalize(V, cnt + CNT_VOF_EXCESS, st);
+    if ((e = vof_interface_layer(V, st)) != cudaSuccess) return e;
+    if (collapse_due) {
+        // exterior marks: capped 6-connected flood from the top row
+        if ((e = cudaMemsetAsync(cnt + CNT_SWEEPS, 0, sizeof(int), st)) != cudaSuccess) return e;
+        k_vof_flood_seed<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
+        const int S = V.P.vof_collapse_flood_sweeps;
+        const int batch = 16;
+        for (int s0 = 0; s0 < S; s0 += batch) {
+            const int s1 = s0 + batch < S ? s0 + batch : S;
+            for (int s = s0; s < s1; ++s) {
+                k_vof_flood_level<<<vblocks(V), 256, 0, st>>>(V, s, cnt + CNT_SWEEPS); LAUNCHED(1);
+            }
+            int reached = 0;
+            if ((e = cudaMemcpyAsync(&reached, cnt + CNT_SWEEPS, sizeof(int), cudaMemcpyDeviceToHost, st)) !=
+                cudaSuccess)
+                return e;
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+            if (reached < s1) break;   // a level of this batch added nothing: the flood is complete
+        }
+        // FP64 sums of trapped mass, trapped volume and exterior capacity
+        const long long nb = (long long)((n + 255) / 256);
+        double *lm = tree + 2 * (n / 256 + 2), *lv = tree + 3 * (n / 256 + 2), *lc = tree + 4 * (n / 256 + 2);
+        double *tp = tree + 5 * (n / 256 + 2);
+        k_vof_collapse_sums<<<(unsigned)nb, 256, 0, st>>>(V, lm, lv, lc); LAUNCHED(1);
+        // reduce each partial array; results are copied to three fixed slots
+        double *res = tp;   // tp[0..2]
+        const double *rm = tree_reduce(lm, nb, ping, pong, st);
+        if ((e = cudaMemcpyAsync(res + 0, rm, sizeof(double), cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+        const double *rv = tree_reduce(lv, nb, ping, pong, st);
+        if ((e = cudaMemcpyAsync(res + 1, rv, sizeof(double), cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+        const double *rc = tree_reduce(lc, nb, ping, pong, st);
+        if ((e = cudaMemcpyAsync(res + 2, rc, sizeof(double), cudaMemcpyDeviceToDevice, st)) != cudaSuccess) return e;
+        k_vof_collapse_decide<<<1, 1, 0, st>>>(res + 0, res + 1, res + 2, V.P.vof_collapse_max_volume_m3, V.fcount);
+        LAUNCHED(1);
+        k_vof_collapse_apply<<<vblocks(V), 256, 0, st>>>(V, cnt + CNT_COLLAPSE); LAUNCHED(1);
+    }
+    if ((e = vof_interface_layer(V, st)) != cudaSuccess) return e;
+    launch_vof_height(V, st);
+    return cudaGetLastError();
+}
+
+void launch_vof_coalesce(const VofArgs &V, cudaStream_t st) {
+    switch (V.P.pop_storage) {
+        case LBM_STORE_F16S: k_vof_coalesce<LBM_STORE_F16S><<<vblocks(V), 256, 0, st>>>(V, V.count + CNT_COALESCE); break;
+        case LBM_STORE_BF16S: k_vof_coalesce<LBM_STORE_BF16S><<<vblocks(V), 256, 0, st>>>(V, V.count + CNT_COALESCE); break;
+        default: k_vof_coalesce<LBM_STORE_F32><<<vblocks(V), 256, 0, st>>>(V, V.count + CNT_COALESCE); break;
+    }
+    LAUNCHED(1);
+}
+void launch_vof_exterior(const Dom &D, const int *dist, int32_t *out, cudaStream_t st) {
+    k_vof_exterior<<<blocks_for(D.n, 256), 256, 0, st>>>((int)D.n, dist, out); LAUNCHED(1);
 }
 
 }  // namespace lbm

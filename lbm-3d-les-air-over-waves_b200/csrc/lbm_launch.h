@@ -20,6 +20,9 @@ enum {
     KER_PREPASS_CANON = 0, KER_PREPASS_FUSED = 1, KER_COLLIDE_CANON = 2, KER_COLLIDE_FUSED = 3, KER_STREAM = 4,
     KER_TILE_CANON = 5, KER_TILE_FUSED = 6, KER_STREAM_INTERIOR = 7
 };
+// device counters of a context (int slots)
+enum { CNT_CUT = 0, CNT_FSCUT = 1, CNT_BRIDGE = 2, CNT_FS_REFILL = 3, CNT_COALESCE = 4, CNT_VOF_EXCESS = 5,
+       CNT_ORPHAN = 6, CNT_COLLAPSE = 7, CNT_DET = 8, CNT_CMP = 9, CNT_SWEEPS = 10, CNT_N = 16 };
 #define LBM_TILE 16   // interior tile edge (x and y); the tile path needs nx, ny multiples of it
 
 struct StepArgs {
@@ -63,6 +66,29 @@ struct InitArgs {
     int8_t *fs_type, *fs_type_prev, *fs_excess_dir;
 };
 
+// state and scratch of the VOF kernels
+struct VofArgs {
+    lbm_params P;
+    int slot;
+    Dom D;
+    void *f;                          // populations after the stream (read/written in place)
+    int8_t *type, *type_prev, *excess_dir;
+    float *fill, *mass, *mass_excess;
+    float *rho, *ux, *uy, *uz;
+    const float *bed_h;               // bed height of the step
+    float *fs_h, *fs_h_last;
+    int8_t *open;                     // lattice_open[0] of the step's geometry
+    float *lf0;                       // lattice_open_frac[0]
+    float *m0, *x0;                   // snapshots: mass, and excess or fill
+    int8_t *t0;                       // snapshot: type
+    float *fa;                        // 6 n floats
+    int8_t *ba;                       // 2 n bytes
+    double *dd;                       // n doubles
+    int *dist;                        // flood-fill distance of the last collapse pass (-1: not reached)
+    int *count;                       // integer counters (CNT_*)
+    float *fcount;                    // float counters
+};
+
 struct ExportArgs {
     float *phi;
     int32_t *obstacle, *near_obstacle;
@@ -94,5 +120,12 @@ void launch_vof_block(const InitArgs &I, cudaStream_t st);
 void launch_init_fields(const InitArgs &I, cudaStream_t st);
 void launch_vof_mass_init(const InitArgs &I, cudaStream_t st);
 void launch_export(const InitArgs &I, const ExportArgs &E, cudaStream_t st);
+
+void launch_vof_open(const VofArgs &V, const BedView &B, cudaStream_t st);
+cudaError_t vof_interface_layer(const VofArgs &V, cudaStream_t st);
+void launch_vof_height(const VofArgs &V, cudaStream_t st);
+cudaError_t vof_sequence(const VofArgs &V, bool collapse_due, double *tree, cudaStream_t st);
+void launch_vof_coalesce(const VofArgs &V, cudaStream_t st);
+void launch_vof_exterior(const Dom &D, const int *dist, int32_t *out, cudaStream_t st);
 
 }  // namespace lbm

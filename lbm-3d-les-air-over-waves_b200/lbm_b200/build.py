@@ -21,7 +21,7 @@ INCLUDE = os.path.join(REPO, "include")
 OUT_DIR = os.path.join(PKG, "_native")
 LIB = os.path.join(OUT_DIR, "liblbm_b200.so")
 SOURCES = ["lbm_api.cu", "lbm_device.cu"]
-HEADERS = ["lbm_dev.cuh", "lbm_geom.cuh", "lbm_stages.cuh", "lbm_tile.cuh", "lbm_launch.h"]
+HEADERS = ["lbm_dev.cuh", "lbm_geom.cuh", "lbm_stages.cuh", "lbm_tile.cuh", "lbm_vof.cuh", "lbm_launch.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -10,10 +10,15 @@ STATE = ["rho", "ux", "uy", "uz", "omega", "water_h", "water_h_last", "u_wave", 
          "fs_h_last", "fs_flux_x", "fs_flux_y", "u_inlet_profile", "fs_fill", "fs_type", "fs_type_prev",
          "fs_mass", "fs_mass_excess", "fs_excess_dir"]
 DIAG = ["phi", "obstacle", "near_obstacle", "lattice_open", "lattice_open_frac", "lattice_wall_type",
-        "pressure_reference_head", "gravity_body_fraction"]
+        "pressure_reference_head", "gravity_body_fraction", "vof_exterior_gas"]
 COUNTERS = ["boundary_cut_link_count", "free_surface_cut_link_count", "free_surface_thin_gap_bridge_count",
             "free_surface_refill_count", "free_surface_coalescence_repair_count", "free_surface_vof_excess_count",
-            "free_surface_vof_orphan_count", "free_surface_vof_collapse_cell_count", "step", "status_flags"]
+            "free_surface_vof_orphan_count", "free_surface_vof_collapse_cell_count",
+            "free_surface_vof_detached_advect_count", "free_surface_vof_detached_compress_count", "flood_sweeps_used",
+            "free_surface_vof_collapse_candidate_volume_m3", "free_surface_vof_collapse_applied_volume_m3",
+            "free_surface_vof_collapse_removal_scale", "free_surface_vof_collapse_candidate_mass",
+            "free_surface_vof_collapse_exterior_capacity", "free_surface_vof_detached_advect_mass",
+            "free_surface_vof_detached_compress_mass", "step", "status_flags"]
 
 
 def gpu_f32(dom, name):

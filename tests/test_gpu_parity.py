@@ -11,13 +11,13 @@ import pytest
 
 from golden_compare import load_golden
 from gpu_compare import compare_states
-from lbm_b200.config import air_wave_env, water_gaussian_env
+from lbm_b200.config import air_wave_env, vof_block_env, water_gaussian_env
 from oracle_runner import OracleSim
 
 pytestmark = pytest.mark.gpu
 
 GOLDEN_ENVS = ["air_kbc_default", "air_regularized_sine", "air_bed_cube_solidx", "air_phi_geometry",
-               "water_height_gaussian", "water_height_solitary"]
+               "water_height_gaussian", "water_height_solitary", "vof_block_kbc", "vof_gaussian_directional"]
 
 
 def _run_pair(env, chunks=(1, 3, 4)):
@@ -52,6 +52,15 @@ def test_gpu_matches_oracle_air_wave_benchmark_shape():
 def test_gpu_matches_oracle_water_gaussian_benchmark_shape():
     problems = _run_pair(water_gaussian_env(48, 8, 24, depth=12.0, amp=3.0, sigma=6.0, g_lb=1e-3),
                          chunks=(1, 4, 7))
+    assert not problems, "\n".join(problems[:20])
+
+
+def test_gpu_matches_oracle_vof_block_benchmark_shape():
+    """The VOF falling-block configuration at a small size, FP32 storage,
+    with the trapped-gas collapse every 3 steps (flood fill, FP64 sums)."""
+    env = vof_block_env(32, 8, 40, storage="f32", depth=10.0, block=8.0, bottom=20.0)
+    env["LBM_VOF_COLLAPSE_INTERVAL"] = "3"
+    problems = _run_pair(env, chunks=(1, 3, 5))
     assert not problems, "\n".join(problems[:20])
 
 

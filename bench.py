@@ -380,12 +380,98 @@ def ours(args):
     return 0
 
 
+def _device_time(streams, fn):
+    """Device time of fn() whose work runs on `streams`: events on the
+    current stream bracket the work, joined through per-stream events."""
+    import torch
+
+    torch.cuda.synchronize()
+    cur = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(cur)
+    for st in streams:
+        st.wait_event(e0)
+    fn()
+    for st in streams:
+        ev = torch.cuda.Event()
+        ev.record(st)
+        cur.wait_event(ev)
+    e1.record(cur)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def batched(args):
+    """The batched ensemble: 96 seeded air-over-wave domains of uneven size,
+    shifted-FP16 populations by default, all stepped together."""
+    import torch
+
+    from lbm_b200.batch import Batch, stable_ensemble_envs
+
+    storage = args.storage or "f16s"
+    envs = stable_ensemble_envs(args.domains, seed=7, storage=storage)
+    b = Batch(envs, chunk=25)
+    K, W = args.steps, max(args.warmup, 3)
+    b.step(W)
+    b.synchronize()
+    ms = _device_time([d.stream for d in b.domains], lambda: b.step(K))
+    cells = b.cells
+    bytes_cell = 76 if storage != "f32" else 152
+    line = {
+        "metric": METRIC, "value": cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": 1, "steps": K,
+        "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if storage == "f32" else f"f32 compute, {storage} storage", "data": "synthetic",
+        "mode": "batched",
+        "config": {"workload": f"batched ensemble of {len(envs)} air-over-wave domains (seed 7, stability-screened "
+                               f"draws), uneven sizes",
+                   "cells": cells, "storage": storage, "steps_per_call": b.chunk,
+                   "streams": len(envs)},
+        "roofline_step_frac": bytes_cell * cells * K / (ms * 1e-3) / (measured_hbm_peak()[0] * 1e9),
+    }
+    for d in b.domains:
+        if d.counters()["status_flags"]:
+            raise SystemExit("non-finite state in the batched run")
+    b.close()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def serving(args):
+    """The continuous-batching request loop on a seeded Poisson trace."""
+    from lbm_b200.serving import Server, poisson_trace
+
+    storage = args.storage or "f16s"
+    reqs = poisson_trace(args.requests, rate_hz=20.0, seed=3, cells_range=(1e5, 2e7),
+                         steps_range=(args.min_steps, args.max_steps), storage=storage)
+    rep = Server(budget_bytes=150e9, chunk=50).run(reqs)
+    line = {
+        "metric": "MLUPS (served trace)", "value": rep["mlups"], "unit": UNIT, "n_gpus": 1,
+        "higher_is_better": True, "mode": "serving", "data": "synthetic",
+        "p50_s": rep["p50_s"], "p99_s": rep["p99_s"], "wall_s": rep["wall_s"], "requests": rep["requests"],
+        "rounds": rep["rounds"], "peak_active": rep["peak_active"], "setup_s": rep["setup_s"],
+        "config": {"workload": "Poisson(20/s) arrivals, half air-over-wave, half water Gaussian, cells log-uniform "
+                               "[1e5, 2e7], seed 3", "steps_range": [args.min_steps, args.max_steps],
+                   "storage": storage, "hbm_budget_gb": 150, "round_steps": 50},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--mode", choices=("plain", "batched", "serving"), default="plain",
+                    help="plain: the 512x256x256 step (default); batched: the 96-domain ensemble; "
+                         "serving: the request loop on a Poisson trace")
+    ap.add_argument("--storage", choices=("f32", "f16s", "bf16s"), default=None,
+                    help="population storage of the batched and serving modes (default f16s)")
+    ap.add_argument("--domains", type=int, default=96, help="batched mode: ensemble size")
+    ap.add_argument("--requests", type=int, default=24, help="serving mode: trace length")
+    ap.add_argument("--min-steps", type=int, default=100, help="serving mode: fewest steps of a request")
+    ap.add_argument("--max-steps", type=int, default=600, help="serving mode: most steps of a request")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed CPU oracle sample")
     ap.add_argument("--size", type=str, default=None,
                     help="NXxNYxNZ: another domain size of the same workload (profiling of small cases)")
@@ -396,6 +482,10 @@ def main():
         WORKLOAD = f"air over moving wave, LES regularized, {NX}x{NY}x{NZ}, FP32 populations"
     if args.impl == "reference":
         return reference_arm(args)
+    if args.mode == "batched":
+        return batched(args)
+    if args.mode == "serving":
+        return serving(args)
     return ours(args)
 
 

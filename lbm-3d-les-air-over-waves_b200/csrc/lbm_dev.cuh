@@ -22,10 +22,12 @@ namespace lbm {
 
 // Solver constants of every live context, for device code that is not
 // inlined into a kernel (the near-wall paths).  Inlined code reads the
-// copy passed by value in the kernel arguments instead.
-#define LBM_MAX_SLOTS 64
+// copy passed by value in the kernel arguments instead.  Global memory
+// (cached reads), so that a process can hold many contexts at once
+// (batched ensembles, served requests).
+#define LBM_MAX_SLOTS 1024
 #ifdef LBM_DEVICE_TU
-__constant__ lbm_params c_params[LBM_MAX_SLOTS];
+__device__ lbm_params c_params[LBM_MAX_SLOTS];
 #endif
 
 // f32 constants of the collision kernels (CODEX.py:3165-3171, 3326-3328),

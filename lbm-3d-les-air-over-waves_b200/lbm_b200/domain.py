@@ -17,7 +17,7 @@ import numpy as np
 
 from . import abi, native, state
 from .config import SolverConfig, load_config
-from .hostinit import make_init_noise, prepare_initial_density
+from .hostinit import prepare_initial_density
 
 
 class Domain:
@@ -51,7 +51,12 @@ class Domain:
         return C.c_void_p(self.stream.cuda_stream)
 
     def initialize(self, noise=None, rho_initial=None):
-        """init sequence of main() (CODEX.py:3776-3792)."""
+        """init sequence of main() (CODEX.py:3776-3792).
+
+        noise: the uniform [-1, 1) kick of init_fields, shape (3, nz, ny, nx);
+        default: seeded (LBM_RANDOM_SEED) draws made on the device.
+        rho_initial: the initial density; default: rho0 in air, the host
+        prepare_initial_density_field restatement with a free surface."""
         import torch
 
         torch.cuda.synchronize(self.device)
@@ -59,11 +64,18 @@ class Domain:
         self.stream.synchronize()
         a = self.arrays
         if noise is None:
-            noise = make_init_noise(self.cfg)
-        if rho_initial is None:
-            rho_initial = prepare_initial_density(self.cfg, a["fs_h"].cpu().numpy(), a["water_h"].cpu().numpy())
-        a["init_noise"].copy_(torch.as_tensor(np.ascontiguousarray(noise)))
-        a["rho_initial"].copy_(torch.as_tensor(np.ascontiguousarray(rho_initial)))
+            # seeded uniform [-1, 1) draws made on the device
+            g = torch.Generator(device=self.device)
+            g.manual_seed(int(self.cfg.random_seed))
+            a["init_noise"].copy_(torch.rand(a["init_noise"].shape, generator=g, device=self.device) * 2.0 - 1.0)
+        else:
+            a["init_noise"].copy_(torch.as_tensor(np.ascontiguousarray(noise)))
+        if rho_initial is None and self.cfg.water_free_surface_enabled != 1:
+            a["rho_initial"].fill_(float(np.float32(self.cfg.rho0)))
+        else:
+            if rho_initial is None:
+                rho_initial = prepare_initial_density(self.cfg, a["fs_h"].cpu().numpy(), a["water_h"].cpu().numpy())
+            a["rho_initial"].copy_(torch.as_tensor(np.ascontiguousarray(rho_initial)))
         torch.cuda.synchronize(self.device)
         self._check(self.lib.lbm_init_fields(self.ctx, self._sp()), "lbm_init_fields")
         self.stream.synchronize()

@@ -1,0 +1,214 @@
+"""The solver module surface of LBM_3D_LES_air_over_waves_CODEX.py on top of
+the B200 engine, so that the reference's drivers use it as a drop-in.
+
+run_ab_case.py loads a solver file by path, sets `steps`, `plot_freq`,
+`plot_step_start` and `visualize`, and calls `main()`; its metrics read
+module globals, fields through `.to_numpy()` and counters through `[None]`
+(run_ab_case.py:261-280, 283-679, 899-912).  `install(namespace)` fills a
+module namespace with:
+
+  - the configuration globals, evaluated from the LBM_* environment at
+    import exactly as the reference evaluates them (dx, Nx, Ny, Nz, Lx_m ...,
+    x_phys/y_phys/z_phys, X_phys/Y_phys/Z_phys, vel_scale, rho0, U_ref_phys,
+    FS_GAS/FS_LIQUID/FS_INTERFACE, cube parameters, mode flags);
+  - field objects (rho, ux, uy, uz, obstacle, phi, water_h, free_surface_*,
+    pressure_reference_head, cx, cy, cz) whose to_numpy() returns the
+    current values in the reference's (Nz, Ny, Nx) layout;
+  - counter objects (boundary_cut_link_count, free_surface_* ...) read with
+    `[None]`;
+  - main(): the reference's initialisation and time loop (CODEX.py:3757-3954):
+    `visualize(step, time_phys, Re_phys_air, Re_lb_base)` every plot_freq
+    steps after plot_step_start, the health line every 100 steps.  Steps
+    between those events run as one call of the engine.
+
+The engine itself (buffers on the device, kernels) is created on first use.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+from .config import load_config
+
+D3Q19_CX = (0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0)
+D3Q19_CY = (0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, -1, 1)
+D3Q19_CZ = (0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1)
+
+# reference field name -> (engine buffer, dtype of the reference field, needs export_diagnostics)
+FIELDS = {
+    "rho": ("rho", np.float32, False), "ux": ("ux", np.float32, False), "uy": ("uy", np.float32, False),
+    "uz": ("uz", np.float32, False), "omega": ("omega", np.float32, False),
+    "water_h": ("water_h", np.float32, False), "water_h_last": ("water_h_last", np.float32, False),
+    "u_wave": ("u_wave", np.float32, False), "v_wave": ("v_wave", np.float32, False),
+    "w_wave": ("w_wave", np.float32, False),
+    "free_surface_h": ("fs_h", np.float32, False), "free_surface_h_last": ("fs_h_last", np.float32, False),
+    "free_surface_fill": ("fs_fill", np.float32, False), "free_surface_type": ("fs_type", np.int32, False),
+    "free_surface_type_prev": ("fs_type_prev", np.int32, False), "free_surface_mass": ("fs_mass", np.float32, False),
+    "free_surface_mass_excess": ("fs_mass_excess", np.float32, False),
+    "phi": ("phi", np.float32, True), "obstacle": ("obstacle", np.int32, True),
+    "near_obstacle": ("near_obstacle", np.int32, True), "lattice_open": ("lattice_open", np.int32, True),
+    "lattice_open_frac": ("lattice_open_frac", np.float32, True),
+    "pressure_reference_head": ("pressure_reference_head", np.float32, True),
+    "gravity_body_fraction": ("gravity_body_fraction", np.float32, True),
+    "free_surface_vof_exterior_gas": ("vof_exterior_gas", np.int32, True),
+}
+COUNTERS = (
+    "boundary_cut_link_count", "free_surface_cut_link_count", "boundary_refill_count", "free_surface_refill_count",
+    "free_surface_coalescence_repair_count", "free_surface_thin_gap_bridge_count", "free_surface_vof_excess_count",
+    "free_surface_vof_orphan_count", "free_surface_vof_collapse_cell_count",
+    "free_surface_vof_collapse_candidate_volume_m3", "free_surface_vof_collapse_applied_volume_m3",
+    "free_surface_vof_detached_advect_count", "free_surface_vof_detached_advect_mass",
+    "free_surface_vof_detached_compress_count", "free_surface_vof_detached_compress_mass",
+)
+
+
+class _Engine:
+    """Lazily created Domain shared by the field and counter views."""
+
+    def __init__(self, cfg):
+        self.cfg = cfg
+        self.dom = None
+        self.export_step = -1
+
+    def domain(self):
+        if self.dom is None:
+            from .domain import Domain
+
+            self.dom = Domain(self.cfg, device=os.environ.get("LBM_B200_DEVICE", "cuda:0"), with_diag=True,
+                              init=False)
+        return self.dom
+
+    def buffer(self, name, diag):
+        dom = self.domain()
+        if diag:
+            step = dom.counters()["step"]
+            if step != self.export_step:
+                dom.export_diagnostics()
+                self.export_step = step
+        dom.synchronize()
+        return dom.field(name)
+
+
+class Field:
+    """A reference field: to_numpy() gives the current values."""
+
+    def __init__(self, engine, name, buf, dtype, diag):
+        self._engine, self.name, self._buf, self._dtype, self._diag = engine, name, buf, dtype, diag
+
+    def to_numpy(self):
+        arr = self._engine.buffer(self._buf, self._diag).detach().cpu().numpy().astype(self._dtype)
+        if arr.ndim == 4 and arr.shape[0] == 19:
+            # per-link fields: the reference's ti.Vector.field(19) layout (Nz, Ny, Nx, 19)
+            arr = np.ascontiguousarray(np.moveaxis(arr, 0, -1))
+        return arr
+
+    @property
+    def shape(self):
+        return tuple(self._engine.domain().field(self._buf).shape)
+
+
+class _Const:
+    """A small constant field (the lattice vectors)."""
+
+    def __init__(self, values):
+        self._v = np.asarray(values, dtype=np.int32)
+
+    def to_numpy(self):
+        return self._v.copy()
+
+    def __getitem__(self, i):
+        return int(self._v[i])
+
+    @property
+    def shape(self):
+        return self._v.shape
+
+
+class Counter:
+    """A scalar counter of the reference, read as counter[None]."""
+
+    def __init__(self, engine, key):
+        self._engine, self._key = engine, key
+
+    def __getitem__(self, idx):
+        if idx is not None:
+            raise IndexError("scalar fields are indexed with [None]")
+        if self._engine.dom is None:
+            return 0
+        return self._engine.dom.counters()[self._key]
+
+
+def install(ns: dict, environ=None) -> None:
+    cfg = load_config(os.environ if environ is None else environ)
+    for k, v in cfg.values.items():
+        if not k.startswith("_"):
+            ns[k] = v
+    Nx, Ny, Nz, dx = cfg.Nx, cfg.Ny, cfg.Nz, cfg.dx
+    ns.update(dx=dx, Nx=Nx, Ny=Ny, Nz=Nz, rho0=cfg.rho0, FS_GAS=0, FS_LIQUID=1, FS_INTERFACE=2)
+    x_phys = (np.arange(Nx) + 0.5) * dx
+    y_phys = (np.arange(Ny) + 0.5) * dx
+    z_phys = (np.arange(Nz) + 0.5) * dx
+    Z_phys, Y_phys, X_phys = np.meshgrid(z_phys, y_phys, x_phys, indexing="ij")
+    ns.update(x_phys=x_phys, y_phys=y_phys, z_phys=z_phys, X_phys=X_phys, Y_phys=Y_phys, Z_phys=Z_phys)
+    ns.setdefault("Re_phys_air", cfg.Re_phys_air)
+    ns.setdefault("Re_lb_base", cfg.Re_lb_base)
+    eng = _Engine(cfg)
+    ns["_engine"] = eng
+    for name, (buf, dt, diag) in FIELDS.items():
+        ns[name] = Field(eng, name, buf, dt, diag)
+    ns["cx"], ns["cy"], ns["cz"] = _Const(D3Q19_CX), _Const(D3Q19_CY), _Const(D3Q19_CZ)
+    for key in COUNTERS:
+        ns[key] = Counter(eng, key)
+    ns.setdefault("visualize", lambda *a, **k: None)
+
+    def main():
+        """Initialisation and time loop of the reference (CODEX.py:3757-3954)."""
+        dom = eng.domain()
+        dom.initialize()
+        eng.export_step = -1
+        steps = int(ns["steps"])
+        plot_freq = max(1, int(ns["plot_freq"]))
+        plot_start = int(ns["plot_step_start"])
+        dt_phys = float(cfg.dt_phys)
+        step = 0
+        while step < steps:
+            # next step with an event: a plot, a health report, or the end
+            nxt = min(steps, (step // plot_freq + 1) * plot_freq, (step // 100 + 1) * 100)
+            dom.step(nxt - step)
+            step = nxt
+            time_phys = (step + 1) * dt_phys
+            if step % plot_freq == 0 and step > plot_start:
+                ns["visualize"](step, time_phys, ns["Re_phys_air"], ns["Re_lb_base"])
+            if step % 100 == 0:
+                _health(ns, dom, step)
+        print("Simulation Complete.")
+
+    ns["main"] = main
+
+
+def _health(ns, dom, step):
+    """The reference's periodic health line (CODEX.py:3930-3954)."""
+    ux, uy, uz = (ns[k].to_numpy() for k in ("ux", "uy", "uz"))
+    active = ns["obstacle"].to_numpy() == 0
+    if ns["water_free_surface_enabled"] == 1:
+        active &= ns["free_surface_type"].to_numpy() != 0
+    speed = np.sqrt(ux ** 2 + uy ** 2 + uz ** 2)
+    max_u = float(np.nanmax(speed[active])) if active.any() else float("nan")
+    c = dom.counters()
+    print(
+        f"Time Step {step}, Max |U| (LB units) = {max_u:.4f}, "
+        f"Max U (phys) ~ {max_u * ns['vel_scale']:.2f} m/s, "
+        f"cut_links={c['boundary_cut_link_count']}, refill={c['boundary_refill_count']}, "
+        f"fs_refill={c['free_surface_refill_count']}, fs_coalesce={c['free_surface_coalescence_repair_count']}, "
+        f"fs_bridge={c['free_surface_thin_gap_bridge_count']}, "
+        f"vof_excess={c['free_surface_vof_excess_count']}, "
+        f"vof_orphans={c['free_surface_vof_orphan_count']}, "
+        f"vof_detached={c['free_surface_vof_detached_advect_count']} "
+        f"({c['free_surface_vof_detached_advect_mass']:.3e}), "
+        f"vof_compact={c['free_surface_vof_detached_compress_count']} "
+        f"({c['free_surface_vof_detached_compress_mass']:.3e}), "
+        f"vof_collapse_cells={c['free_surface_vof_collapse_cell_count']}, "
+        f"vof_collapse_vol={c['free_surface_vof_collapse_applied_volume_m3']:.3f} m^3",
+        flush=True,
+    )

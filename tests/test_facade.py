@@ -1,0 +1,72 @@
+"""The drop-in solver module: loaded by path the way run_ab_case.py loads a
+solver (run_ab_case.py:261-280), driven through steps / plot_freq /
+plot_step_start / visualize / main() (899-912), read through module globals,
+.to_numpy() fields and [None] counters (283-679)."""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+MODULE = os.path.join(ROOT, "lbm-3d-les-air-over-waves_b200", "LBM_3D_LES_air_over_waves_B200.py")
+
+
+def _load(env, monkeypatch, label="t"):
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    spec = importlib.util.spec_from_file_location(f"lbm_ab_{label}", MODULE)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_module_surface_matches_the_reference_globals(monkeypatch):
+    from lbm_b200.config import air_wave_env
+
+    m = _load(air_wave_env(64, 16, 32), monkeypatch)
+    assert (m.Nx, m.Ny, m.Nz) == (64, 16, 32) and m.dx == 1.0
+    assert m.FS_GAS == 0 and m.FS_INTERFACE == 2
+    assert np.allclose(m.x_phys, (np.arange(64) + 0.5) * m.dx)
+    assert m.X_phys.shape == (32, 16, 64) and m.Z_phys[3, 0, 0] == 3.5
+    assert list(m.cx.to_numpy()) == [0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1, 0, 0, 0, 0]
+    assert m.boundary_cut_link_count[None] == 0
+    for name in ("Lx_m", "Ly_m", "Lz_m", "vel_scale", "U_ref_phys", "rho0", "rho_air_phys", "free_surface_base_m",
+                 "water_free_surface_enabled", "free_surface_tracking_mode", "x_boundary_mode",
+                 "use_hydrostatic_balanced_pressure", "use_component_balanced_pressure", "vof_empty_fill_threshold",
+                 "include_cube_geometry", "cube_side_m", "cube_yaw_sin", "cube_pitch_cos", "steps", "plot_freq",
+                 "plot_step_start", "Re_phys_air", "Re_lb_base", "gravity_phys"):
+        assert hasattr(m, name), name
+    assert callable(m.main) and callable(m.visualize)
+
+
+@pytest.mark.gpu
+def test_main_drives_the_engine_like_the_reference_loop(monkeypatch, capsys):
+    from lbm_b200.config import air_wave_env
+    from lbm_b200.domain import Domain
+
+    env = air_wave_env(64, 16, 32, amp=2.0, level=6.0, wavelength=32.0)
+    m = _load(env, monkeypatch, "main")
+    m.steps, m.plot_freq, m.plot_step_start = 120, 40, 0
+    seen = []
+
+    def visualize(step, time_phys, re_phys, re_lb):
+        seen.append((step, m.ux.to_numpy().copy(), m.obstacle.to_numpy().copy(), m.boundary_cut_link_count[None]))
+
+    m.visualize = visualize
+    m.main()
+    out = capsys.readouterr().out
+    assert [s[0] for s in seen] == [40, 80, 120]
+    assert "Time Step 100, Max |U|" in out and "Simulation Complete." in out
+    assert seen[-1][1].shape == (32, 16, 64) and seen[-1][2].dtype == np.int32
+    assert seen[-1][3] > 0
+    # the same 120 steps through the engine directly: identical fields
+    dom = Domain(env, device="cuda:0")
+    dom.step(40)
+    dom.step(40)
+    dom.step(40)
+    dom.synchronize()
+    a = dom.field("ux").cpu().numpy()
+    assert np.array_equal(a.view(np.uint32), seen[-1][1].view(np.uint32))
+    dom.close()
+    m._engine.dom.close()

@@ -198,6 +198,34 @@ __device__ __forceinline__ void store_cell(const StepArgs &A, int c, const float
 // post-stream state; IN = 1: stream + BC of the previous step from its
 // post-collision state.  Cells away from every wall and boundary take the
 // plain gather; the general path handles the rest.
+// Stream-stage class of a water cell on the height path: 1 = gas cell away
+// from every wall (stream_bc gives the rest equilibrium on every link),
+// 2 = cell whose 18 sources are all wet and in the domain, away from every
+// wall (stream_bc gives the plain gather), 0 = anything else.  Wet sources:
+// the lowest free-surface height over the 3x3 columns is more than 1.01
+// cells above the top source plane, so every source fill exceeds 1e-4.
+__device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int j, int i) {
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    if (P.fs_mode == LBM_FS_NONE || (A.flags & F_VOF_STATE)) return 0;
+    if (k < 1 || k > D.nz - 2) return 0;
+    if (P.x_solid && (i == 0 || i == D.nx - 1)) return 0;
+    if (P.enable_x_fringe || P.enable_top_drive) return 0;
+    if (!geo_far(P, D, A.bed_s, k, j, i)) return 0;
+    int type;
+    float fill;
+    classify_height(P, __ldg(A.fs_h + D.col(j, i)), k, true, type, fill);
+    if (type == LBM_FS_GAS) return 1;
+    const int im = i == 0 ? D.nx - 1 : i - 1, ip = i + 1 == D.nx ? 0 : i + 1;
+    const int jm = j == 0 ? D.ny - 1 : j - 1, jp = j + 1 == D.ny ? 0 : j + 1;
+    float hmin = __ldg(A.fs_h + D.col(j, i));
+    const int cols[8] = {D.col(jm, im), D.col(jm, i), D.col(jm, ip), D.col(j, im), D.col(j, ip), D.col(jp, im),
+                         D.col(jp, i), D.col(jp, ip)};
+#pragma unroll
+    for (int u = 0; u < 8; ++u) hmin = fminf(hmin, __ldg(A.fs_h + cols[u]));
+    return hmin > ((float)k + 1.01f) * P.dx ? 2 : 0;
+}
+
 template <int S, int IN, bool CG>
 __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, int i, float f[19], bool &fast_c,
                                       bool &open, int &type, float &gbf, float &r, float &vx, float &vy, float &vz) {
@@ -300,9 +328,29 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream
     int cut = 0, fscut = 0, bridge = 0;
     if (cell_xyz(A, i, j, k, c)) {
         float f[19];
+        const int wcls = CG ? 0 : water_stream_class(A, k, j, i);
         if (cell_fast(A, true, false, k, j, i)) {
             stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
             store_cell<S>(A, c, f);
+        } else if (wcls != 0) {
+            // water, height path, away from the bed and the x walls: a gas
+            // cell takes the rest equilibrium, a cell whose sources are all
+            // wet the plain gather; then the post-stream macro step
+            if (wcls == 1) {
+                f[0] = feq<0>(A.P.rho0, 0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+                for (int q = 1; q < 19; ++q) f[q] = A.P.rho0 * wq(q) * 1.0f;
+            } else {
+                stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
+            }
+            store_cell<S>(A, c, f);
+            int type;
+            float fill;
+            fs_state(A, c, k, j, i, true, type, fill);
+            const float gbf = gbf_of(A.P, k, true, type);
+            float r, vx, vy, vz;
+            macro(A.P, A.D, f, k, true, type, gbf, r, vx, vy, vz);
+            A.rho[c] = r; A.ux[c] = vx; A.uy[c] = vy; A.uz[c] = vz;
         } else {
             GeoLinks Ls;
             Geo gs = geo_cell<CG>(A.P, A.slot, A.D, A.bed_s, k, j, i, Ls, true, A.P.use_link_wall_velocity && A.P.include_bed);

@@ -198,32 +198,47 @@ __device__ __forceinline__ void store_cell(const StepArgs &A, int c, const float
 // post-stream state; IN = 1: stream + BC of the previous step from its
 // post-collision state.  Cells away from every wall and boundary take the
 // plain gather; the general path handles the rest.
-// Stream-stage class of a water cell on the height path: 1 = gas cell away
-// from every wall (stream_bc gives the rest equilibrium on every link),
-// 2 = cell whose 18 sources are all wet and in the domain, away from every
-// wall (stream_bc gives the plain gather), 0 = anything else.  Wet sources:
-// the lowest free-surface height over the 3x3 columns is more than 1.01
-// cells above the top source plane, so every source fill exceeds 1e-4.
+// Stream-stage class of a water cell on the height path: 1 = gas cell,
+// 2 = cell whose sources are all wet, 0 = anything else; in classes 1 and 2
+// the cell is away from the bed (its link endpoints are more than half a
+// cell above the 3x3 bed maximum), away from the top and bottom rows, and
+// there is no cube, phi geometry, fringe or top drive, so stream_bc gives:
+// the rest equilibrium (gas) or the plain gather (wet sources) on every
+// link, except the links through a solid x wall, which carry the cell's own
+// opposite population.  Wet sources: the lowest free-surface height over
+// the 3x3 columns is more than 1.01 cells above the top source plane's
+// bottom, so every source fill exceeds 1e-4.
 __device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int j, int i) {
     const lbm_params &P = A.P;
     const Dom &D = A.D;
     if (P.fs_mode == LBM_FS_NONE || (A.flags & F_VOF_STATE)) return 0;
     if (k < 1 || k > D.nz - 2) return 0;
-    if (P.x_solid && (i == 0 || i == D.nx - 1)) return 0;
-    if (P.enable_x_fringe || P.enable_top_drive) return 0;
-    if (!geo_far(P, D, A.bed_s, k, j, i)) return 0;
+    if (P.enable_x_fringe || P.enable_top_drive || P.include_cube || P.use_phi_open_fraction ||
+        P.use_phi_open_flags)
+        return 0;
+    const float dx = P.dx, hdx = 0.5f * dx;
+    if (P.include_bed) {
+        const float zc = ((float)k + 0.5f) * dx;
+        const float hm = __ldg(A.bed_s.hmax + D.col(j, i));
+        const float margin = 1e-4f * dx + 1e-6f * (fabsf(zc) + fabsf(hm));
+        if (!((zc - hdx) - hm >= hdx + margin)) return 0;
+    }
     int type;
     float fill;
     classify_height(P, __ldg(A.fs_h + D.col(j, i)), k, true, type, fill);
     if (type == LBM_FS_GAS) return 1;
-    const int im = i == 0 ? D.nx - 1 : i - 1, ip = i + 1 == D.nx ? 0 : i + 1;
+    int im = i == 0 ? D.nx - 1 : i - 1, ip = i + 1 == D.nx ? 0 : i + 1;
+    if (P.x_solid) {
+        if (i == 0) im = i;
+        if (i + 1 == D.nx) ip = i;
+    }
     const int jm = j == 0 ? D.ny - 1 : j - 1, jp = j + 1 == D.ny ? 0 : j + 1;
     float hmin = __ldg(A.fs_h + D.col(j, i));
     const int cols[8] = {D.col(jm, im), D.col(jm, i), D.col(jm, ip), D.col(j, im), D.col(j, ip), D.col(jp, im),
                          D.col(jp, i), D.col(jp, ip)};
 #pragma unroll
     for (int u = 0; u < 8; ++u) hmin = fminf(hmin, __ldg(A.fs_h + cols[u]));
-    return hmin > ((float)k + 1.01f) * P.dx ? 2 : 0;
+    return hmin > ((float)k + 1.01f) * dx ? 2 : 0;
 }
 
 template <int S, int IN, bool CG>
@@ -336,12 +351,33 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream
             // water, height path, away from the bed and the x walls: a gas
             // cell takes the rest equilibrium, a cell whose sources are all
             // wet the plain gather; then the post-stream macro step
+            const bool xwall = A.P.x_solid && (i == 0 || i + 1 == A.D.nx);
             if (wcls == 1) {
                 f[0] = feq<0>(A.P.rho0, 0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
                 for (int q = 1; q < 19; ++q) f[q] = A.P.rho0 * wq(q) * 1.0f;
-            } else {
+            } else if (!xwall) {
                 stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
+            } else {
+                // pull from inside the domain (periodic y); the wall links are set below
+                const typename Store<S>::T *fs = (const typename Store<S>::T *)A.fsrc;
+#pragma unroll
+                for (int q = 0; q < 19; ++q) {
+                    const int si = i - cxq(q);
+                    if (si < 0 || si >= A.D.nx) continue;
+                    const int sj = (j - cyq(q) + A.D.ny) % A.D.ny;
+                    f[q] = Store<S>::ld(fs, (size_t)q * A.D.n + A.D.cell(k - czq(q), sj, si), q, A.P.rho0);
+                }
+            }
+            if (xwall) {
+                const typename Store<S>::T *fs = (const typename Store<S>::T *)A.fsrc;
+#pragma unroll
+                for (int q = 1; q < 19; ++q) {
+                    if ((i == 0 && cxq(q) > 0) || (i + 1 == A.D.nx && cxq(q) < 0)) {
+                        f[q] = Store<S>::ld(fs, (size_t)oppq(q) * A.D.n + c, oppq(q), A.P.rho0);
+                        if (wcls == 2) cut++;
+                    }
+                }
             }
             store_cell<S>(A, c, f);
             int type;

@@ -326,7 +326,10 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     A.bed_c = slot_view(ctx, (int)((n + 1) & 1));
     A.bed_s = A.bed_c;
     A.step = (uint64_t)(n + 1);
-    const int tflag = R.classic ? F_TILE_CLASSIC : 0;
+    // with LES the pre-pass stores the post-condition populations of the
+    // general planes for their collide pass (FP32 populations, column-cache path)
+    const int tflag = (R.classic ? F_TILE_CLASSIC : 0) |
+                      ((les && ctx->use_cg && ctx->P.pop_storage == LBM_STORE_F32) ? F_STASH : 0);
     A.flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
     if (les) {
         launch_step_kernel(KER_PREPASS_CANON, A, st);

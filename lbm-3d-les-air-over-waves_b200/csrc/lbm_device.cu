@@ -305,6 +305,9 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_prepas
     A.u_out[c] = vx;
     A.u_out[A.D.n + c] = vy;
     A.u_out[2 * A.D.n + c] = vz;
+    // the collide pass of these cells reads the populations back from its
+    // own destination slots (FP32 only: exact round trip)
+    if (CG && S == LBM_STORE_F32 && (A.flags & F_STASH)) store_cell<S>(A, c, f);
 }
 
 template <int S, int IN, bool CG>
@@ -314,7 +317,22 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collid
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
-    front<S, IN, CG>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
+    if (CG && S == LBM_STORE_F32 && (A.flags & F_STASH)) {
+        // populations after stream, boundary conditions and condition
+        // stage, left in the destination slots by the pre-pass
+        const float *fd = (const float *)A.fdst;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) f[q] = fd[(size_t)q * A.D.n + c];
+        GeoLinks Lc;
+        Geo gc = geo_cell<CG>(A.P, A.slot, A.D, A.bed_c, k, j, i, Lc, true, false);
+        fast_c = gc.fast;
+        open = (gc.lo & 1u) != 0u;
+        type = LBM_FS_LIQUID;
+        gbf = 0.0f;
+        macro(A.P, A.D, f, k, false, type, gbf, r, vx, vy, vz);
+    } else {
+        front<S, IN, CG>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
+    }
     const lbm_params &P = A.P;
     const bool water = !CG && P.fs_mode != LBM_FS_NONE;
     const bool gas = water && type == LBM_FS_GAS;

@@ -243,35 +243,18 @@ def ours(args):
     import numpy as np
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device")
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
+    from lbm_b200.replicas import Replicas
 
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(vals):
-        t = torch.tensor(vals, dtype=torch.float64, device=dev)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.tolist()
+    reps = Replicas("nccl")
+    world, rank, local, dev = reps.world, reps.rank, reps.local, reps.device
+    barrier, max_over_ranks = reps.barrier, reps.max
 
     from lbm_b200.domain import Domain
 
     K, W = args.steps, max(args.warmup, 3)
-    env = workload_env(seed=12345 + rank)
+    env = workload_env(seed=reps.seed(12345))
     dom = Domain(env, device=dev, with_diag=False)
     lib = dom.lib
     s = dom.stream
@@ -372,9 +355,7 @@ def ours(args):
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
         }
     dom.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    reps.close()
     if out is not None:
         print(json.dumps(out), flush=True)
     return 0

@@ -364,7 +364,10 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
                 su[sl][2][ry + 1][rx + 1] = __ldg(A.u_les + 2 * n + cr);
             }
         }
-        if (LES) __syncthreads();
+        // No barrier here: the collide of plane p - 1 reads other threads'
+        // velocities only in plane p - 1 (published in the previous
+        // iteration, ordered by the barrier above); planes p and p - 2 are
+        // read at the thread's own column, written by the thread itself.
         const int k = p - 1;
         if (k >= z0 && k < z1) {
             const int c = k * nxy + col;

@@ -260,7 +260,10 @@ def ours(args):
     s = dom.stream
     ncell = NX * NY * NZ
 
-    # ---- warm-up
+    # ---- warm-up: pick the interior kernel's planes per block, then W steps
+    from lbm_b200.tuning import autotune_tile_chunk
+
+    tuned = autotune_tile_chunk(dom)
     run_steps(dom, W)
     dom.synchronize()
     if dom.counters()["status_flags"]:
@@ -349,7 +352,9 @@ def ours(args):
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic", "config": base_config(),
+            "dtype": "f32", "data": "synthetic",
+            "config": dict(base_config(), tile_chunk=tuned["chunk"],
+                           tile_chunk_ms={str(k): round(v, 4) for k, v in tuned["ms_per_step"].items()}),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K},
             "gpu_launches": int(l1.value - l0.value),
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,

@@ -297,6 +297,12 @@ int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out);
    reports zeros. */
 int lbm_set_kernel_timing(lbm_ctx *ctx, int32_t enable);
 int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t *cells_per_launch);
+/* Tuning hook (no counterpart in the reference): planes per thread block of
+   the interior kernel, the work unit of its z march (0 restores the built-in
+   choice).  lbm_b200.tuning picks it by timing candidates.  The CPU oracle
+   accepts and ignores it. */
+int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes);
+
 /* Measurement hook (no counterpart in the reference): number of kernels the
    library has launched in this process, over all contexts.  The CPU oracle
    reports 0. */

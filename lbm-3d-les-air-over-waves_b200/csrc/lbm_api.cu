@@ -71,6 +71,7 @@ struct lbm_ctx {
     float *bed_uw[2] = {nullptr, nullptr}, *bed_vw[2] = {nullptr, nullptr}, *bed_ww[2] = {nullptr, nullptr};
     float *bed_cg[2] = {nullptr, nullptr};  // per-column link-endpoint cache (bed-only geometry)
     bool use_cg = false;
+    int tile_chunk = 0;   // planes per block of the interior kernel (0: heuristic)
     // VOF scratch (VOF contexts only)
     int8_t *v_open = nullptr, *v_t0 = nullptr, *v_ba = nullptr;
     float *v_lf0 = nullptr, *v_m0 = nullptr, *v_x0 = nullptr, *v_fa = nullptr;
@@ -292,6 +293,7 @@ static Plan plan_planes(const lbm_ctx *ctx) {
     int chunk = (ni + want_chunks - 1) / want_chunks;
     if (chunk < 8) chunk = 8;
     if (chunk > 64) chunk = 64;
+    if (ctx->tile_chunk > 0) chunk = ctx->tile_chunk;   // set by lbm_set_tile_chunk (autotuner)
     const char *ch = getenv("LBM_B200_TILE_CHUNK");
     if (ch && atoi(ch) > 0) chunk = atoi(ch);
     R.chunk = chunk;
@@ -750,6 +752,12 @@ int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t
     *total_ms = tot;
     *launches = (int64_t)(ctx->ev_used / 2);
     *cells_per_launch = ctx->timed_cells;
+    return LBM_OK;
+}
+
+int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes) {
+    if (!ctx || planes < 0 || planes > 4096) return LBM_ERR_BAD_ARG;
+    ctx->tile_chunk = planes;
     return LBM_OK;
 }
 

@@ -174,7 +174,8 @@ __global__ void __launch_bounds__(256, 2) k_tile(StepArgs A) {
                 su[sl][1][ry + 1][rx + 1] = b;
                 su[sl][2][ry + 1][rx + 1] = d;
             }
-            __syncthreads();
+            // (no barrier: the collide below reads other threads' velocities
+            // only in plane p - 1; plane p's are read from the next iteration)
         }
         const int k = p - 1;
         if (k >= z0 && k < z1) {

@@ -100,6 +100,10 @@ class Domain:
         self._check(self.lib.lbm_kernel_timing(self.ctx, C.byref(ms), C.byref(n), C.byref(cells)), "lbm_kernel_timing")
         return ms.value, n.value, cells.value
 
+    def set_tile_chunk(self, planes: int):
+        """Planes per block of the interior kernel (0: built-in choice)."""
+        self._check(self.lib.lbm_set_tile_chunk(self.ctx, int(planes)), "lbm_set_tile_chunk")
+
     def synchronize(self):
         self.stream.synchronize()
 

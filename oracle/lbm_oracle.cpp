@@ -752,6 +752,9 @@ int lbm_link_geometry_noalloc(const lbm_params *, const float *, float *, int32_
     if (err && err_len) snprintf(err, err_len, "%s", "the CPU oracle has no allocation-free variant");
     return LBM_ERR_UNSUPPORTED;
 }
+int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes) {
+    return (ctx && planes >= 0) ? LBM_OK : LBM_ERR_BAD_ARG;
+}
 int lbm_launch_count(int64_t *count) {
     if (!count) return LBM_ERR_BAD_ARG;
     *count = 0;

@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(256, 2) k_tile(StepArgs A) {
     const int i = blockIdx.x * LBM_TILE + tx, j = blockIdx.y * LBM_TILE + ty;
     const int z0 = A.zi0 + blockIdx.z * A.chunk;
     const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
-    __shared__ float su[3][3][LBM_TILE + 2][LBM_TILE + 2];  // [plane slot][component][y][x]
+    __shared__ float su[3][3][LBM_TILE + 2][LBM_TILE + 2];  // [plane slot][component][x][y]
     __shared__ float ringf[LES ? 19 : 1][64];               // ring populations of the current plane
 
     // ring cell whose moments this thread takes (threads 0..63)
@@ -144,22 +144,22 @@ __global__ void __launch_bounds__(256, 2) k_tile(StepArgs A) {
             interior_front<S, IN>(A, p, j, i, fc);
             macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
             if (LES) {
-                su[sl][0][ty + 1][tx + 1] = vx;
-                su[sl][1][ty + 1][tx + 1] = vy;
-                su[sl][2][ty + 1][tx + 1] = vz;
+                su[sl][0][tx + 1][ty + 1] = vx;
+                su[sl][1][tx + 1][ty + 1] = vy;
+                su[sl][2][tx + 1][ty + 1] = vz;
             }
             if (LES) ring_gather<S, IN>(A, p, t, ringf);
         } else if (LES) {
             // plane handled by the general kernels: velocity from their pre-pass
             const int c = D.cell(p, j, i);
-            su[sl][0][ty + 1][tx + 1] = __ldg(A.u_les + c);
-            su[sl][1][ty + 1][tx + 1] = __ldg(A.u_les + n + c);
-            su[sl][2][ty + 1][tx + 1] = __ldg(A.u_les + 2 * n + c);
+            su[sl][0][tx + 1][ty + 1] = __ldg(A.u_les + c);
+            su[sl][1][tx + 1][ty + 1] = __ldg(A.u_les + n + c);
+            su[sl][2][tx + 1][ty + 1] = __ldg(A.u_les + 2 * n + c);
             if (ring) {
                 const int cr = D.cell(p, rj, ri);
-                su[sl][0][ry + 1][rx + 1] = __ldg(A.u_les + cr);
-                su[sl][1][ry + 1][rx + 1] = __ldg(A.u_les + n + cr);
-                su[sl][2][ry + 1][rx + 1] = __ldg(A.u_les + 2 * n + cr);
+                su[sl][0][rx + 1][ry + 1] = __ldg(A.u_les + cr);
+                su[sl][1][rx + 1][ry + 1] = __ldg(A.u_les + n + cr);
+                su[sl][2][rx + 1][ry + 1] = __ldg(A.u_les + 2 * n + cr);
             }
         }
         if (LES) __syncthreads();
@@ -170,9 +170,9 @@ __global__ void __launch_bounds__(256, 2) k_tile(StepArgs A) {
 #pragma unroll
                 for (int q = 0; q < 19; ++q) fr[q] = ringf[q][t];
                 macro(P, D, fr, p, false, LBM_FS_LIQUID, 0.0f, rr, a, b, d);
-                su[sl][0][ry + 1][rx + 1] = a;
-                su[sl][1][ry + 1][rx + 1] = b;
-                su[sl][2][ry + 1][rx + 1] = d;
+                su[sl][0][rx + 1][ry + 1] = a;
+                su[sl][1][rx + 1][ry + 1] = b;
+                su[sl][2][rx + 1][ry + 1] = d;
             }
             // (no barrier: the collide below reads other threads' velocities
             // only in plane p - 1; plane p's are read from the next iteration)
@@ -186,11 +186,11 @@ __global__ void __launch_bounds__(256, 2) k_tile(StepArgs A) {
             if (LES) {
                 const int sm = (p + 1) % 3, s0 = (p + 2) % 3, sp = sl;  // planes k-1, k, k+1
                 const int y = ty + 1, x = tx + 1;
-                om = les_interior(P, su[s0][0][y][x + 1], su[s0][0][y][x - 1], su[s0][0][y + 1][x],
-                                  su[s0][0][y - 1][x], su[sp][0][y][x], su[sm][0][y][x], su[s0][1][y][x + 1],
-                                  su[s0][1][y][x - 1], su[s0][1][y + 1][x], su[s0][1][y - 1][x], su[sp][1][y][x],
-                                  su[sm][1][y][x], su[s0][2][y][x + 1], su[s0][2][y][x - 1], su[s0][2][y + 1][x],
-                                  su[s0][2][y - 1][x], su[sp][2][y][x], su[sm][2][y][x]);
+                om = les_interior(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
+                                  su[s0][0][x][y - 1], su[sp][0][x][y], su[sm][0][x][y], su[s0][1][x + 1][y],
+                                  su[s0][1][x - 1][y], su[s0][1][x][y + 1], su[s0][1][x][y - 1], su[sp][1][x][y],
+                                  su[sm][1][x][y], su[s0][2][x + 1][y], su[s0][2][x - 1][y], su[s0][2][x][y + 1],
+                                  su[s0][2][x][y - 1], su[sp][2][x][y], su[sm][2][x][y]);
                 if (A.flags & F_WRITE_ALL_OMEGA) A.omega[c] = om;
                 if (k == A.zi0 || k == A.zi1) {
                     // velocity of the interior planes next to the general ones,
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
     extern __shared__ __align__(16) float smem[];
     float *sf = smem;                                   // [slot][q][256] own-cell populations
     float *sr = smem + PIPE_SLOTS * 19 * 256;           // [slot][q][64] ring populations
-    float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =        // [plane slot][component][y][x]
+    float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =        // [plane slot][component][x][y]
         (float (*)[3][LBM_TILE + 2][LBM_TILE + 2])(sr + PIPE_SLOTS * 19 * 64);
     const lbm_params &P = A.P;
     const Dom &D = A.D;
@@ -338,31 +338,31 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
         if (interior) {
             macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
             if (LES) {
-                su[sl][0][ty + 1][tx + 1] = vx;
-                su[sl][1][ty + 1][tx + 1] = vy;
-                su[sl][2][ty + 1][tx + 1] = vz;
+                su[sl][0][tx + 1][ty + 1] = vx;
+                su[sl][1][tx + 1][ty + 1] = vy;
+                su[sl][2][tx + 1][ty + 1] = vz;
                 if (ring) {
                     const float *rs = sr + sl * 19 * 64 + t;
                     float fr[19], rr, a, b, d;
 #pragma unroll
                     for (int q = 0; q < 19; ++q) fr[q] = rs[q * 64];
                     macro(P, D, fr, p, false, LBM_FS_LIQUID, 0.0f, rr, a, b, d);
-                    su[sl][0][ry + 1][rx + 1] = a;
-                    su[sl][1][ry + 1][rx + 1] = b;
-                    su[sl][2][ry + 1][rx + 1] = d;
+                    su[sl][0][rx + 1][ry + 1] = a;
+                    su[sl][1][rx + 1][ry + 1] = b;
+                    su[sl][2][rx + 1][ry + 1] = d;
                 }
             }
         } else if (LES) {
             // plane handled by the general kernels: velocity from their pre-pass
             const int c = p * nxy + col;
-            su[sl][0][ty + 1][tx + 1] = __ldg(A.u_les + c);
-            su[sl][1][ty + 1][tx + 1] = __ldg(A.u_les + n + c);
-            su[sl][2][ty + 1][tx + 1] = __ldg(A.u_les + 2 * n + c);
+            su[sl][0][tx + 1][ty + 1] = __ldg(A.u_les + c);
+            su[sl][1][tx + 1][ty + 1] = __ldg(A.u_les + n + c);
+            su[sl][2][tx + 1][ty + 1] = __ldg(A.u_les + 2 * n + c);
             if (ring) {
                 const int cr = (p * D.ny + rj) * D.nx + ri;
-                su[sl][0][ry + 1][rx + 1] = __ldg(A.u_les + cr);
-                su[sl][1][ry + 1][rx + 1] = __ldg(A.u_les + n + cr);
-                su[sl][2][ry + 1][rx + 1] = __ldg(A.u_les + 2 * n + cr);
+                su[sl][0][rx + 1][ry + 1] = __ldg(A.u_les + cr);
+                su[sl][1][rx + 1][ry + 1] = __ldg(A.u_les + n + cr);
+                su[sl][2][rx + 1][ry + 1] = __ldg(A.u_les + 2 * n + cr);
             }
         }
         // No barrier here: the collide of plane p - 1 reads other threads'
@@ -376,11 +376,11 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
             if (LES) {
                 const int sm = (p + 1) % 3, s0 = (p + 2) % 3, sp = sl;  // planes k-1, k, k+1
                 const int y = ty + 1, x = tx + 1;
-                om = les_interior(P, su[s0][0][y][x + 1], su[s0][0][y][x - 1], su[s0][0][y + 1][x],
-                                  su[s0][0][y - 1][x], su[sp][0][y][x], su[sm][0][y][x], su[s0][1][y][x + 1],
-                                  su[s0][1][y][x - 1], su[s0][1][y + 1][x], su[s0][1][y - 1][x], su[sp][1][y][x],
-                                  su[sm][1][y][x], su[s0][2][y][x + 1], su[s0][2][y][x - 1], su[s0][2][y + 1][x],
-                                  su[s0][2][y - 1][x], su[sp][2][y][x], su[sm][2][y][x]);
+                om = les_interior(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
+                                  su[s0][0][x][y - 1], su[sp][0][x][y], su[sm][0][x][y], su[s0][1][x + 1][y],
+                                  su[s0][1][x - 1][y], su[s0][1][x][y + 1], su[s0][1][x][y - 1], su[sp][1][x][y],
+                                  su[sm][1][x][y], su[s0][2][x + 1][y], su[s0][2][x - 1][y], su[s0][2][x][y + 1],
+                                  su[s0][2][x][y - 1], su[sp][2][x][y], su[sm][2][x][y]);
                 if (A.flags & F_WRITE_ALL_OMEGA) A.omega[c] = om;
                 if (k == A.zi0 || k == A.zi1) {
                     // velocity of the interior planes next to the general ones,

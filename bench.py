@@ -263,7 +263,11 @@ def ours(args):
     # ---- warm-up: pick the interior kernel's planes per block, then W steps
     from lbm_b200.tuning import autotune_tile_chunk
 
-    tuned = autotune_tile_chunk(dom)
+    if args.tile_chunk:
+        dom.set_tile_chunk(args.tile_chunk)
+        tuned = {"chunk": args.tile_chunk, "ms_per_step": {}}
+    else:
+        tuned = autotune_tile_chunk(dom)
     run_steps(dom, W)
     dom.synchronize()
     if dom.counters()["status_flags"]:
@@ -459,6 +463,8 @@ def main():
     ap.add_argument("--min-steps", type=int, default=100, help="serving mode: fewest steps of a request")
     ap.add_argument("--max-steps", type=int, default=600, help="serving mode: most steps of a request")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed CPU oracle sample")
+    ap.add_argument("--tile-chunk", type=int, default=0,
+                    help="planes per block of the interior kernel (default: autotuned in warm-up)")
     ap.add_argument("--size", type=str, default=None,
                     help="NXxNYxNZ: another domain size of the same workload (profiling of small cases)")
     args = ap.parse_args()

@@ -1022,6 +1022,24 @@ static bool pipe_smem_ready() {
     }
     return ok[dev];
 }
+template <int S>
+static bool pipe16_smem_ready() {
+    static bool done[64] = {false}, ok[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    if (!done[dev]) {
+        done[dev] = true;
+        ok[dev] = cudaFuncSetAttribute(k_tile_pipe16<S, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       P16_SMEM_BYTES) == cudaSuccess &&
+                  cudaFuncSetAttribute(k_tile_pipe16<S, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       P16_SMEM_BYTES) == cudaSuccess &&
+                  cudaFuncSetAttribute(k_tile_pipe16<S, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       P16_SMEM_BYTES) == cudaSuccess &&
+                  cudaFuncSetAttribute(k_tile_pipe16<S, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       P16_SMEM_BYTES) == cudaSuccess;
+    }
+    return ok[dev];
+}
 
 template <int S>
 static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) {
@@ -1039,6 +1057,11 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
     // pipelined interior kernel: FP32 populations, 32-bit population indices
     const bool pipe = tile_kernel && S == LBM_STORE_F32 && !(A.flags & F_TILE_CLASSIC) &&
                       19.0 * (double)A.D.n < 2147483647.0 && pipe_smem_ready();
+    // pipelined 16-bit interior kernel: staged pairs need an even nx (tiles of 16) and a 32-bit cell count
+    bool pipe16 = false;
+    if constexpr (S != LBM_STORE_F32)
+        pipe16 = tile_kernel && !(A.flags & F_TILE_CLASSIC) && (double)A.D.n < 2147483647.0 &&
+                 pipe16_smem_ready<S>();
     switch (which) {
         case KER_PREPASS_CANON:
             if (cg) k_prepass<S, 0, true><<<g, kBlock3, 0, st>>>(A);
@@ -1066,6 +1089,14 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
             LAUNCHED(1);
             break;
         case KER_TILE_CANON:
+            if constexpr (S != LBM_STORE_F32) {
+                if (pipe16) {
+                    if (les) k_tile_pipe16<S, 0, true><<<gt, 256, P16_SMEM_BYTES, st>>>(A);
+                    else k_tile_pipe16<S, 0, false><<<gt, 256, P16_SMEM_BYTES, st>>>(A);
+                    LAUNCHED(1);
+                    break;
+                }
+            }
             if (pipe) {
                 if (les) k_tile_pipe<0, true><<<gt, 256, PIPE_SMEM_BYTES, st>>>(A);
                 else k_tile_pipe<0, false><<<gt, 256, PIPE_SMEM_BYTES, st>>>(A);
@@ -1076,6 +1107,14 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
             LAUNCHED(1);
             break;
         case KER_TILE_FUSED:
+            if constexpr (S != LBM_STORE_F32) {
+                if (pipe16) {
+                    if (les) k_tile_pipe16<S, 1, true><<<gt, 256, P16_SMEM_BYTES, st>>>(A);
+                    else k_tile_pipe16<S, 1, false><<<gt, 256, P16_SMEM_BYTES, st>>>(A);
+                    LAUNCHED(1);
+                    break;
+                }
+            }
             if (pipe) {
                 if (les) k_tile_pipe<1, true><<<gt, 256, PIPE_SMEM_BYTES, st>>>(A);
                 else k_tile_pipe<1, false><<<gt, 256, PIPE_SMEM_BYTES, st>>>(A);

@@ -405,6 +405,206 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
+// ------------------------------------------- pipelined 16-bit interior kernel
+// k_tile_pipe16: k_tile_pipe for shifted FP16/BF16 populations.  cp.async
+// copies at least 4 bytes, so the block copies aligned pairs of 16-bit
+// values: for each population and tile row the 9 pairs x0 .. x0+17 (x0-2 ..
+// x0+15 for the populations pulled from x - 1), in which every cell of the
+// row finds its pulled value; the ring rows likewise, and for the two ring
+// columns the pair that holds each value.  Values are widened with the
+// storage's own conversion (Store<S>::ld) when read from shared memory.
+constexpr int P16_ROWW = 9;                              // words (pairs) per staged row
+constexpr int P16_MAIN = 19 * 16 * P16_ROWW;             // words per plane slot
+constexpr int P16_RROW = 19 * 2 * P16_ROWW;              // ring rows, words
+constexpr int P16_RCOL = 19 * 2 * 16;                    // ring columns, words
+constexpr int P16_RING = P16_RROW + P16_RCOL;
+constexpr int P16_SMEM_BYTES =
+    (PIPE_SLOTS * P16_MAIN + PIPE_SLOTS * P16_RING) * 4 + 3 * 3 * (LBM_TILE + 2) * (LBM_TILE + 2) * 4;
+
+LBM_DEV void cp_async4v(void *smem, const void *gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+LBM_DEV int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+template <int S, int IN, bool LES>
+__global__ void __launch_bounds__(256, 2) k_tile_pipe16(StepArgs A) {
+    typedef typename Store<S>::T T;
+    extern __shared__ __align__(16) float smem[];
+    uint32_t *sw = (uint32_t *)smem;                     // [slot][P16_MAIN] words
+    uint32_t *rw = sw + PIPE_SLOTS * P16_MAIN;           // [slot][P16_RING] words
+    float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =         // [plane slot][component][x][y]
+        (float (*)[3][LBM_TILE + 2][LBM_TILE + 2])(rw + PIPE_SLOTS * P16_RING);
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    const int x0 = blockIdx.x * LBM_TILE, y0 = blockIdx.y * LBM_TILE;
+    const int i = x0 + tx, j = y0 + ty;
+    const int z0 = A.zi0 + blockIdx.z * A.chunk;
+    const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
+    const int n = (int)D.n, nxy = D.nx * D.ny;
+    const T *fsrc = (const T *)A.fsrc;
+    T *fdst = (T *)A.fdst;
+    {
+        const int kc = max(z0, A.zi0);
+        bool ok = geo_far(P, D, A.bed_c, kc, j, i) && (IN == 0 || geo_far(P, D, A.bed_s, kc, j, i));
+        if (z0 == A.zi0)
+            ok = ok && geo_far(P, D, A.bed_c, z0 - 1, j, i) && (IN == 0 || geo_far(P, D, A.bed_s, z0 - 1, j, i));
+        if (!ok) atomicOr(A.status, 2u);
+    }
+    const int col = j * D.nx + i;
+    int rx = 0, ry = 0;
+    ring_cell(t & 63, rx, ry);
+    const int ri = (x0 + rx + D.nx) % D.nx;
+    const int rj = (y0 + ry + D.ny) % D.ny;
+    const bool ring = LES && t < 64;
+
+    // copies of plane p into slot p % 3
+    auto issue = [&](int p) {
+        if (p >= A.zi0 && p <= A.zi1 && p <= z1) {
+            const int slot = p % PIPE_SLOTS;
+            uint32_t *dst = sw + slot * P16_MAIN;
+#pragma unroll
+            for (int v = 0; v < (P16_MAIN + 255) / 256; ++v) {
+                const int m = t + 256 * v;
+                if (m < P16_MAIN) {
+                    const int q = m / (16 * P16_ROWW), r = m - q * (16 * P16_ROWW);
+                    const int row = r / P16_ROWW, pr = r - row * P16_ROWW;
+                    const int cx = IN ? c_tile_cx[q] : 0, cy = IN ? c_tile_cy[q] : 0, cz = IN ? c_tile_cz[q] : 0;
+                    const int xs = cx > 0 ? x0 - 2 : x0;
+                    const int sx = wrapi(xs + 2 * pr, D.nx), sy = wrapi(y0 + row - cy, D.ny);
+                    cp_async4v(dst + m, fsrc + ((size_t)q * n + (size_t)(p - cz) * nxy + (size_t)sy * D.nx + sx));
+                }
+            }
+            if (LES) {
+                uint32_t *rdst = rw + slot * P16_RING;
+#pragma unroll
+                for (int v = 0; v < (P16_RING + 255) / 256; ++v) {
+                    const int m = t + 256 * v;
+                    if (m < P16_RROW) {
+                        const int q = m / (2 * P16_ROWW), r2 = m - q * (2 * P16_ROWW);
+                        const int side = r2 / P16_ROWW, pr = r2 - side * P16_ROWW;
+                        const int cx = IN ? c_tile_cx[q] : 0, cy = IN ? c_tile_cy[q] : 0, cz = IN ? c_tile_cz[q] : 0;
+                        const int xs = cx > 0 ? x0 - 2 : x0;
+                        const int sx = wrapi(xs + 2 * pr, D.nx);
+                        const int sy = wrapi((side ? y0 + LBM_TILE : y0 - 1) - cy, D.ny);
+                        cp_async4v(rdst + m, fsrc + ((size_t)q * n + (size_t)(p - cz) * nxy + (size_t)sy * D.nx + sx));
+                    } else if (m < P16_RING) {
+                        const int m2 = m - P16_RROW;
+                        const int q = m2 / 32, r2 = m2 - q * 32;
+                        const int side = r2 / 16, rr = r2 - side * 16;
+                        const int cx = IN ? c_tile_cx[q] : 0, cy = IN ? c_tile_cy[q] : 0, cz = IN ? c_tile_cz[q] : 0;
+                        const int sx = wrapi((side ? x0 + LBM_TILE : x0 - 1) - cx, D.nx) & ~1;
+                        const int sy = wrapi(y0 + rr - cy, D.ny);
+                        cp_async4v(rdst + m, fsrc + ((size_t)q * n + (size_t)(p - cz) * nxy + (size_t)sy * D.nx + sx));
+                    }
+                }
+            }
+        }
+        cp_async_commit();
+    };
+
+    issue(z0 - 1);
+    issue(z0);
+    float fp[19];
+    float rp = 0.0f, vxp = 0.0f, vyp = 0.0f, vzp = 0.0f;
+    for (int p = z0 - 1; p <= z1; ++p) {
+        const int sl = p % 3;
+        const bool interior = p >= A.zi0 && p <= A.zi1;
+        cp_async_wait1();       // plane p has landed (p + 1 may still be in flight)
+        __syncthreads();        // the staged rows come from other threads
+        float fc[19];
+        float r = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
+        if (interior) {
+            const T *sb = (const T *)(sw + sl * P16_MAIN);
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                const int off = (IN && cxq(q) != 0) ? 1 : 0;
+                fc[q] = Store<S>::ld_rw(sb, (size_t)(q * 16 * 2 * P16_ROWW + ty * 2 * P16_ROWW + tx + off), q, P.rho0);
+            }
+        }
+        float frr[19];
+        if (interior && ring) {
+            const T *rb = (const T *)(rw + sl * P16_RING);
+            const int rr = t;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) {
+                const int cx = IN ? cxq(q) : 0;
+                size_t e;
+                if (rr < 32) {
+                    const int side = rr >> 4, rx2 = rr & 15;
+                    e = (size_t)(q * 2 * 2 * P16_ROWW + side * 2 * P16_ROWW + rx2 + (cx != 0 ? 1 : 0));
+                } else {
+                    const int side = (rr - 32) >> 4, ry2 = rr & 15;
+                    const int sx = wrapi((side ? x0 + LBM_TILE : x0 - 1) - cx, D.nx);
+                    e = (size_t)(2 * P16_RROW + 2 * (q * 32 + side * 16 + ry2) + (sx & 1));
+                }
+                frr[q] = Store<S>::ld_rw(rb, e, q, P.rho0);
+            }
+        }
+        issue(p + 2);           // into the slot consumed before the barrier above
+        if (interior) {
+            macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
+            if (LES) {
+                su[sl][0][tx + 1][ty + 1] = vx;
+                su[sl][1][tx + 1][ty + 1] = vy;
+                su[sl][2][tx + 1][ty + 1] = vz;
+                if (ring) {
+                    float rr2, a, b, d;
+                    macro(P, D, frr, p, false, LBM_FS_LIQUID, 0.0f, rr2, a, b, d);
+                    su[sl][0][rx + 1][ry + 1] = a;
+                    su[sl][1][rx + 1][ry + 1] = b;
+                    su[sl][2][rx + 1][ry + 1] = d;
+                }
+            }
+        } else if (LES) {
+            // plane handled by the general kernels: velocity from their pre-pass
+            const int c = p * nxy + col;
+            su[sl][0][tx + 1][ty + 1] = __ldg(A.u_les + c);
+            su[sl][1][tx + 1][ty + 1] = __ldg(A.u_les + n + c);
+            su[sl][2][tx + 1][ty + 1] = __ldg(A.u_les + 2 * n + c);
+            if (ring) {
+                const int cr = (p * D.ny + rj) * D.nx + ri;
+                su[sl][0][rx + 1][ry + 1] = __ldg(A.u_les + cr);
+                su[sl][1][rx + 1][ry + 1] = __ldg(A.u_les + n + cr);
+                su[sl][2][rx + 1][ry + 1] = __ldg(A.u_les + 2 * n + cr);
+            }
+        }
+        // no barrier: other threads' velocities are read one plane back
+        const int k = p - 1;
+        if (k >= z0 && k < z1) {
+            const int c = k * nxy + col;
+            float om = P.omega0;
+            if (LES) {
+                const int sm = (p + 1) % 3, s0 = (p + 2) % 3, sp = sl;  // planes k-1, k, k+1
+                const int y = ty + 1, x = tx + 1;
+                om = les_interior(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
+                                  su[s0][0][x][y - 1], su[sp][0][x][y], su[sm][0][x][y], su[s0][1][x + 1][y],
+                                  su[s0][1][x - 1][y], su[s0][1][x][y + 1], su[s0][1][x][y - 1], su[sp][1][x][y],
+                                  su[sm][1][x][y], su[s0][2][x + 1][y], su[s0][2][x - 1][y], su[s0][2][x][y + 1],
+                                  su[s0][2][x][y - 1], su[sp][2][x][y], su[sm][2][x][y]);
+                if (A.flags & F_WRITE_ALL_OMEGA) A.omega[c] = om;
+                if (k == A.zi0 || k == A.zi1) {
+                    A.u_out[c] = vxp;
+                    A.u_out[n + c] = vyp;
+                    A.u_out[2 * n + c] = vzp;
+                }
+            }
+            if (A.flags & F_WRITE_MACRO) {
+                A.rho[c] = rp; A.ux[c] = vxp; A.uy[c] = vyp; A.uz[c] = vzp;
+            }
+            if (!(rp == rp) || fabsf(rp) > 3.0e38f) atomicOr(A.status, 1u);
+            collide(A, c, k, false, false, false, 0.0f, rp, vxp, vyp, vzp, om, fp);
+#pragma unroll
+            for (int q = 0; q < 19; ++q) Store<S>::st(fdst, (size_t)q * n + (size_t)c, fp[q], q, P.rho0);
+        }
+#pragma unroll
+        for (int q = 0; q < 19; ++q) fp[q] = fc[q];
+        rp = r; vxp = vx; vyp = vy; vzp = vz;
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // stream only (the last pass of a call) for interior cells
 template <int S>
 __global__ void __launch_bounds__(256) k_stream_interior(StepArgs A) {

@@ -18,6 +18,8 @@
 //
 // The 2-D bed of step m lives in scratch slot m & 1, so the fused pass can
 // see the bed of both steps it spans.
+#include <cuda.h>
+#include <cudaTypedefs.h>   // PFN_cuTensorMapEncodeTiled (resolved at run time: no driver library link)
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -88,6 +90,10 @@ struct lbm_ctx {
     std::vector<cudaEvent_t> ev;  // pairs (start, stop)
     size_t ev_used = 0;
     int64_t timed_cells = 0;
+    // tensor maps of f[0] and f[1] for the tile-copy interior kernel: boxes 24x18 and 20x18
+    CUtensorMap tmap[2][2];
+    void *tmap_src[2] = {nullptr, nullptr};   // buffers the maps were encoded for
+    bool tmap_ok = false;
 };
 
 static void timed_mark(lbm_ctx *ctx, cudaStream_t st) {
@@ -256,6 +262,7 @@ static int bed_step(lbm_ctx *ctx, int64_t m, cudaStream_t st) {
 struct Plan {
     bool tile = false;
     bool classic = false;   // unpipelined interior kernel even for FP32 (LBM_B200_TILE_KERNEL=classic)
+    bool no_tma = false;    // cp.async-staged interior kernel instead of tile copies (LBM_B200_TILE_KERNEL=pipe)
     int zi0 = 0, zi1 = -1, chunk = 64;
     int zlo[3] = {0, 0, 0}, zcnt[3] = {0, 0, 0};
 };
@@ -283,6 +290,7 @@ static Plan plan_planes(const lbm_ctx *ctx) {
     R.tile = true;
     const char *tk = getenv("LBM_B200_TILE_KERNEL");
     R.classic = tk && strcmp(tk, "classic") == 0;
+    R.no_tma = tk && strcmp(tk, "pipe") == 0;
     R.zi0 = zi0;
     R.zi1 = zi1;
     // planes per block: enough blocks for ~4 waves of 2 blocks per SM, at
@@ -314,6 +322,56 @@ static void apply_plan(StepArgs &A, const Plan &R) {
     A.chunk = R.chunk;
 }
 
+// cuTensorMapEncodeTiled, found through the runtime's driver entry points
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::mutex mu;
+    static bool tried = false;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// Tensor maps over the FP32 populations f[q][z][y][x] as a 4-D tensor
+// (x, y, z, q) for the tile-copy interior kernel.  Requirements of tile
+// copies: 16-byte aligned base, strides multiples of 16 bytes (nx multiple
+// of 4), inner box extent a multiple of 16 bytes (24 and 20 floats).
+static bool tile_maps_ready(lbm_ctx *ctx) {
+    if (ctx->tmap_ok && ctx->tmap_src[0] == ctx->b.f[0] && ctx->tmap_src[1] == ctx->b.f[1]) return true;
+    ctx->tmap_ok = false;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t nx = (cuuint64_t)ctx->P.nx, ny = (cuuint64_t)ctx->P.ny, nz = (cuuint64_t)ctx->P.nz;
+    if (nx % 4 != 0) return false;
+    const cuuint64_t dims[4] = {nx, ny, nz, 19};
+    const cuuint64_t strides[3] = {nx * 4, nx * ny * 4, nx * ny * nz * 4};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    for (int b = 0; b < 2; ++b) {
+        if (((uintptr_t)ctx->b.f[b] & 15u) != 0) return false;
+        for (int w = 0; w < 2; ++w) {
+            const cuuint32_t box[4] = {w == 0 ? 24u : 20u, (cuuint32_t)(LBM_TILE + 2), 1u, 1u};
+            if (enc(&ctx->tmap[b][w], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->b.f[b], dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return false;
+        }
+    }
+    ctx->tmap_src[0] = ctx->b.f[0];
+    ctx->tmap_src[1] = ctx->b.f[1];
+    ctx->tmap_ok = true;
+    return true;
+}
+
 static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     const int64_t n = ctx->nstep;
     const bool les = ctx->P.use_les != 0;
@@ -333,6 +391,9 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     const int tflag = (R.classic ? F_TILE_CLASSIC : 0) |
                       ((les && ctx->use_cg && ctx->P.pop_storage == LBM_STORE_F32) ? F_STASH : 0);
     A.flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
+    // fused interior steps with LES and FP32 populations: the tile-copy kernel (32-bit population indices)
+    const bool tma = R.tile && les && !R.classic && !R.no_tma && ctx->P.pop_storage == LBM_STORE_F32 &&
+                     19.0 * (double)ctx->D.n < 2147483647.0 && tile_maps_ready(ctx);
     if (les) {
         launch_step_kernel(KER_PREPASS_CANON, A, st);
         CK_LAUNCH("prepass");
@@ -358,7 +419,8 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
         }
         if (R.tile) {
             if (ctx->timing) timed_mark(ctx, st);
-            launch_step_kernel(KER_TILE_FUSED, A, st);
+            if (!(tma && launch_tile_tma(A, &ctx->tmap[src][0], &ctx->tmap[src][1], st)))
+                launch_step_kernel(KER_TILE_FUSED, A, st);
             CK_LAUNCH("tile fused");
             if (ctx->timing) {
                 timed_mark(ctx, st);

@@ -2,6 +2,7 @@
 // translation unit (lbm_device.cu) and the host API (lbm_api.cu).
 #pragma once
 
+#include <cuda.h>   // CUtensorMap (the type only)
 #include <cuda_runtime.h>
 
 #include "lbm_dev.cuh"
@@ -108,6 +109,10 @@ void launch_bed(const lbm_params &P, const Dom &D, const float *h_prev, float *h
 void launch_hmax(const Dom &D, const float *h, float *hmax, cudaStream_t st);
 void launch_colgeo(const lbm_params &P, const Dom &D, const BedView &B, float *cg, cudaStream_t st);
 void launch_step_kernel(int which, const StepArgs &A, cudaStream_t st);
+// fused interior step with LES (FP32) staged by tile copies; m24 / m20 are
+// the source populations' tensor maps with boxes 24x18x1x1 and 20x18x1x1.
+// false: not launched (shared memory of that size unavailable)
+bool launch_tile_tma(const StepArgs &A, const CUtensorMap *m24, const CUtensorMap *m20, cudaStream_t st);
 void launch_column_flux(const StepArgs &A, float *qx, float *qy, cudaStream_t st);
 void launch_advect(const lbm_params &P, const Dom &D, const float *bed_h, const float *qx, const float *qy,
                    const float *h_in, float *h_out, float *h_last, float t, cudaStream_t st);

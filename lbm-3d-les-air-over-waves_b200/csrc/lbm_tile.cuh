@@ -20,6 +20,8 @@
 // precondition fails.
 #pragma once
 
+#include <cuda.h>   // CUtensorMap (the type only; nothing links the driver library)
+
 #include "lbm_stages.cuh"
 
 namespace lbm {
@@ -239,8 +241,7 @@ LBM_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "me
 LBM_DEV void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <int IN, bool LES>
-__global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
-    extern __shared__ __align__(16) float smem[];
+LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by) {
     float *sf = smem;                                   // [slot][q][256] own-cell populations
     float *sr = smem + PIPE_SLOTS * 19 * 256;           // [slot][q][64] ring populations
     float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =        // [plane slot][component][x][y]
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
     const lbm_params &P = A.P;
     const Dom &D = A.D;
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-    const int i = blockIdx.x * LBM_TILE + tx, j = blockIdx.y * LBM_TILE + ty;
+    const int i = bx * LBM_TILE + tx, j = by * LBM_TILE + ty;
     const int z0 = A.zi0 + blockIdx.z * A.chunk;
     const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
     const int n = (int)D.n, nxy = D.nx * D.ny;
@@ -270,8 +271,8 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
     // ring items of this thread: ring cell r = t & 63, q = (t >> 6) + 4u
     int rx = 0, ry = 0;
     ring_cell(t & 63, rx, ry);
-    const int ri = (blockIdx.x * LBM_TILE + rx + D.nx) % D.nx;
-    const int rj = (blockIdx.y * LBM_TILE + ry + D.ny) % D.ny;
+    const int ri = (bx * LBM_TILE + rx + D.nx) % D.nx;
+    const int rj = (by * LBM_TILE + ry + D.ny) % D.ny;
     int roff[5];
 #pragma unroll
     for (int u = 0; u < 5; ++u) {
@@ -403,6 +404,12 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
         rp = r; vxp = vx; vyp = vy; vzp = vz;
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+template <int IN, bool LES>
+__global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
+    extern __shared__ __align__(16) float smem[];
+    tile_pipe_body<IN, LES>(A, smem, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------- pipelined 16-bit interior kernel
@@ -603,6 +610,251 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe16(StepArgs A) {
         rp = r; vxp = vx; vyp = vy; vzp = vz;
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// ------------------------------------------------ TMA-staged interior kernel
+// k_tile_tma: the fused step (pull from the previous step's post-collision
+// state) with LES for FP32 populations, staged by the tensor memory
+// accelerator.  For population q one 4-D tile copy (x, y, z, q) brings the
+// box x in [xs, xs + W), y in [y0 - 1 - cy, y0 + 17 - cy), plane p - cz into
+// shared memory: it holds the pulled value of each tile cell and of each ring
+// cell (x0 - 1 .. x0 + 16 before the shift by -cx).  W = 24 from xs = x0 - 4
+// when cx = 0; W = 20 from xs = x0 - 4 (cx = 1) or xs = x0 (cx = -1), so x
+// coordinates stay multiples of 4 floats (16 bytes) and each box starts on a
+// 128-byte boundary of its slot.  Lanes 0..18 of warp 0 issue the 19 copies
+// of plane p + 2 into a ring of 3 slots, each completing on its own
+// mbarrier; no thread spends instructions on addresses or copies.  Plane
+// p + 1 is copied while plane p is worked on, and the populations of plane
+// p - 1 are read again from their slot when it is collided (registers stay
+// at 96, no spills).  A tile copy cannot wrap the periodic x and y
+// boundaries, so this kernel covers the tiles off the domain edge, and
+// k_tile_edges (the cp.async-staged body of k_tile_pipe) the ring of edge
+// tiles.  This grid is launched behind k_tile_edges as a programmatic
+// dependent, so its blocks fill the SMs that grid's tail leaves idle.
+// Arithmetic, and so every result, is that of k_tile.
+constexpr int TMA_H = LBM_TILE + 2;                    // box rows
+constexpr int TMA_REG24 = 448, TMA_REG20 = 384;        // floats per population (24x18, 20x18, padded to 128 B)
+__host__ __device__ constexpr unsigned tma_cx0_mask(int q = 0) {
+    return q == 19 ? 0u : (((cxq(q) == 0) ? 1u : 0u) << q) | tma_cx0_mask(q + 1);
+}
+__host__ __device__ constexpr int popc32(unsigned v) {   // no loop or call: folds for a constant argument
+    const unsigned a = v - ((v >> 1) & 0x55555555u);
+    const unsigned b = (a & 0x33333333u) + ((a >> 2) & 0x33333333u);
+    return (int)((((b + (b >> 4)) & 0x0F0F0F0Fu) * 0x01010101u) >> 24);
+}
+__host__ __device__ constexpr int tma_shift(int q) {   // box column of tile x = 0
+    return cxq(q) == 0 ? 4 : (cxq(q) > 0 ? 3 : 1);
+}
+constexpr unsigned TMA_CX0 = tma_cx0_mask();
+__host__ __device__ constexpr int tma_base(int q) {    // floats before population q in a slot
+    return TMA_REG20 * q + (TMA_REG24 - TMA_REG20) * popc32(TMA_CX0 & ((1u << q) - 1u));
+}
+constexpr int TMA_SLOT = tma_base(19);                 // floats per plane slot
+constexpr unsigned TMA_BYTES = 9u * 24u * TMA_H * 4u + 10u * 20u * TMA_H * 4u;   // bytes landing per plane
+constexpr int TMA_SMEM_BYTES = 128 + PIPE_SLOTS * TMA_SLOT * 4 + 3 * 3 * (LBM_TILE + 2) * (LBM_TILE + 2) * 4 +
+                               PIPE_SLOTS * 8;
+constexpr int TMA_WAIT_LIMIT = 1 << 22;                // try_wait rounds before a wait gives up (status bit 2)
+static_assert(TMA_SLOT == 9 * TMA_REG24 + 10 * TMA_REG20, "slot layout");
+static_assert(tma_base(1) == TMA_REG24 && tma_base(3) == TMA_REG24 + 2 * TMA_REG20 && tma_base(18) == 8 * TMA_REG24 + 10 * TMA_REG20,
+              "population offsets");
+static_assert((TMA_REG24 * 4) % 128 == 0 && (TMA_REG20 * 4) % 128 == 0, "boxes start on 128-byte boundaries");
+
+LBM_DEV unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+LBM_DEV void mbar_init(unsigned bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+LBM_DEV void mbar_expect_tx(unsigned bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+LBM_DEV bool mbar_try_wait(unsigned bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+LBM_DEV void tma_load_4d(unsigned dst, const CUtensorMap *map, int x, int y, int z, int w, unsigned bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+        "[%6];\n" ::"r"(dst),
+        "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(bar)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(256, 2)
+    k_tile_tma(StepArgs A, const __grid_constant__ CUtensorMap m24, const __grid_constant__ CUtensorMap m20) {
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    float *sf = (float *)(tma_smem + ((128u - (smem_addr(tma_smem) & 127u)) & 127u));   // [slot][TMA_SLOT]
+    float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =        // [plane slot][component][x][y]
+        (float (*)[3][LBM_TILE + 2][LBM_TILE + 2])(sf + PIPE_SLOTS * TMA_SLOT);
+    uint64_t *bar = (uint64_t *)(sf + PIPE_SLOTS * TMA_SLOT + 3 * 3 * (LBM_TILE + 2) * (LBM_TILE + 2));
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    const int x0 = (blockIdx.x + 1) * LBM_TILE, y0 = (blockIdx.y + 1) * LBM_TILE;   // tiles off the domain edge
+    const int i = x0 + tx, j = y0 + ty;
+    const int z0 = A.zi0 + blockIdx.z * A.chunk;
+    const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
+    const int n = (int)D.n, nxy = D.nx * D.ny;
+    float *fdst = (float *)A.fdst;
+    {
+        const int kc = max(z0, A.zi0);
+        bool ok = geo_far(P, D, A.bed_c, kc, j, i) && geo_far(P, D, A.bed_s, kc, j, i);
+        if (z0 == A.zi0) ok = ok && geo_far(P, D, A.bed_c, z0 - 1, j, i) && geo_far(P, D, A.bed_s, z0 - 1, j, i);
+        if (!ok) atomicOr(A.status, 2u);
+    }
+    const int col = j * D.nx + i;
+    int rx = 0, ry = 0;
+    ring_cell(t & 63, rx, ry);
+    const int ri = (x0 + rx + D.nx) % D.nx;
+    const int rj = (y0 + ry + D.ny) % D.ny;
+    const bool ring = t < 64;
+    if (t == 0) {
+        for (int s = 0; s < PIPE_SLOTS; ++s) mbar_init(smem_addr(bar + s), 1u);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    // tile copies of plane p into slot p % 3 (lanes 0..18 of warp 0, one population each)
+    auto issue = [&](int p) {
+        if (t < 32 && p >= A.zi0 && p <= A.zi1 && p <= z1) {
+            const int slot = p % PIPE_SLOTS;
+            const unsigned b = smem_addr(bar + slot);
+            if (t == 0) mbar_expect_tx(b, TMA_BYTES);
+            __syncwarp();
+            if (t < 19) {
+                const int q = t, cx = cxq(q);
+                const int qb = TMA_REG20 * q + (TMA_REG24 - TMA_REG20) * __popc(TMA_CX0 & ((1u << q) - 1u));   // tma_base(q)
+                tma_load_4d(smem_addr(sf + slot * TMA_SLOT + qb), cx == 0 ? &m24 : &m20, cx < 0 ? x0 : x0 - 4,
+                            y0 - 1 - cyq(q), p - czq(q), q, b);
+            }
+        }
+    };
+
+    // Plane p + 1 is copied while plane p is worked on; the populations of
+    // plane p - 1, collided in iteration p, are read again from their slot
+    // instead of being held in registers (and its velocity from su).
+    issue(z0 - 1);
+    unsigned phase = 0u;   // bit s: parity of the next completion of slot s
+    float rp = 0.0f;       // density of plane p - 1
+    for (int p = z0 - 1; p <= z1; ++p) {
+        const int sl = p % 3;
+        const bool interior = p >= A.zi0 && p <= A.zi1;
+        if (interior) {
+            const unsigned b = smem_addr(bar + sl);
+            int it = 0;
+            while (!mbar_try_wait(b, (phase >> sl) & 1u)) {
+                if (++it == TMA_WAIT_LIMIT) {
+                    atomicOr(A.status, 4u);
+                    break;
+                }
+            }
+            phase ^= 1u << sl;
+        }
+        __syncthreads();        // slot (p + 1) % 3 is free: every thread is done with plane p - 2
+        issue(p + 1);
+        float r = 0.0f;
+        const float *sb = sf + sl * TMA_SLOT;
+        if (interior) {
+            if (ring) {
+                // ring cell: box row ry + 1, column rx + tma_shift(q)
+                float fr[19], rr, a, b, d;
+                const float *b24 = sb + (ry + 1) * 24 + rx, *b20 = sb + (ry + 1) * 20 + rx;
+#pragma unroll
+                for (int q = 0; q < 19; ++q) fr[q] = (cxq(q) == 0 ? b24 : b20)[tma_base(q) + tma_shift(q)];
+                macro(P, D, fr, p, false, LBM_FS_LIQUID, 0.0f, rr, a, b, d);
+                su[sl][0][rx + 1][ry + 1] = a;
+                su[sl][1][rx + 1][ry + 1] = b;
+                su[sl][2][rx + 1][ry + 1] = d;
+            }
+            // own cell: box row ty + 1, column tx + tma_shift(q)
+            float fc[19], vx, vy, vz;
+            const float *b24 = sb + (ty + 1) * 24 + tx, *b20 = sb + (ty + 1) * 20 + tx;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) fc[q] = (cxq(q) == 0 ? b24 : b20)[tma_base(q) + tma_shift(q)];
+            macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
+            su[sl][0][tx + 1][ty + 1] = vx;
+            su[sl][1][tx + 1][ty + 1] = vy;
+            su[sl][2][tx + 1][ty + 1] = vz;
+        } else {
+            // plane handled by the general kernels: velocity from their pre-pass
+            const int c = p * nxy + col;
+            su[sl][0][tx + 1][ty + 1] = __ldg(A.u_les + c);
+            su[sl][1][tx + 1][ty + 1] = __ldg(A.u_les + n + c);
+            su[sl][2][tx + 1][ty + 1] = __ldg(A.u_les + 2 * n + c);
+            if (ring) {
+                const int cr = (p * D.ny + rj) * D.nx + ri;
+                su[sl][0][rx + 1][ry + 1] = __ldg(A.u_les + cr);
+                su[sl][1][rx + 1][ry + 1] = __ldg(A.u_les + n + cr);
+                su[sl][2][rx + 1][ry + 1] = __ldg(A.u_les + 2 * n + cr);
+            }
+        }
+        // no barrier: other threads' velocities are read one plane back
+        const int k = p - 1;
+        if (k >= z0 && k < z1) {
+            const int c = k * nxy + col;
+            const int sm = (p + 1) % 3, s0 = (p + 2) % 3, sp = sl;  // planes k-1, k, k+1
+            const int y = ty + 1, x = tx + 1;
+            const float om = les_interior(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
+                                          su[s0][0][x][y - 1], su[sp][0][x][y], su[sm][0][x][y], su[s0][1][x + 1][y],
+                                          su[s0][1][x - 1][y], su[s0][1][x][y + 1], su[s0][1][x][y - 1],
+                                          su[sp][1][x][y], su[sm][1][x][y], su[s0][2][x + 1][y], su[s0][2][x - 1][y],
+                                          su[s0][2][x][y + 1], su[s0][2][x][y - 1], su[sp][2][x][y], su[sm][2][x][y]);
+            const float vxp = su[s0][0][x][y], vyp = su[s0][1][x][y], vzp = su[s0][2][x][y];
+            if (A.flags & F_WRITE_ALL_OMEGA) A.omega[c] = om;
+            if (k == A.zi0 || k == A.zi1) {
+                // velocity of the interior planes next to the general ones,
+                // for the general kernels' stencils
+                A.u_out[c] = vxp;
+                A.u_out[n + c] = vyp;
+                A.u_out[2 * n + c] = vzp;
+            }
+            if (A.flags & F_WRITE_MACRO) {
+                A.rho[c] = rp; A.ux[c] = vxp; A.uy[c] = vyp; A.uz[c] = vzp;
+            }
+            if (!(rp == rp) || fabsf(rp) > 3.0e38f) atomicOr(A.status, 1u);
+            float fp[19];
+            const float *pb = sf + s0 * TMA_SLOT;
+            const float *b24 = pb + (ty + 1) * 24 + tx, *b20 = pb + (ty + 1) * 20 + tx;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) fp[q] = (cxq(q) == 0 ? b24 : b20)[tma_base(q) + tma_shift(q)];
+            collide(A, c, k, false, false, false, 0.0f, rp, vxp, vyp, vzp, om, fp);
+#pragma unroll
+            for (int q = 0; q < 19; ++q) fdst[q * n + c] = fp[q];
+        }
+        rp = r;
+    }
+    // complete only after the edge-tile grid this one was launched behind,
+    // so that the work after it sees both grids' results
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+
+// tile e of the ring of edge tiles of a TX x TY tiling: the rows by = 0
+// and by = TY - 1, then the columns bx = 0 and bx = TX - 1 between them
+LBM_DEV void edge_tile(int e, int TX, int TY, int &bx, int &by) {
+    if (e < TX) { bx = e; by = 0; return; }
+    e -= TX;
+    if (TY > 1) {
+        if (e < TX) { bx = e; by = TY - 1; return; }
+        e -= TX;
+    }
+    by = 1 + (e >> 1);
+    bx = (e & 1) ? TX - 1 : 0;
+}
+
+// the fused interior step with LES on the edge tiles (grid.x = their
+// count), cp.async-staged.  k_tile_tma is launched after it as a
+// programmatic dependent: it may start as soon as every block of this grid
+// is running (the two grids share no output)
+__global__ void __launch_bounds__(256, 2) k_tile_edges(StepArgs A) {
+    extern __shared__ __align__(16) float smem[];
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+    int bx = 0, by = 0;
+    edge_tile(blockIdx.x, A.D.nx / LBM_TILE, A.D.ny / LBM_TILE, bx, by);
+    tile_pipe_body<1, true>(A, smem, bx, by);
 }
 
 // stream only (the last pass of a call) for interior cells

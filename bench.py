@@ -346,7 +346,7 @@ def ours(args):
             tpc = profile_traffic_per_cell()
             roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": (tpc * k_cells) if tpc else None, "peak_kind": peak_kind,
-                    "kernel": "k_tile (interior one-pass stream+LES+collide)", "cells_per_launch": k_cells,
+                    "kernel": "k_tile_edges + k_tile_tma (interior one-pass stream+LES+collide; TMA-staged off the domain edge)", "cells_per_launch": k_cells,
                     "bytes_per_cell": B_ALG, "launch_ms": per_launch_s * 1e3,
                     "step_frac": B_ALG * value * 1e6 / world / (peak * 1e9)}
         cpu = None

@@ -621,9 +621,9 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe16(StepArgs A) {
 // cell (x0 - 1 .. x0 + 16 before the shift by -cx).  W = 24 from xs = x0 - 4
 // when cx = 0; W = 20 from xs = x0 - 4 (cx = 1) or xs = x0 (cx = -1), so x
 // coordinates stay multiples of 4 floats (16 bytes) and each box starts on a
-// 128-byte boundary of its slot.  Lanes 0..18 of warp 0 issue the 19 copies
-// of plane p + 2 into a ring of 3 slots, each completing on its own
-// mbarrier; no thread spends instructions on addresses or copies.  Plane
+// 128-byte boundary of its slot.  Lane 0 of each warp issues 2 or 3 of the
+// 19 copies of a plane into a ring of 3 slots, each completing on its own
+// mbarrier; no other thread spends instructions on addresses or copies.  Plane
 // p + 1 is copied while plane p is worked on, and the populations of plane
 // p - 1 are read again from their slot when it is collided (registers stay
 // at 96, no spills).  A tile copy cannot wrap the periodic x and y
@@ -718,15 +718,19 @@ __global__ void __launch_bounds__(256, 2)
     }
     __syncthreads();
 
-    // tile copies of plane p into slot p % 3 (lanes 0..18 of warp 0, one population each)
+    // tile copies of plane p into slot p % 3, issued by lane 0 of every warp
+    // (populations w, w + 8, w + 16): copies issued by one warp's lanes
+    // leave one at a time, those of different warps side by side.  The
+    // expected byte count may be posted after some copies have completed
+    // (the transaction count goes negative until then; the phase cannot
+    // complete before thread 0 has arrived).
     auto issue = [&](int p) {
-        if (t < 32 && p >= A.zi0 && p <= A.zi1 && p <= z1) {
+        if ((t & 31) == 0 && p >= A.zi0 && p <= A.zi1 && p <= z1) {
             const int slot = p % PIPE_SLOTS;
             const unsigned b = smem_addr(bar + slot);
             if (t == 0) mbar_expect_tx(b, TMA_BYTES);
-            __syncwarp();
-            if (t < 19) {
-                const int q = t, cx = cxq(q);
+            for (int q = t >> 5; q < 19; q += 8) {
+                const int cx = cxq(q);
                 const int qb = TMA_REG20 * q + (TMA_REG24 - TMA_REG20) * __popc(TMA_CX0 & ((1u << q) - 1u));   // tma_base(q)
                 tma_load_4d(smem_addr(sf + slot * TMA_SLOT + qb), cx == 0 ? &m24 : &m20, cx < 0 ? x0 : x0 - 4,
                             y0 - 1 - cyq(q), p - czq(q), q, b);

@@ -273,8 +273,15 @@ def ours(args):
     if dom.counters()["status_flags"]:
         raise SystemExit("non-finite state after warm-up")
 
-    # ---- device-resident throughput (+ live timing of the dominant kernel)
-    dom.set_kernel_timing(True)
+    # ---- device-resident throughput: step-graph replays (each call of
+    # CHUNK steps one graph launch; the shapes of the timed calls are
+    # captured in warm-up)
+    graphs = not args.no_graphs
+    if graphs:
+        dom.set_step_graphs(True)
+        run_steps(dom, 2 * CHUNK)
+        W += 2 * CHUNK
+        dom.synchronize()
     l0 = C.c_int64()
     lib.lbm_launch_count(C.byref(l0))
     clocks = ClockSampler(local)
@@ -292,10 +299,24 @@ def ours(args):
     l1 = C.c_int64()
     lib.lbm_launch_count(C.byref(l1))
     ms = e0.elapsed_time(e1)
+    if dom.counters()["status_flags"]:
+        raise SystemExit("non-finite state in the timed region")
+    # ---- the dominant kernel's launches timed with events: the same K steps
+    # as eager calls (events cannot be read per replay inside a graph)
+    dom.set_step_graphs(False)
+    dom.set_kernel_timing(True)
+    barrier()
+    torch.cuda.synchronize(dev)
+    r0, r1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r0.record(s)
+    run_steps(dom, K)
+    r1.record(s)
+    r1.synchronize()
+    eager_ms = r0.elapsed_time(r1)
     k_ms, k_launches, k_cells = dom.kernel_timing()
     dom.set_kernel_timing(False)
     if dom.counters()["status_flags"]:
-        raise SystemExit("non-finite state in the timed region")
+        raise SystemExit("non-finite state in the timed kernel pass")
 
     # ---- end to end through the API with host buffers: the reference's main
     # loop (initial state from the host, steps in chunks of 100, the health
@@ -358,7 +379,10 @@ def ours(args):
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": dict(base_config(), tile_chunk=tuned["chunk"],
-                           tile_chunk_ms={str(k): round(v, 4) for k, v in tuned["ms_per_step"].items()}),
+                           tile_chunk_ms={str(k): round(v, 4) for k, v in tuned["ms_per_step"].items()},
+                           step_graphs=graphs, eager_ms_per_step=round(eager_ms / K, 4),
+                           roofline_timing="interior grids timed with CUDA events over the same K steps run as "
+                                           "eager calls right after the timed region"),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K},
             "gpu_launches": int(l1.value - l0.value),
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
@@ -400,8 +424,10 @@ def batched(args):
 
     storage = args.storage or "f16s"
     envs = stable_ensemble_envs(args.domains, seed=7, storage=storage)
-    b = Batch(envs, chunk=25)
+    b = Batch(envs, chunk=25, graphs=not args.no_graphs)
     K, W = args.steps, max(args.warmup, 3)
+    if not args.no_graphs:
+        W = max(W, 3 * b.chunk)   # an eager call, then the captures of both step parities
     b.step(W)
     b.synchronize()
     ms = _device_time([d.stream for d in b.domains], lambda: b.step(K))
@@ -415,7 +441,7 @@ def batched(args):
         "config": {"workload": f"batched ensemble of {len(envs)} air-over-wave domains (seed 7, stability-screened "
                                f"draws), uneven sizes",
                    "cells": cells, "storage": storage, "steps_per_call": b.chunk,
-                   "streams": len(envs)},
+                   "streams": len(envs), "step_graphs": not args.no_graphs},
         "roofline_step_frac": bytes_cell * cells * K / (ms * 1e-3) / (measured_hbm_peak()[0] * 1e9),
     }
     for d in b.domains:
@@ -463,6 +489,8 @@ def main():
     ap.add_argument("--min-steps", type=int, default=100, help="serving mode: fewest steps of a request")
     ap.add_argument("--max-steps", type=int, default=600, help="serving mode: most steps of a request")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed CPU oracle sample")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="time eager step calls instead of CUDA step-graph replays")
     ap.add_argument("--tile-chunk", type=int, default=0,
                     help="planes per block of the interior kernel (default: autotuned in warm-up)")
     ap.add_argument("--size", type=str, default=None,

@@ -302,6 +302,21 @@ int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t
    choice).  lbm_b200.tuning picks it by timing candidates.  The CPU oracle
    accepts and ignores it. */
 int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes);
+/* Step graphs (no counterpart in the reference; the reference launches
+   every kernel from its Python step loop): when enabled, each lbm_step call
+   of the air path runs as one CUDA graph launch.  The first call of a given
+   step count, step parity and current population buffer is captured on the
+   caller's stream (nothing runs during the capture) and kept; every later
+   call of that shape replays it after one launch that writes the step
+   number to a device clock, from which the captured kernels take the bed
+   time and the random-kick key.  Results are those of the eager calls, bit
+   for bit.  Graphs need a stream of the caller's (not the legacy default
+   stream) and start after one eager call; they are dropped by lbm_bind,
+   lbm_set_tile_chunk with a new value and lbm_destroy, and not used while
+   kernel timing is on.  A refused capture turns the context back to eager
+   calls.  Water modes return LBM_ERR_UNSUPPORTED (their steps synchronise
+   with the host).  The CPU oracle accepts and ignores it. */
+int lbm_set_step_graphs(lbm_ctx *ctx, int32_t enable);
 
 /* Measurement hook (no counterpart in the reference): number of kernels the
    library has launched in this process, over all contexts.  The CPU oracle

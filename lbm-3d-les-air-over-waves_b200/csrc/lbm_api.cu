@@ -90,11 +90,27 @@ struct lbm_ctx {
     std::vector<cudaEvent_t> ev;  // pairs (start, stop)
     size_t ev_used = 0;
     int64_t timed_cells = 0;
+    // step graphs (air mode): one captured graph per (steps per call, step parity, current buffer); the kernels
+    // of a captured call read the step number from the device clock, set by one launch before each replay
+    struct StepGraph {
+        int steps, parity, cur, cur_after;
+        long long launches;
+        cudaGraphExec_t exec;
+    };
+    bool graphs = false, capturing = false, warm = false;
+    int64_t cap_n0 = 0;
+    long long *dclock = nullptr;
+    std::vector<StepGraph> graph_cache;
     // tensor maps of f[0] and f[1] for the tile-copy interior kernel: boxes 24x18 and 20x18
     CUtensorMap tmap[2][2];
     void *tmap_src[2] = {nullptr, nullptr};   // buffers the maps were encoded for
     bool tmap_ok = false;
 };
+
+static void drop_graphs(lbm_ctx *ctx) {
+    for (auto &g : ctx->graph_cache) cudaGraphExecDestroy(g.exec);
+    ctx->graph_cache.clear();
+}
 
 static void timed_mark(lbm_ctx *ctx, cudaStream_t st) {
     if (ctx->ev_used == ctx->ev.size()) {
@@ -248,7 +264,8 @@ static int store_bed_slot(lbm_ctx *ctx, int s, const float *h_prev, cudaStream_t
 static int bed_step(lbm_ctx *ctx, int64_t m, cudaStream_t st) {
     int s = (int)(m & 1), sp = (int)((m - 1) & 1);
     launch_bed(ctx->P, ctx->D, ctx->bed_h[sp], ctx->bed_h[s], ctx->bed_hmax[s], ctx->bed_uw[s], ctx->bed_vw[s],
-               ctx->bed_ww[s], ctx->b.piecewise_bed_z, step_time(ctx, m), st);
+               ctx->bed_ww[s], ctx->b.piecewise_bed_z, step_time(ctx, m), st, ctx->capturing ? ctx->dclock : nullptr,
+               (long long)(m - ctx->cap_n0));
     CK_LAUNCH("bed");
     return refresh_column_cache(ctx, s, st);
 }
@@ -385,7 +402,9 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     A.fdst = ctx->b.f[1 - src];
     A.bed_c = slot_view(ctx, (int)((n + 1) & 1));
     A.bed_s = A.bed_c;
-    A.step = (uint64_t)(n + 1);
+    if (ctx->capturing) A.clock = ctx->dclock;   // step numbers below become offsets from the clock
+    const int64_t key0 = ctx->capturing ? ctx->cap_n0 : 0;
+    A.step = (uint64_t)(n + 1 - key0);
     // with LES the pre-pass stores the post-condition populations of the
     // general planes for their collide pass (FP32 populations, column-cache path)
     const int tflag = (R.classic ? F_TILE_CLASSIC : 0) |
@@ -411,7 +430,7 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
         A.fdst = ctx->b.f[1 - src];
         A.bed_s = slot_view(ctx, (int)(m & 1));
         A.bed_c = slot_view(ctx, (int)((m + 1) & 1));
-        A.step = (uint64_t)(m + 1);
+        A.step = (uint64_t)(m + 1 - key0);
         A.flags = ((m + 1 == n + K) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
         if (les) {
             launch_step_kernel(KER_PREPASS_FUSED, A, st);
@@ -598,6 +617,7 @@ int lbm_bind(lbm_ctx *ctx, const lbm_buffers *bufs) {
         !b.piecewise_bed_z || !b.u_inlet_profile || !b.rho_initial || !b.init_noise || !b.fs_fill ||
         !b.fs_type || !b.fs_type_prev || !b.fs_mass || !b.fs_mass_excess || !b.fs_excess_dir)
         return fail(ctx, LBM_ERR_BAD_ARG, "lbm_bind: a required state buffer is NULL");
+    drop_graphs(ctx);   // captured graphs hold the previous buffers' addresses
     ctx->b = b;
     if (!ctx->bound) {
         int s;
@@ -712,12 +732,9 @@ int lbm_init_fields(lbm_ctx *ctx, void *stream) {
     return LBM_OK;
 }
 
-int lbm_step(lbm_ctx *ctx, int32_t nsteps, void *stream) {
-    if (!ctx || nsteps < 0) return LBM_ERR_BAD_ARG;
-    if (!ctx->bound) return LBM_ERR_NOT_BOUND;
-    if (nsteps == 0) return LBM_OK;
-    cudaStream_t st = (cudaStream_t)stream;
-    ctx->last_stream = st;
+}  // extern "C"
+
+static int step_call(lbm_ctx *ctx, int32_t nsteps, cudaStream_t st) {
     int s;
     int64_t n0 = ctx->nstep;
     if ((s = load_bed_slot(ctx, (int)(n0 & 1), st)) != LBM_OK) return s;
@@ -727,6 +744,78 @@ int lbm_step(lbm_ctx *ctx, int32_t nsteps, void *stream) {
     if (s != LBM_OK) return s;
     int64_t n1 = ctx->nstep;
     return store_bed_slot(ctx, (int)(n1 & 1), ctx->bed_h[(n1 - 1) & 1], st);
+}
+
+// A call of nsteps as one graph launch.  The first call of a shape is
+// captured (nothing runs during capture), then replayed like every later
+// one.  LBM_ERR_UNSUPPORTED: capture refused; the caller runs the call eagerly.
+static int step_graph(lbm_ctx *ctx, int32_t nsteps, cudaStream_t st) {
+    const int par = (int)(ctx->nstep & 1), cur = ctx->cur;
+    lbm_ctx::StepGraph *g = nullptr;
+    for (auto &e : ctx->graph_cache)
+        if (e.steps == nsteps && e.parity == par && e.cur == cur) g = &e;
+    if (!g) {
+        if (!ctx->dclock) {
+            int s = alloc(ctx, (void **)&ctx->dclock, sizeof(long long));
+            if (s != LBM_OK) return s;
+        }
+        const int64_t n0 = ctx->nstep;
+        const long long l0 = launch_count();
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+            return LBM_ERR_UNSUPPORTED;
+        }
+        ctx->capturing = true;
+        ctx->cap_n0 = n0;
+        const int s = step_call(ctx, nsteps, st);
+        ctx->capturing = false;
+        ctx->cap_n0 = 0;
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &graph);
+        const int cur_after = ctx->cur;
+        const long long launches = launch_count() - l0;
+        launch_count_add(-launches);   // nothing ran during the capture
+        ctx->nstep = n0;
+        ctx->cur = cur;
+        cudaGraphExec_t exec = nullptr;
+        const bool ok = s == LBM_OK && e == cudaSuccess && graph &&
+                        cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        if (graph) cudaGraphDestroy(graph);
+        if (!ok) {
+            cudaGetLastError();
+            ctx->err.clear();
+            return LBM_ERR_UNSUPPORTED;
+        }
+        ctx->graph_cache.push_back({nsteps, par, cur, cur_after, launches, exec});
+        g = &ctx->graph_cache.back();
+    }
+    launch_clock_set(ctx->dclock, (long long)ctx->nstep, st);
+    CK_LAUNCH("step clock");
+    CK(cudaGraphLaunch(g->exec, st), "step graph launch");
+    launch_count_add(g->launches);
+    ctx->nstep += nsteps;
+    ctx->cur = g->cur_after;
+    return LBM_OK;
+}
+
+extern "C" {
+
+int lbm_step(lbm_ctx *ctx, int32_t nsteps, void *stream) {
+    if (!ctx || nsteps < 0) return LBM_ERR_BAD_ARG;
+    if (!ctx->bound) return LBM_ERR_NOT_BOUND;
+    if (nsteps == 0) return LBM_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->last_stream = st;
+    // step graphs: air mode, a stream of the caller's, no per-launch timing,
+    // after one eager call (which sets the kernels' shared-memory limits)
+    if (ctx->graphs && st != 0 && ctx->P.fs_mode == LBM_FS_NONE && !ctx->timing && ctx->warm) {
+        const int s = step_graph(ctx, nsteps, st);
+        if (s != LBM_ERR_UNSUPPORTED) return s;
+        ctx->graphs = false;   // capture refused: eager from now on
+    }
+    const int s = step_call(ctx, nsteps, st);
+    if (s == LBM_OK) ctx->warm = true;
+    return s;
 }
 
 int lbm_export_diagnostics(lbm_ctx *ctx, void *stream) {
@@ -819,7 +908,16 @@ int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t
 
 int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes) {
     if (!ctx || planes < 0 || planes > 4096) return LBM_ERR_BAD_ARG;
+    if (planes != ctx->tile_chunk) drop_graphs(ctx);
     ctx->tile_chunk = planes;
+    return LBM_OK;
+}
+
+int lbm_set_step_graphs(lbm_ctx *ctx, int32_t enable) {
+    if (!ctx) return LBM_ERR_BAD_ARG;
+    if (enable && ctx->P.fs_mode != LBM_FS_NONE) return fail(ctx, LBM_ERR_UNSUPPORTED, "lbm_set_step_graphs: air mode only");
+    if (!enable) drop_graphs(ctx);
+    ctx->graphs = enable != 0;
     return LBM_OK;
 }
 
@@ -831,6 +929,7 @@ int lbm_launch_count(int64_t *count) {
 
 int lbm_destroy(lbm_ctx *ctx) {
     if (!ctx) return LBM_ERR_BAD_ARG;
+    drop_graphs(ctx);
     for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
     for (void *p : ctx->owned) cudaFree(p);
     release_slot(ctx->slot);

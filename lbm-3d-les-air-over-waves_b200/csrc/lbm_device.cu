@@ -42,6 +42,7 @@ static inline unsigned blocks_for(size_t n, unsigned t) { return (unsigned)((n +
 // kernels launched by this library since the process started
 static std::atomic<long long> g_launches{0};
 long long launch_count() { return g_launches.load(); }
+void launch_count_add(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 #define LAUNCHED(n) g_launches.fetch_add((n), std::memory_order_relaxed)
 
 // 3-D launch of the general kernels: block (32, 8), grid (ceil(nx/32),
@@ -102,9 +103,10 @@ __device__ __forceinline__ float gaussian_h(const lbm_params &P, const Dom &D, f
 // ------------------------------------------------------------- bed (2-D)
 // update_wave_bed_and_velocities, CODEX.py:1082-1162, harmonics generalised
 __global__ void k_bed(lbm_params P, Dom D, const float *__restrict__ h_prev, float *h, float *uw, float *vw,
-                      float *ww, const float *__restrict__ piecewise, float t) {
+                      float *ww, const float *__restrict__ piecewise, float t, const long long *clock, long long off) {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= (int)D.a) return;
+    if (clock) t = (float)((double)(*clock + off + 1) * P.dt_phys);  // the host's step time, CODEX.py:3874
     int i = a % D.nx;
     const bool moving = P.bed_profile == LBM_BED_MOVING_SINE;
     float a1 = 0.0f, a2 = 0.0f;
@@ -991,9 +993,15 @@ __global__ void k_export(InitArgs I, ExportArgs E) {
 }
 
 // ---------------------------------------------------------------- launchers
+__global__ void k_clock_set(long long *clock, long long value) { *clock = value; }
+
+void launch_clock_set(long long *clock, long long value, cudaStream_t st) {
+    k_clock_set<<<1, 1, 0, st>>>(clock, value); LAUNCHED(1);
+}
+
 void launch_bed(const lbm_params &P, const Dom &D, const float *h_prev, float *h, float *hmax, float *uw, float *vw,
-                float *ww, const float *piecewise, float t, cudaStream_t st) {
-    k_bed<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, h_prev, h, uw, vw, ww, piecewise, t); LAUNCHED(1);
+                float *ww, const float *piecewise, float t, cudaStream_t st, const long long *clock, long long off) {
+    k_bed<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, h_prev, h, uw, vw, ww, piecewise, t, clock, off); LAUNCHED(1);
     k_hmax<<<blocks_for(D.a, 256), 256, 0, st>>>(D, h, hmax); LAUNCHED(1);
 }
 void launch_colgeo(const lbm_params &P, const Dom &D, const BedView &B, float *cg, cudaStream_t st) {

@@ -44,7 +44,8 @@ struct StepArgs {
     const float *u_inlet_profile;
     int *counters;       // [0] cut, [1] fs cut, [2] bridge
     unsigned *status;    // bit 0: non-finite density
-    uint64_t step;       // 1-based step number of the collide stage (RNG key)
+    uint64_t step;       // 1-based step number of the collide stage (RNG key); with clock, the offset from *clock
+    const long long *clock;  // device step clock of a captured step graph (null: step is absolute)
     int flags;
     // z planes covered by a launch: up to 3 ranges [zlo, zlo + zcnt), grid.z = sum of zcnt
     int zlo[3], zcnt[3];
@@ -103,9 +104,14 @@ struct ExportArgs {
 
 cudaError_t upload_params(int slot, const lbm_params &P);
 long long launch_count();
+void launch_count_add(long long n);   // kernels run by a graph replay (or taken back after a capture)
 
+// bed at time t; with a step clock, at t = (float)((*clock + off + 1) * dt_phys) read on the device
 void launch_bed(const lbm_params &P, const Dom &D, const float *h_prev, float *h, float *hmax, float *uw, float *vw,
-                float *ww, const float *piecewise, float t, cudaStream_t st);
+                float *ww, const float *piecewise, float t, cudaStream_t st, const long long *clock = nullptr,
+                long long off = 0);
+// *clock = value (the first node of a step-graph replay)
+void launch_clock_set(long long *clock, long long value, cudaStream_t st);
 void launch_hmax(const Dom &D, const float *h, float *hmax, cudaStream_t st);
 void launch_colgeo(const lbm_params &P, const Dom &D, const BedView &B, float *cg, cudaStream_t st);
 void launch_step_kernel(int which, const StepArgs &A, cudaStream_t st);

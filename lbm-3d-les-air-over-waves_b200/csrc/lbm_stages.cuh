@@ -706,7 +706,8 @@ LBM_DEV void collide(const StepArgs &A, int c, int k, bool solid, bool water, bo
         second_moments(d, Pxx, Pyy, Pzz, Pxy, Pxz, Pyz);
         float tr = (Pxx + Pyy + Pzz) / 3.0f;
         Pxx -= tr; Pyy -= tr; Pzz -= tr;
-        float xi = 2.0f * lbm_uniform01(P.seed, A.step, (uint64_t)c) - 1.0f;
+        const uint64_t key = A.clock ? (uint64_t)(*A.clock + (long long)A.step) : A.step;
+        float xi = 2.0f * lbm_uniform01(P.seed, key, (uint64_t)c) - 1.0f;
         float scale = P.c_backscatter * xi;
         float sPxx = scale * Pxx, sPyy = scale * Pyy, sPzz = scale * Pzz;
         float sPxy = scale * Pxy, sPxz = scale * Pxz, sPyz = scale * Pyz;

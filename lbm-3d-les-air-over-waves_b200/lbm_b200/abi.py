@@ -271,6 +271,8 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.lbm_launch_count.argtypes = [C.POINTER(C.c_int64)]
     lib.lbm_set_tile_chunk.restype = C.c_int
     lib.lbm_set_tile_chunk.argtypes = [vp, C.c_int32]
+    lib.lbm_set_step_graphs.restype = C.c_int
+    lib.lbm_set_step_graphs.argtypes = [vp, C.c_int32]
     lib.lbm_link_geometry_noalloc.restype = C.c_int
     lib.lbm_link_geometry_noalloc.argtypes = [C.POINTER(LbmParams), vp, vp, vp, vp, vp, vp, vp, vp, C.c_char_p,
                                               C.c_size_t]
@@ -281,7 +283,7 @@ ABI_SYMBOLS = (
     "lbm_backend_name", "lbm_abi_version", "lbm_struct_size", "lbm_create", "lbm_bind", "lbm_init_geometry",
     "lbm_init_fields", "lbm_step", "lbm_export_diagnostics", "lbm_read_counters", "lbm_destroy", "lbm_last_error",
     "lbm_set_kernel_timing", "lbm_kernel_timing", "lbm_launch_count", "lbm_link_geometry_noalloc",
-    "lbm_set_tile_chunk",
+    "lbm_set_tile_chunk", "lbm_set_step_graphs",
 )
 
 

@@ -97,7 +97,13 @@ def domain_bytes(cfg, with_diag: bool = False) -> int:
 
 
 class Batch:
-    def __init__(self, envs, device="cuda:0", chunk: int = 25):
+    """Domains stepped together, each on its own stream.  With graphs (the
+    default) each air domain's step calls run as CUDA graph replays
+    (lbm_set_step_graphs): after the first eager call, one graph per call
+    shape is captured, then a call costs two launches instead of about
+    seven per step."""
+
+    def __init__(self, envs, device="cuda:0", chunk: int = 25, graphs: bool = True):
         import torch
 
         from .domain import Domain
@@ -106,6 +112,10 @@ class Batch:
         self.chunk = int(chunk)
         self.domains = [Domain(env, device=self.device, stream=torch.cuda.Stream(self.device), with_diag=False)
                         for env in envs]
+        if graphs:
+            for d in self.domains:
+                if d.cfg.physics_mode == "air":
+                    d.set_step_graphs(True)
 
     @property
     def cells(self) -> int:

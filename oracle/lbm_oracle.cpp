@@ -755,6 +755,7 @@ int lbm_link_geometry_noalloc(const lbm_params *, const float *, float *, int32_
 int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes) {
     return (ctx && planes >= 0) ? LBM_OK : LBM_ERR_BAD_ARG;
 }
+int lbm_set_step_graphs(lbm_ctx *ctx, int32_t) { return ctx ? LBM_OK : LBM_ERR_BAD_ARG; }
 int lbm_launch_count(int64_t *count) {
     if (!count) return LBM_ERR_BAD_ARG;
     *count = 0;

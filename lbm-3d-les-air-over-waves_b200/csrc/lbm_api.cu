@@ -100,6 +100,8 @@ struct lbm_ctx {
     bool graphs = false, capturing = false, warm = false;
     int64_t cap_n0 = 0;
     long long *dclock = nullptr;
+    float *stash = nullptr;     // FP32 post-condition populations of the general planes (16-bit storage)
+    size_t stash_cells = 0;
     std::vector<StepGraph> graph_cache;
     // tensor maps of f[0] and f[1] for the tile-copy interior kernel: boxes 24x18 and 20x18
     CUtensorMap tmap[2][2];
@@ -135,6 +137,12 @@ static int cuda_check(lbm_ctx *c, cudaError_t e, const char *what) {
         if (_s != LBM_OK) return _s;                        \
     } while (0)
 #define CK_LAUNCH(what) CK(cudaGetLastError(), what)
+
+static int alloc(lbm_ctx *ctx, void **p, size_t bytes) {
+    CK(cudaMalloc(p, bytes), "scratch allocation");
+    ctx->owned.push_back(*p);
+    return LBM_OK;
+}
 
 static inline int64_t P_nx(const lbm_ctx *c) { return c->P.nx; }
 static inline int64_t P_ny(const lbm_ctx *c) { return c->P.ny; }
@@ -406,9 +414,24 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     const int64_t key0 = ctx->capturing ? ctx->cap_n0 : 0;
     A.step = (uint64_t)(n + 1 - key0);
     // with LES the pre-pass stores the post-condition populations of the
-    // general planes for their collide pass (FP32 populations, column-cache path)
-    const int tflag = (R.classic ? F_TILE_CLASSIC : 0) |
-                      ((les && ctx->use_cg && ctx->P.pop_storage == LBM_STORE_F32) ? F_STASH : 0);
+    // general planes for their collide pass (column-cache path): in the
+    // destination slots with FP32 populations, else in an FP32 stash
+    // (allocated by the first eager call; a capture without it keeps the
+    // general collide's own stream pass)
+    const char *ns = getenv("LBM_B200_NO_STASH");   // the general collide repeats the stream (comparison runs)
+    bool stash = les && ctx->use_cg && !(ns && ns[0] == '1');
+    if (stash && ctx->P.pop_storage != LBM_STORE_F32) {
+        const size_t ng = (size_t)(R.zcnt[0] + R.zcnt[1] + R.zcnt[2]) * P_nx(ctx) * P_ny(ctx);
+        if (ctx->stash_cells < ng && !ctx->capturing) {
+            float *p = nullptr;
+            if ((s = alloc(ctx, (void **)&p, 19 * ng * sizeof(float))) != LBM_OK) return s;
+            ctx->stash = p;
+            ctx->stash_cells = ng;
+        }
+        stash = ctx->stash_cells >= ng;
+        A.stash = ctx->stash;
+    }
+    const int tflag = (R.classic ? F_TILE_CLASSIC : 0) | (stash ? F_STASH : 0);
     A.flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
     // fused interior steps with LES and FP32 populations: the tile-copy kernel (32-bit population indices)
     const bool tma = R.tile && les && !R.classic && !R.no_tma && ctx->P.pop_storage == LBM_STORE_F32 &&
@@ -603,11 +626,6 @@ int lbm_create(const lbm_params *params, lbm_ctx **out) {
     return LBM_OK;
 }
 
-static int alloc(lbm_ctx *ctx, void **p, size_t bytes) {
-    CK(cudaMalloc(p, bytes), "scratch allocation");
-    ctx->owned.push_back(*p);
-    return LBM_OK;
-}
 
 int lbm_bind(lbm_ctx *ctx, const lbm_buffers *bufs) {
     if (!ctx || !bufs) return LBM_ERR_BAD_ARG;

@@ -307,9 +307,19 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_prepas
     A.u_out[c] = vx;
     A.u_out[A.D.n + c] = vy;
     A.u_out[2 * A.D.n + c] = vz;
-    // the collide pass of these cells reads the populations back from its
-    // own destination slots (FP32 only: exact round trip)
-    if (CG && S == LBM_STORE_F32 && (A.flags & F_STASH)) store_cell<S>(A, c, f);
+    // the collide pass of these cells reads the populations back: from its
+    // own destination slots (FP32), or from the FP32 stash indexed by the
+    // launch's plane (16-bit storage would round them)
+    if (CG && (A.flags & F_STASH)) {
+        if (S == LBM_STORE_F32) {
+            store_cell<S>(A, c, f);
+        } else {
+            const size_t ng = (size_t)gridDim.z * A.D.nx * A.D.ny;
+            const size_t g = ((size_t)blockIdx.z * A.D.ny + j) * A.D.nx + i;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) A.stash[q * ng + g] = f[q];
+        }
+    }
 }
 
 template <int S, int IN, bool CG>
@@ -319,12 +329,20 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collid
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
-    if (CG && S == LBM_STORE_F32 && (A.flags & F_STASH)) {
+    if (CG && (A.flags & F_STASH)) {
         // populations after stream, boundary conditions and condition
-        // stage, left in the destination slots by the pre-pass
-        const float *fd = (const float *)A.fdst;
+        // stage, left by the pre-pass in the destination slots (FP32) or
+        // in the stash (16-bit storage)
+        if (S == LBM_STORE_F32) {
+            const float *fd = (const float *)A.fdst;
 #pragma unroll
-        for (int q = 0; q < 19; ++q) f[q] = fd[(size_t)q * A.D.n + c];
+            for (int q = 0; q < 19; ++q) f[q] = fd[(size_t)q * A.D.n + c];
+        } else {
+            const size_t ng = (size_t)gridDim.z * A.D.nx * A.D.ny;
+            const size_t g = ((size_t)blockIdx.z * A.D.ny + j) * A.D.nx + i;
+#pragma unroll
+            for (int q = 0; q < 19; ++q) f[q] = A.stash[q * ng + g];
+        }
         GeoLinks Lc;
         Geo gc = geo_cell<CG>(A.P, A.slot, A.D, A.bed_c, k, j, i, Lc, true, false);
         fast_c = gc.fast;

@@ -46,6 +46,7 @@ struct StepArgs {
     unsigned *status;    // bit 0: non-finite density
     uint64_t step;       // 1-based step number of the collide stage (RNG key); with clock, the offset from *clock
     const long long *clock;  // device step clock of a captured step graph (null: step is absolute)
+    float *stash;        // 16-bit storage with F_STASH: [19][general cells of the launch] FP32 post-condition populations
     int flags;
     // z planes covered by a launch: up to 3 ranges [zlo, zlo + zcnt), grid.z = sum of zcnt
     int zlo[3], zcnt[3];

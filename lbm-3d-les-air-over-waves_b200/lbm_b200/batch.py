@@ -93,6 +93,11 @@ def domain_bytes(cfg, with_diag: bool = False) -> int:
     total += 12 * n + 2 * 42 * 4 * a + 4096     # LES velocity planes, bed slots + column caches, counters
     if getattr(cfg, "free_surface_tracking_mode", "height") == "vof" and getattr(cfg, "water_free_surface_enabled", 0):
         total += 52 * n
+    if getattr(cfg, "pop_storage", "f32") != "f32":
+        # FP32 stash of the general planes (the bed band and the top row): 76 B per cell
+        dx = float(getattr(cfg, "dx", 1.0)) or 1.0
+        band = int(np.ceil((float(getattr(cfg, "offset_m", 0.0)) + 2.0 * float(getattr(cfg, "bed_amp_m", 0.0))) / dx)) + 4
+        total += 76 * a * min(cfg.Nz, band)
     return total
 
 

@@ -367,27 +367,31 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// Tensor maps over the FP32 populations f[q][z][y][x] as a 4-D tensor
-// (x, y, z, q) for the tile-copy interior kernel.  Requirements of tile
-// copies: 16-byte aligned base, strides multiples of 16 bytes (nx multiple
-// of 4), inner box extent a multiple of 16 bytes (24 and 20 floats).
+// Tensor maps over the populations f[q][z][y][x] as a 4-D tensor
+// (x, y, z, q) for the tile-copy interior kernel.  FP32: boxes 24 and 20
+// values wide; 16-bit storage: one box 32 values wide (both map slots).
+// Requirements of tile copies: 16-byte aligned base, strides multiples of
+// 16 bytes (nx a multiple of 8), inner box extent a multiple of 16 bytes.
 static bool tile_maps_ready(lbm_ctx *ctx) {
     if (ctx->tmap_ok && ctx->tmap_src[0] == ctx->b.f[0] && ctx->tmap_src[1] == ctx->b.f[1]) return true;
     ctx->tmap_ok = false;
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return false;
+    const bool f32 = ctx->P.pop_storage == LBM_STORE_F32;
+    const cuuint64_t es_b = f32 ? 4 : 2;
     const cuuint64_t nx = (cuuint64_t)ctx->P.nx, ny = (cuuint64_t)ctx->P.ny, nz = (cuuint64_t)ctx->P.nz;
-    if (nx % 4 != 0) return false;
+    if (nx % 8 != 0) return false;
     const cuuint64_t dims[4] = {nx, ny, nz, 19};
-    const cuuint64_t strides[3] = {nx * 4, nx * ny * 4, nx * ny * nz * 4};
+    const cuuint64_t strides[3] = {nx * es_b, nx * ny * es_b, nx * ny * nz * es_b};
     const cuuint32_t es[4] = {1, 1, 1, 1};
     for (int b = 0; b < 2; ++b) {
         if (((uintptr_t)ctx->b.f[b] & 15u) != 0) return false;
         for (int w = 0; w < 2; ++w) {
-            const cuuint32_t box[4] = {w == 0 ? 24u : 20u, (cuuint32_t)(LBM_TILE + 2), 1u, 1u};
-            if (enc(&ctx->tmap[b][w], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ctx->b.f[b], dims, strides, box, es,
-                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            const cuuint32_t width = f32 ? (w == 0 ? 24u : 20u) : 32u;
+            const cuuint32_t box[4] = {width, (cuuint32_t)(LBM_TILE + 2), 1u, 1u};
+            if (enc(&ctx->tmap[b][w], f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 4,
+                    ctx->b.f[b], dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
                 return false;
         }
     }
@@ -433,9 +437,9 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     }
     const int tflag = (R.classic ? F_TILE_CLASSIC : 0) | (stash ? F_STASH : 0);
     A.flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
-    // fused interior steps with LES and FP32 populations: the tile-copy kernel (32-bit population indices)
-    const bool tma = R.tile && les && !R.classic && !R.no_tma && ctx->P.pop_storage == LBM_STORE_F32 &&
-                     19.0 * (double)ctx->D.n < 2147483647.0 && tile_maps_ready(ctx);
+    // fused interior steps with LES: the tile-copy kernel (32-bit population indices)
+    const bool tma = R.tile && les && !R.classic && !R.no_tma && 19.0 * (double)ctx->D.n < 2147483647.0 &&
+                     tile_maps_ready(ctx);
     if (les) {
         launch_step_kernel(KER_PREPASS_CANON, A, st);
         CK_LAUNCH("prepass");

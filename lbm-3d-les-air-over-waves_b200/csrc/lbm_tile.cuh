@@ -435,9 +435,8 @@ LBM_DEV void cp_async4v(void *smem, const void *gmem) {
 LBM_DEV int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
 template <int S, int IN, bool LES>
-__global__ void __launch_bounds__(256, 2) k_tile_pipe16(StepArgs A) {
+LBM_DEV void tile_pipe16_body(const StepArgs &A, float *smem, int bx, int by) {
     typedef typename Store<S>::T T;
-    extern __shared__ __align__(16) float smem[];
     uint32_t *sw = (uint32_t *)smem;                     // [slot][P16_MAIN] words
     uint32_t *rw = sw + PIPE_SLOTS * P16_MAIN;           // [slot][P16_RING] words
     float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =         // [plane slot][component][x][y]
@@ -445,7 +444,7 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe16(StepArgs A) {
     const lbm_params &P = A.P;
     const Dom &D = A.D;
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-    const int x0 = blockIdx.x * LBM_TILE, y0 = blockIdx.y * LBM_TILE;
+    const int x0 = bx * LBM_TILE, y0 = by * LBM_TILE;
     const int i = x0 + tx, j = y0 + ty;
     const int z0 = A.zi0 + blockIdx.z * A.chunk;
     const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
@@ -612,6 +611,12 @@ __global__ void __launch_bounds__(256, 2) k_tile_pipe16(StepArgs A) {
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
+template <int S, int IN, bool LES>
+__global__ void __launch_bounds__(256, 2) k_tile_pipe16(StepArgs A) {
+    extern __shared__ __align__(16) float smem[];
+    tile_pipe16_body<S, IN, LES>(A, smem, blockIdx.x, blockIdx.y);
+}
+
 // ------------------------------------------------ TMA-staged interior kernel
 // k_tile_tma: the fused step (pull from the previous step's post-collision
 // state) with LES for FP32 populations, staged by the tensor memory
@@ -659,6 +664,39 @@ static_assert(tma_base(1) == TMA_REG24 && tma_base(3) == TMA_REG24 + 2 * TMA_REG
               "population offsets");
 static_assert((TMA_REG24 * 4) % 128 == 0 && (TMA_REG20 * 4) % 128 == 0, "boxes start on 128-byte boundaries");
 
+// Layout of a plane slot.  FP32: boxes 24 or 20 values wide (tma_base,
+// tma_shift above).  16-bit storage: one box of 32 x 18 values per
+// population from x0 - 8 (16-byte aligned x), 1,152 bytes, which covers the
+// columns x0 - 2 .. x0 + 17 that any shift needs.
+constexpr int TMA16_W = 32, TMA16_REG = TMA16_W * TMA_H;
+template <int S> struct TmaTile {   // FP16 / BF16 shifted populations
+    typedef typename Store<S>::T T;
+    static constexpr int SLOT = 19 * TMA16_REG;                 // values per slot
+    static constexpr unsigned BYTES = 19u * TMA16_REG * 2u;     // bytes landing per plane
+    static constexpr int WA = TMA16_W, WB = TMA16_W;            // the two row pitches (one here)
+    static LBM_DEV int base(int q) { return q * TMA16_REG; }
+    static LBM_DEV int x_start(int x0, int) { return x0 - 8; }
+    __host__ __device__ static constexpr int shift(int q) { return 8 - cxq(q); }
+    __host__ __device__ static constexpr bool wide(int) { return true; }   // row pitch WA
+};
+template <> struct TmaTile<LBM_STORE_F32> {
+    typedef float T;
+    static constexpr int SLOT = TMA_SLOT;
+    static constexpr unsigned BYTES = TMA_BYTES;
+    static constexpr int WA = 24, WB = 20;
+    static LBM_DEV int base(int q) { return tma_base(q); }
+    static LBM_DEV int x_start(int x0, int cx) { return cx < 0 ? x0 : x0 - 4; }
+    __host__ __device__ static constexpr int shift(int q) { return tma_shift(q); }
+    __host__ __device__ static constexpr bool wide(int q) { return cxq(q) == 0; }
+};
+template <int S>
+constexpr int tma_smem_bytes() {
+    return 128 + PIPE_SLOTS * TmaTile<S>::SLOT * (int)sizeof(typename TmaTile<S>::T) +
+           3 * 3 * (LBM_TILE + 2) * (LBM_TILE + 2) * 4 + PIPE_SLOTS * 8;
+}
+static_assert((TMA16_REG * 2) % 128 == 0, "16-bit boxes start on 128-byte boundaries");
+static_assert(tma_smem_bytes<LBM_STORE_F32>() == TMA_SMEM_BYTES, "FP32 slot layout");
+
 LBM_DEV unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 LBM_DEV void mbar_init(unsigned bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
@@ -683,13 +721,16 @@ LBM_DEV void tma_load_4d(unsigned dst, const CUtensorMap *map, int x, int y, int
         : "memory");
 }
 
+template <int S>
 __global__ void __launch_bounds__(256, 2)
     k_tile_tma(StepArgs A, const __grid_constant__ CUtensorMap m24, const __grid_constant__ CUtensorMap m20) {
+    typedef TmaTile<S> L;
+    typedef typename L::T T;
     extern __shared__ __align__(128) unsigned char tma_smem[];
-    float *sf = (float *)(tma_smem + ((128u - (smem_addr(tma_smem) & 127u)) & 127u));   // [slot][TMA_SLOT]
+    T *sf = (T *)(tma_smem + ((128u - (smem_addr(tma_smem) & 127u)) & 127u));   // [slot][L::SLOT]
     float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =        // [plane slot][component][x][y]
-        (float (*)[3][LBM_TILE + 2][LBM_TILE + 2])(sf + PIPE_SLOTS * TMA_SLOT);
-    uint64_t *bar = (uint64_t *)(sf + PIPE_SLOTS * TMA_SLOT + 3 * 3 * (LBM_TILE + 2) * (LBM_TILE + 2));
+        (float (*)[3][LBM_TILE + 2][LBM_TILE + 2])(sf + PIPE_SLOTS * L::SLOT);
+    uint64_t *bar = (uint64_t *)((float *)(sf + PIPE_SLOTS * L::SLOT) + 3 * 3 * (LBM_TILE + 2) * (LBM_TILE + 2));
     const lbm_params &P = A.P;
     const Dom &D = A.D;
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
@@ -698,7 +739,7 @@ __global__ void __launch_bounds__(256, 2)
     const int z0 = A.zi0 + blockIdx.z * A.chunk;
     const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
     const int n = (int)D.n, nxy = D.nx * D.ny;
-    float *fdst = (float *)A.fdst;
+    T *fdst = (T *)A.fdst;
     {
         const int kc = max(z0, A.zi0);
         bool ok = geo_far(P, D, A.bed_c, kc, j, i) && geo_far(P, D, A.bed_s, kc, j, i);
@@ -728,12 +769,10 @@ __global__ void __launch_bounds__(256, 2)
         if ((t & 31) == 0 && p >= A.zi0 && p <= A.zi1 && p <= z1) {
             const int slot = p % PIPE_SLOTS;
             const unsigned b = smem_addr(bar + slot);
-            if (t == 0) mbar_expect_tx(b, TMA_BYTES);
+            if (t == 0) mbar_expect_tx(b, L::BYTES);
             for (int q = t >> 5; q < 19; q += 8) {
-                const int cx = cxq(q);
-                const int qb = TMA_REG20 * q + (TMA_REG24 - TMA_REG20) * __popc(TMA_CX0 & ((1u << q) - 1u));   // tma_base(q)
-                tma_load_4d(smem_addr(sf + slot * TMA_SLOT + qb), cx == 0 ? &m24 : &m20, cx < 0 ? x0 : x0 - 4,
-                            y0 - 1 - cyq(q), p - czq(q), q, b);
+                tma_load_4d(smem_addr(sf + slot * L::SLOT + L::base(q)), L::wide(q) ? &m24 : &m20,
+                            L::x_start(x0, cxq(q)), y0 - 1 - cyq(q), p - czq(q), q, b);
             }
         }
     };
@@ -761,24 +800,26 @@ __global__ void __launch_bounds__(256, 2)
         __syncthreads();        // slot (p + 1) % 3 is free: every thread is done with plane p - 2
         issue(p + 1);
         float r = 0.0f;
-        const float *sb = sf + sl * TMA_SLOT;
+        const T *sb = sf + sl * L::SLOT;
         if (interior) {
             if (ring) {
-                // ring cell: box row ry + 1, column rx + tma_shift(q)
+                // ring cell: box row ry + 1, column rx + L::shift(q)
                 float fr[19], rr, a, b, d;
-                const float *b24 = sb + (ry + 1) * 24 + rx, *b20 = sb + (ry + 1) * 20 + rx;
+                const T *bA = sb + (ry + 1) * L::WA + rx, *bB = sb + (ry + 1) * L::WB + rx;
 #pragma unroll
-                for (int q = 0; q < 19; ++q) fr[q] = (cxq(q) == 0 ? b24 : b20)[tma_base(q) + tma_shift(q)];
+                for (int q = 0; q < 19; ++q)
+                    fr[q] = Store<S>::ld_rw(L::wide(q) ? bA : bB, (size_t)(L::base(q) + L::shift(q)), q, P.rho0);
                 macro(P, D, fr, p, false, LBM_FS_LIQUID, 0.0f, rr, a, b, d);
                 su[sl][0][rx + 1][ry + 1] = a;
                 su[sl][1][rx + 1][ry + 1] = b;
                 su[sl][2][rx + 1][ry + 1] = d;
             }
-            // own cell: box row ty + 1, column tx + tma_shift(q)
+            // own cell: box row ty + 1, column tx + L::shift(q)
             float fc[19], vx, vy, vz;
-            const float *b24 = sb + (ty + 1) * 24 + tx, *b20 = sb + (ty + 1) * 20 + tx;
+            const T *bA = sb + (ty + 1) * L::WA + tx, *bB = sb + (ty + 1) * L::WB + tx;
 #pragma unroll
-            for (int q = 0; q < 19; ++q) fc[q] = (cxq(q) == 0 ? b24 : b20)[tma_base(q) + tma_shift(q)];
+            for (int q = 0; q < 19; ++q)
+                fc[q] = Store<S>::ld_rw(L::wide(q) ? bA : bB, (size_t)(L::base(q) + L::shift(q)), q, P.rho0);
             macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
             su[sl][0][tx + 1][ty + 1] = vx;
             su[sl][1][tx + 1][ty + 1] = vy;
@@ -821,13 +862,14 @@ __global__ void __launch_bounds__(256, 2)
             }
             if (!(rp == rp) || fabsf(rp) > 3.0e38f) atomicOr(A.status, 1u);
             float fp[19];
-            const float *pb = sf + s0 * TMA_SLOT;
-            const float *b24 = pb + (ty + 1) * 24 + tx, *b20 = pb + (ty + 1) * 20 + tx;
+            const T *pb = sf + s0 * L::SLOT;
+            const T *bA = pb + (ty + 1) * L::WA + tx, *bB = pb + (ty + 1) * L::WB + tx;
 #pragma unroll
-            for (int q = 0; q < 19; ++q) fp[q] = (cxq(q) == 0 ? b24 : b20)[tma_base(q) + tma_shift(q)];
+            for (int q = 0; q < 19; ++q)
+                fp[q] = Store<S>::ld_rw(L::wide(q) ? bA : bB, (size_t)(L::base(q) + L::shift(q)), q, P.rho0);
             collide(A, c, k, false, false, false, 0.0f, rp, vxp, vyp, vzp, om, fp);
 #pragma unroll
-            for (int q = 0; q < 19; ++q) fdst[q * n + c] = fp[q];
+            for (int q = 0; q < 19; ++q) Store<S>::st(fdst, (size_t)(q * n + c), fp[q], q, P.rho0);
         }
         rp = r;
     }
@@ -850,15 +892,17 @@ LBM_DEV void edge_tile(int e, int TX, int TY, int &bx, int &by) {
 }
 
 // the fused interior step with LES on the edge tiles (grid.x = their
-// count), cp.async-staged.  k_tile_tma is launched after it as a
+// count), cp.async-staged (k_tile_pipe's or k_tile_pipe16's body).  k_tile_tma is launched after it as a
 // programmatic dependent: it may start as soon as every block of this grid
 // is running (the two grids share no output)
+template <int S>
 __global__ void __launch_bounds__(256, 2) k_tile_edges(StepArgs A) {
     extern __shared__ __align__(16) float smem[];
     asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     int bx = 0, by = 0;
     edge_tile(blockIdx.x, A.D.nx / LBM_TILE, A.D.ny / LBM_TILE, bx, by);
-    tile_pipe_body<1, true>(A, smem, bx, by);
+    if constexpr (S == LBM_STORE_F32) tile_pipe_body<1, true>(A, smem, bx, by);
+    else tile_pipe16_body<S, 1, true>(A, smem, bx, by);
 }
 
 // stream only (the last pass of a call) for interior cells

@@ -88,7 +88,10 @@ class Server:
 
         from .domain import Domain
 
-        return Domain(env, device=self.device, stream=torch.cuda.Stream(torch.device(self.device)), with_diag=False)
+        dom = Domain(env, device=self.device, stream=torch.cuda.Stream(torch.device(self.device)), with_diag=False)
+        if dom.cfg.physics_mode == "air":
+            dom.set_step_graphs(True)   # rounds of `chunk` steps replay one captured graph per call shape
+        return dom
 
     @staticmethod
     def _result(dom) -> dict:

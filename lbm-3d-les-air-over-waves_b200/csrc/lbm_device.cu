@@ -179,6 +179,9 @@ __global__ void k_colgeo(lbm_params P, Dom D, BedView B, float *cg) {
 #ifndef LBM_GEN_MINB
 #define LBM_GEN_MINB 1
 #endif
+#ifndef LBM_CG_PRE_MINB
+#define LBM_CG_PRE_MINB 3   // the column-cache pre-pass: 3 blocks of 256 per SM (85 registers)
+#endif
 #ifndef LBM_CG_MINB
 #define LBM_CG_MINB 2
 #endif
@@ -297,7 +300,7 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
 }
 
 template <int S, int IN, bool CG>
-__global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_prepass(StepArgs A) {
+__global__ void __launch_bounds__(256, CG ? LBM_CG_PRE_MINB : LBM_GEN_MINB) k_prepass(StepArgs A) {
     int i, j, k, c;
     if (!cell_xyz(A, i, j, k, c)) return;
     float f[19], r, vx, vy, vz, gbf;

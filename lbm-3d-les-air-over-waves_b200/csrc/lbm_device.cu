@@ -1070,6 +1070,9 @@ static bool pipe16_smem_ready() {
     return ok[dev];
 }
 
+#ifndef LBM_EDGE_CHUNK_DIV
+#define LBM_EDGE_CHUNK_DIV 2
+#endif
 template <int S>
 static bool tma_smem_ready() {
     static bool done[64] = {false}, ok[64] = {false};
@@ -1094,7 +1097,12 @@ static bool launch_tile_tma_s(const StepArgs &A, const CUtensorMap *m24, const C
     if (TX < 3 || TY < 3 || !tma_smem_ready<S>()) return false;   // no tile off the edge
     const unsigned zc = (unsigned)((ni + A.chunk - 1) / A.chunk);
     const int edge_bytes = S == LBM_STORE_F32 ? PIPE_SMEM_BYTES : P16_SMEM_BYTES;
-    k_tile_edges<S><<<dim3(2 * TX + 2 * TY - 4, 1, zc), 256, edge_bytes, st>>>(A);
+    // the edge grid marches shorter z chunks: more, shorter blocks, so that
+    // its last wave ends sooner and the grid behind it starts sooner
+    StepArgs Ae = A;
+    Ae.chunk = A.chunk / LBM_EDGE_CHUNK_DIV > 8 ? A.chunk / LBM_EDGE_CHUNK_DIV : (A.chunk < 8 ? A.chunk : 8);
+    const unsigned zce = (unsigned)((ni + Ae.chunk - 1) / Ae.chunk);
+    k_tile_edges<S><<<dim3(2 * TX + 2 * TY - 4, 1, zce), 256, edge_bytes, st>>>(Ae);
     LAUNCHED(1);
     // tiles off the edge: a programmatic dependent launch (it may start while
     // the grid above drains; plain stream order when the attribute is refused)

@@ -8,12 +8,14 @@ Workload: air over a moving sinusoidal bed, 512x256x256 cells, FP32
 populations (A-B buffers, 5.1 GB, larger than L2), regularized collision,
 Smagorinsky Cs = 0.16, tau0 = 0.52, bed z = 8 + 4 sin(2 pi (x - 0.02 t)/64),
 seeded synthetic initial state.  Steps run through the public C ABI in
-chunks of 100 (the reference's health-report cadence).
+chunks of 100 (the reference's health-report cadence); in the timed region
+each chunk is one CUDA step-graph replay (--no-graphs: eager calls).
 
 Printed (rank 0, one JSON line): MLUPS over all ranks (replicas, weak
-scaling; device time, max over ranks), the roofline of the dominant kernel
-(the interior one-pass step kernel, timed live with CUDA events on its
-stream), the end-to-end figure through the API with host buffers, the SM
+scaling; device time, max over ranks), the roofline of the dominant kernels
+(the interior grids, timed with CUDA events on their stream over the same
+K steps run as eager calls right after the timed region), the end-to-end
+figure through the API with host buffers, the SM
 clocks sampled during the timed region, and the CPU oracle timed on a
 bounded sample of the same workload.
 

@@ -17,7 +17,12 @@ scaling; device time, max over ranks), the roofline of the dominant kernels
 K steps run as eager calls right after the timed region), the end-to-end
 figure through the API with host buffers, the SM
 clocks sampled during the timed region, and the CPU oracle timed on a
-bounded sample of the same workload.
+bounded sample of the same workload.  On one GPU the same line also
+carries the batched and served halves of the metric: "batched" (the
+96-domain ensemble in shifted FP16, MLUPS and its ratio to the plain
+figure) and "serving" (a seeded Poisson request trace through the
+continuous-batching server: p50/p99 latency and aggregate MLUPS);
+--plain-only skips them.
 
 --impl reference times the reference algorithm's CPU implementation (the
 FP32 C++ restatement in oracle/, OpenMP over all host cores) on a bounded
@@ -29,7 +34,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -49,7 +53,15 @@ METRIC, UNIT = "MLUPS", "MLUPS"
 # bounded CPU samples: periodic sub-blocks of the workload with its full height
 # (same bed, same vertical structure), largest first
 CPU_SAMPLES = [(128, 64, 256), (64, 64, 256), (64, 32, 256), (64, 16, 256)]
-PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_tile_air_interior.md")
+# DRAM bytes per cell update of the interior grids, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum over one launch of each
+# interior grid, divided by the cells of the launch).  A profile figure, not
+# a live one: the source says which grid, kernels and commit it was taken on.
+PROFILE_TRAFFIC = {
+    "bytes_per_cell": 163.9,
+    "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, k_tile_edges + k_tile_tma, 256x256x96 air "
+              "(scaled per cell to the launch), commit 6a8f1aa; profiles/k_tile_air_interior.md",
+}
 
 
 def workload_env(nx=None, ny=None, nz=None, seed=12345):
@@ -209,20 +221,6 @@ def reference_arm(args):
 
 
 # ------------------------------------------------------------------ GPU arm
-def profile_traffic_per_cell():
-    """DRAM bytes per cell update of the interior kernel from the committed
-    ncu summary (a line 'dram_bytes_per_cell: X')."""
-    try:
-        with open(PROFILE_SUMMARY) as fh:
-            for line in fh:
-                m = re.match(r"\s*[-*]?\s*dram_bytes_per_cell:\s*([0-9.]+)", line)
-                if m:
-                    return float(m.group(1))
-    except OSError:
-        pass
-    return None
-
-
 def measured_hbm_peak():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
@@ -279,10 +277,16 @@ def ours(args):
     # CHUNK steps one graph launch; the shapes of the timed calls are
     # captured in warm-up)
     graphs = not args.no_graphs
+    extra_warm = 0
     if graphs:
+        # The timed region's calls are replays of captured graphs: step graphs
+        # are cached per (steps per call, step parity, current buffer), and
+        # two passes of the timed call sequence capture every one of them
+        # (parity and buffer flip together, once per step).
         dom.set_step_graphs(True)
-        run_steps(dom, 2 * CHUNK)
-        W += 2 * CHUNK
+        run_steps(dom, K)
+        run_steps(dom, K)
+        extra_warm = 2 * K
         dom.synchronize()
     l0 = C.c_int64()
     lib.lbm_launch_count(C.byref(l0))
@@ -366,9 +370,9 @@ def ours(args):
         if k_launches > 0 and k_ms > 0:
             per_launch_s = k_ms / k_launches * 1e-3
             achieved = B_ALG * k_cells / per_launch_s / 1e9
-            tpc = profile_traffic_per_cell()
+            tpc = PROFILE_TRAFFIC["bytes_per_cell"]
             roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": (tpc * k_cells) if tpc else None, "peak_kind": peak_kind,
+                    "traffic": tpc * k_cells, "traffic_source": PROFILE_TRAFFIC["source"], "peak_kind": peak_kind,
                     "kernel": "k_tile_edges + k_tile_tma (interior one-pass stream+LES+collide; TMA-staged off the domain edge)", "cells_per_launch": k_cells,
                     "bytes_per_cell": B_ALG, "launch_ms": per_launch_s * 1e3,
                     "step_frac": B_ALG * value * 1e6 / world / (peak * 1e9)}
@@ -377,12 +381,15 @@ def ours(args):
             rate, sample = oracle_sample_rate(budget_s=12.0, max_steps=20)
             cpu = {"value": rate, "unit": UNIT, "cores": host_cores(), "kind": "port", "sample": sample}
         out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W + extra_warm,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": dict(base_config(), tile_chunk=tuned["chunk"],
                            tile_chunk_ms={str(k): round(v, 4) for k, v in tuned["ms_per_step"].items()},
                            step_graphs=graphs, eager_ms_per_step=round(eager_ms / K, 4),
+                           warmup_note=(f"{W} eager warm-up steps, then {extra_warm} steps that capture the timed "
+                                        f"region's step graphs; before them the autotuner's timing steps "
+                                        f"({len(tuned['ms_per_step'])} chunk candidates x 13 steps)"),
                            roofline_timing="interior grids timed with CUDA events over the same K steps run as "
                                            "eager calls right after the timed region"),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K},
@@ -390,6 +397,23 @@ def ours(args):
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
         }
     dom.close()
+    del dom
+    if out is not None and world == 1 and not args.plain_only:
+        # the batched and served halves of the metric, same process and GPU
+        import torch
+
+        torch.cuda.empty_cache()
+        storage = args.storage or "f16s"
+        b = run_batched(args.domains, args.batched_steps, 3, storage, graphs=not args.no_graphs)
+        b["vs_plain"] = b["value"] / value
+        out["batched"] = b
+        torch.cuda.empty_cache()
+        srv = run_serving(args.requests, args.min_steps, args.max_steps, storage)
+        srv["vs_plain"] = srv["value"] / value
+        srv["reduction"] = (f"{args.requests} requests with {args.min_steps}-{args.max_steps} steps each, against "
+                            f"200 requests with 500-5000 steps in the full trace, so that the run takes minutes")
+        out["serving"] = srv
+        torch.cuda.empty_cache()
     reps.close()
     if out is not None:
         print(json.dumps(out), flush=True)
@@ -417,59 +441,89 @@ def _device_time(streams, fn):
     return e0.elapsed_time(e1)
 
 
-def batched(args):
-    """The batched ensemble: 96 seeded air-over-wave domains of uneven size,
-    shifted-FP16 populations by default, all stepped together."""
-    import torch
-
+def run_batched(domains: int, K: int, W: int, storage: str, graphs: bool = True) -> dict:
+    """The batched ensemble (seeded air-over-wave domains of uneven size),
+    all stepped together; device time of K ensemble steps."""
     from lbm_b200.batch import Batch, stable_ensemble_envs
 
-    storage = args.storage or "f16s"
-    envs = stable_ensemble_envs(args.domains, seed=7, storage=storage)
-    b = Batch(envs, chunk=25, graphs=not args.no_graphs)
-    K, W = args.steps, max(args.warmup, 3)
-    if not args.no_graphs:
+    envs = stable_ensemble_envs(domains, seed=7, storage=storage)
+    b = Batch(envs, chunk=25, graphs=graphs)
+    W = max(W, 3)
+    if graphs:
         W = max(W, 3 * b.chunk)   # an eager call, then the captures of both step parities
     b.step(W)
     b.synchronize()
-    ms = _device_time([d.stream for d in b.domains], lambda: b.step(K))
+    l0 = _launches()
+    ms = _device_time(b.streams(), lambda: b.step(K))
+    launches = _launches() - l0
     cells = b.cells
-    bytes_cell = 76 if storage != "f32" else 152
-    line = {
-        "metric": METRIC, "value": cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": 1, "steps": K,
-        "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if storage == "f32" else f"f32 compute, {storage} storage", "data": "synthetic",
-        "mode": "batched",
-        "config": {"workload": f"batched ensemble of {len(envs)} air-over-wave domains (seed 7, stability-screened "
-                               f"draws), uneven sizes",
-                   "cells": cells, "storage": storage, "steps_per_call": b.chunk,
-                   "streams": len(envs), "step_graphs": not args.no_graphs},
-        "roofline_step_frac": bytes_cell * cells * K / (ms * 1e-3) / (measured_hbm_peak()[0] * 1e9),
-    }
     for d in b.domains:
         if d.counters()["status_flags"]:
             raise SystemExit("non-finite state in the batched run")
+    bytes_cell = 76 if storage != "f32" else 152
+    out = {
+        "value": cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "steps": K, "warmup": W, "ms_per_step": ms / K,
+        "domains": len(envs), "cells": cells, "storage": storage, "bytes_per_cell": bytes_cell,
+        "step_graphs": graphs, "launch": b.mode, "gpu_launches": launches,
+        "roofline_step_frac": bytes_cell * cells * K / (ms * 1e-3) / (measured_hbm_peak()[0] * 1e9),
+        "workload": f"batched ensemble of {len(envs)} air-over-wave domains (seed 7, stability-screened draws), "
+                    f"uneven sizes nx 64-320, ny 32-160, nz 32-128",
+    }
     b.close()
+    return out
+
+
+def run_serving(requests: int, min_steps: int, max_steps: int, storage: str) -> dict:
+    """The continuous-batching request loop on a seeded Poisson trace."""
+    from lbm_b200.serving import Server, poisson_trace
+
+    reqs = poisson_trace(requests, rate_hz=20.0, seed=3, cells_range=(1e5, 2e7),
+                         steps_range=(min_steps, max_steps), storage=storage)
+    rep = Server(budget_bytes=150e9, chunk=50).run(reqs)
+    return {
+        "value": rep["mlups"], "unit": UNIT, "p50_s": rep["p50_s"], "p99_s": rep["p99_s"], "wall_s": rep["wall_s"],
+        "requests": rep["requests"], "rounds": rep["rounds"], "peak_active": rep["peak_active"],
+        "setup_s": rep["setup_s"], "storage": storage, "steps_range": [min_steps, max_steps],
+        "workload": f"Poisson(20/s) arrivals, {requests} requests, half air-over-wave, half water Gaussian, cells "
+                    f"log-uniform [1e5, 2e7], steps uniform [{min_steps}, {max_steps}], seed 3, HBM budget 150 GB",
+    }
+
+
+def _launches() -> int:
+    import ctypes as C
+
+    from lbm_b200 import native
+
+    v = C.c_int64()
+    native.load().lbm_launch_count(C.byref(v))
+    return int(v.value)
+
+
+def batched(args):
+    storage = args.storage or "f16s"
+    r = run_batched(args.domains, args.steps, args.warmup, storage, graphs=not args.no_graphs)
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": r["steps"],
+        "warmup": r["warmup"], "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if storage == "f32" else f"f32 compute, {storage} storage",
+        "data": "synthetic", "mode": "batched",
+        "config": {"workload": r["workload"], "cells": r["cells"], "storage": storage, "steps_per_call": 25,
+                   "step_graphs": r["step_graphs"], "launch": r["launch"]},
+        "gpu_launches": r["gpu_launches"], "roofline_step_frac": r["roofline_step_frac"],
+    }
     print(json.dumps(line), flush=True)
     return 0
 
 
 def serving(args):
-    """The continuous-batching request loop on a seeded Poisson trace."""
-    from lbm_b200.serving import Server, poisson_trace
-
     storage = args.storage or "f16s"
-    reqs = poisson_trace(args.requests, rate_hz=20.0, seed=3, cells_range=(1e5, 2e7),
-                         steps_range=(args.min_steps, args.max_steps), storage=storage)
-    rep = Server(budget_bytes=150e9, chunk=50).run(reqs)
+    r = run_serving(args.requests, args.min_steps, args.max_steps, storage)
     line = {
-        "metric": "MLUPS (served trace)", "value": rep["mlups"], "unit": UNIT, "n_gpus": 1,
+        "metric": "MLUPS (served trace)", "value": r["value"], "unit": UNIT, "n_gpus": 1,
         "higher_is_better": True, "mode": "serving", "data": "synthetic",
-        "p50_s": rep["p50_s"], "p99_s": rep["p99_s"], "wall_s": rep["wall_s"], "requests": rep["requests"],
-        "rounds": rep["rounds"], "peak_active": rep["peak_active"], "setup_s": rep["setup_s"],
-        "config": {"workload": "Poisson(20/s) arrivals, half air-over-wave, half water Gaussian, cells log-uniform "
-                               "[1e5, 2e7], seed 3", "steps_range": [args.min_steps, args.max_steps],
-                   "storage": storage, "hbm_budget_gb": 150, "round_steps": 50},
+        "p50_s": r["p50_s"], "p99_s": r["p99_s"], "wall_s": r["wall_s"], "requests": r["requests"],
+        "rounds": r["rounds"], "peak_active": r["peak_active"], "setup_s": r["setup_s"],
+        "config": {"workload": r["workload"], "storage": storage, "hbm_budget_gb": 150, "round_steps": 50},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -487,9 +541,12 @@ def main():
     ap.add_argument("--storage", choices=("f32", "f16s", "bf16s"), default=None,
                     help="population storage of the batched and serving modes (default f16s)")
     ap.add_argument("--domains", type=int, default=96, help="batched mode: ensemble size")
-    ap.add_argument("--requests", type=int, default=24, help="serving mode: trace length")
-    ap.add_argument("--min-steps", type=int, default=100, help="serving mode: fewest steps of a request")
-    ap.add_argument("--max-steps", type=int, default=600, help="serving mode: most steps of a request")
+    ap.add_argument("--requests", type=int, default=32, help="serving: trace length")
+    ap.add_argument("--min-steps", type=int, default=100, help="serving: fewest steps of a request")
+    ap.add_argument("--max-steps", type=int, default=1000, help="serving: most steps of a request")
+    ap.add_argument("--batched-steps", type=int, default=100, help="plain mode: timed steps of the batched sub-run")
+    ap.add_argument("--plain-only", action="store_true",
+                    help="plain mode: skip the batched and serving sub-runs")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the timed CPU oracle sample")
     ap.add_argument("--no-graphs", action="store_true",
                     help="time eager step calls instead of CUDA step-graph replays")

@@ -236,7 +236,10 @@ typedef struct lbm_counters {
     int32_t free_surface_vof_detached_advect_count;
     int32_t free_surface_vof_detached_compress_count;
     int32_t boundary_cut_link_count;
-    int32_t status_flags;                /* bit 0: non-finite density seen */
+    int32_t status_flags;                /* bit 0: non-finite density seen; bit 1: an interior-kernel
+                                            precondition (cell far from the bed) failed; bit 2: a
+                                            bounded wait for a tile copy gave up (that launch's
+                                            results are incomplete) */
     float free_surface_vof_collapse_candidate_volume_m3;
     float free_surface_vof_collapse_applied_volume_m3;
     float free_surface_vof_collapse_removal_scale;
@@ -342,8 +345,11 @@ int lbm_launch_count(int64_t *count);
    rejected with LBM_ERR_BAD_ARG.  Bed geometry only (no cube, no phi
    geometry, periodic x), else LBM_ERR_UNSUPPORTED.  Runs on the calling
    thread's current device, asynchronously on stream (which must belong to
-   that device).  The first call on a device looks up the array's device
-   address; make that first call before any stream capture.  All calls
+   that device).  Outside stream capture every call looks up the array's
+   device address afresh, so a device reset or a new driver context is
+   picked up; a call made while stream is being captured uses the address
+   of the last call on that device outside capture, so make one call
+   before any capture (and again after a device reset).  All calls
    share the one array: calls that overlap on the GPU (other streams, other
    threads) race and must be serialised by the caller.  Each call rewrites
    every entry it reads, so nothing needs clearing between calls.  err (may

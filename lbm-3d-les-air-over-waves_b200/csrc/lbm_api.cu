@@ -435,7 +435,11 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
         stash = ctx->stash_cells >= ng;
         A.stash = ctx->stash;
     }
-    const int tflag = (R.classic ? F_TILE_CLASSIC : 0) | (stash ? F_STASH : 0);
+    // LBM_B200_TEST_TMA_TIMEOUT=1: the tile-copy kernel takes its wait-timeout
+    // exit (status bit 2) at its first plane; used only by the error-path test
+    const char *tt = getenv("LBM_B200_TEST_TMA_TIMEOUT");
+    const int tflag = (R.classic ? F_TILE_CLASSIC : 0) | (stash ? F_STASH : 0) |
+                      ((tt && tt[0] == '1') ? F_TEST_WAIT_TIMEOUT : 0);
     A.flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
     // fused interior steps with LES: the tile-copy kernel (32-bit population indices)
     const bool tma = R.tile && les && !R.classic && !R.no_tma && 19.0 * (double)ctx->D.n < 2147483647.0 &&

@@ -1500,21 +1500,30 @@ __global__ void k_noalloc_links(lbm_params P, Dom D, const float *__restrict__ b
 
 // Device address of g_noalloc_endpoints on the current device.  In host
 // code the array's name is only a host-side stand-in, so the address is
-// looked up once per device (with that device current) and kept.
+// looked up with the device current.  Outside stream capture it is looked
+// up on every call (a device reset or another driver context loads the
+// module again, at a new address) and remembered per device; while the
+// stream is being captured the remembered address is used, since a lookup
+// may have to load the module, which capture does not allow.
 static std::mutex g_noalloc_mutex;
 static float *g_noalloc_address[LBM_MAX_DEVICES] = {};
 
-static cudaError_t noalloc_endpoints_address(float **out) {
+static cudaError_t noalloc_endpoints_address(cudaStream_t st, float **out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= LBM_MAX_DEVICES) return cudaErrorInvalidDevice;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_address[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void *p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_endpoints);
         if (e != cudaSuccess) return e;
         g_noalloc_address[dev] = (float *)p;
+    } else if (!g_noalloc_address[dev]) {
+        return cudaErrorStreamCaptureUnsupported;   // no call outside capture on this device yet
     }
     *out = g_noalloc_address[dev];
     return cudaSuccess;
@@ -1556,7 +1565,8 @@ extern "C" int lbm_link_geometry_noalloc(const lbm_params *params, const float *
                             "lbm_link_geometry_noalloc: only bed geometry with periodic x is supported "
                             "(no cube, no phi geometry, no solid x walls)");
     float *cache = nullptr;
-    cudaError_t e = noalloc_endpoints_address(&cache);
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = noalloc_endpoints_address(st, &cache);
     if (e != cudaSuccess) {
         char msg[200];
         snprintf(msg, sizeof msg, "lbm_link_geometry_noalloc: device address of the fixed array: %s",
@@ -1577,7 +1587,6 @@ extern "C" int lbm_link_geometry_noalloc(const lbm_params *params, const float *
     E.lattice_open = lattice_open;
     E.lattice_open_frac = lattice_open_frac;
     E.lattice_wall_type = lattice_wall_type;
-    cudaStream_t st = (cudaStream_t)stream;
     k_noalloc_endpoints<<<blocks_for(D.a, 128), 128, 0, st>>>(P, D, bed_h, cache); LAUNCHED(1);
     k_noalloc_links<<<blocks_for(D.n, 256), 256, 0, st>>>(P, D, bed_h, cache, E); LAUNCHED(1);
     e = cudaGetLastError();

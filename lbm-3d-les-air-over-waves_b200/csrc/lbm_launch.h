@@ -16,6 +16,7 @@ enum : int {
     F_VOF_STATE = 8,        // free-surface state from stored type/fill (else from column height)
     F_TILE_CLASSIC = 16,    // interior planes: the unpipelined tile kernel even for FP32
     F_STASH = 32,           // general planes: the pre-pass leaves its populations in the destination for the collide
+    F_TEST_WAIT_TIMEOUT = 64,  // tile-copy kernel: treat the first wait as timed out (tests of the error path)
 };
 
 enum {

@@ -786,18 +786,36 @@ __global__ void __launch_bounds__(256, 2)
     for (int p = z0 - 1; p <= z1; ++p) {
         const int sl = p % 3;
         const bool interior = p >= A.zi0 && p <= A.zi1;
+        bool gave_up = false;
         if (interior) {
+            // bounded wait for the copies of plane p (F_TEST_WAIT_TIMEOUT:
+            // give up at once, to exercise the error path below)
             const unsigned b = smem_addr(bar + sl);
-            int it = 0;
-            while (!mbar_try_wait(b, (phase >> sl) & 1u)) {
-                if (++it == TMA_WAIT_LIMIT) {
-                    atomicOr(A.status, 4u);
-                    break;
-                }
+            if (A.flags & F_TEST_WAIT_TIMEOUT) {
+                gave_up = true;
+            } else {
+                int it = 0;
+                while (!mbar_try_wait(b, (phase >> sl) & 1u))
+                    if (++it == TMA_WAIT_LIMIT) {
+                        gave_up = true;
+                        break;
+                    }
             }
-            phase ^= 1u << sl;
         }
-        __syncthreads();        // slot (p + 1) % 3 is free: every thread is done with plane p - 2
+        // slot (p + 1) % 3 is free: every thread is done with plane p - 2
+        if (__syncthreads_or(gave_up)) {
+            // A wait gave up: status bit 2, and the whole block leaves.  The
+            // copies of plane p are the only ones in flight (plane p - 1's
+            // completed in the last iteration), so they are waited for first,
+            // again with a bound, before the block's shared memory goes away.
+            if (t == 0) atomicOr(A.status, 4u);
+            const unsigned b = smem_addr(bar + sl);
+            for (int it = 0; it < TMA_WAIT_LIMIT && !mbar_try_wait(b, (phase >> sl) & 1u); ++it) {
+            }
+            asm volatile("griddepcontrol.wait;\n" ::: "memory");
+            return;
+        }
+        if (interior) phase ^= 1u << sl;
         issue(p + 1);
         float r = 0.0f;
         const T *sb = sf + sl * L::SLOT;

@@ -122,9 +122,15 @@ class Batch:
                 if d.cfg.physics_mode == "air":
                     d.set_step_graphs(True)
 
+    mode = "one stream and one step graph per domain"
+
     @property
     def cells(self) -> int:
         return sum(d.cfg.Nx * d.cfg.Ny * d.cfg.Nz for d in self.domains)
+
+    def streams(self) -> list:
+        """The CUDA streams the ensemble's work runs on."""
+        return [d.stream for d in self.domains]
 
     def step(self, n: int):
         done = 0

@@ -1,9 +1,12 @@
 """Generate golden vectors by running the reference solver's own kernels.
 
-Run in the development container (the reference is mounted read-only at
-/root/reference; it does not exist on GPU machines):
+Run where a checkout of the reference is available (it is read, never
+written; GPU machines do not need it):
 
-    python tests/golden/gen_golden.py [--only NAME]
+    python tests/golden/gen_golden.py --reference PATH [--only NAME]
+
+PATH is the reference checkout (default: the LBM_REFERENCE_DIR environment
+variable).
 
 Each case sets LBM_* options, imports LBM_3D_LES_air_over_waves_CODEX.py
 with taichi_shim standing in for Taichi, runs main() for a few steps on a
@@ -26,8 +29,8 @@ import warnings
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE = "/root/reference"
-SOLVER = os.path.join(REFERENCE, "LBM_3D_LES_air_over_waves_CODEX.py")
+SOLVER_FILE = "LBM_3D_LES_air_over_waves_CODEX.py"
+REFERENCE = os.environ.get("LBM_REFERENCE_DIR", "")
 
 sys.path.insert(0, HERE)
 import taichi_shim  # noqa: E402
@@ -140,7 +143,7 @@ def run_case(name: str, env: dict, seed: int = 12345) -> dict:
         os.environ["LBM_TI_CACHE_DIR"] = cache
         sys.modules["taichi"] = taichi_shim
         sys.path.insert(0, REFERENCE)
-        spec = importlib.util.spec_from_file_location(f"ref_{name}", SOLVER)
+        spec = importlib.util.spec_from_file_location(f"ref_{name}", os.path.join(REFERENCE, SOLVER_FILE))
         mod = importlib.util.module_from_spec(spec)
         spec.loader.exec_module(mod)
         shape = (mod.Nz, mod.Ny, mod.Nx)
@@ -194,9 +197,14 @@ def run_case(name: str, env: dict, seed: int = 12345) -> dict:
 
 
 def main():
+    global REFERENCE
     ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=REFERENCE, help="reference checkout (default: $LBM_REFERENCE_DIR)")
     ap.add_argument("--only", default=None)
     args = ap.parse_args()
+    REFERENCE = os.path.abspath(args.reference) if args.reference else ""
+    if not REFERENCE or not os.path.exists(os.path.join(REFERENCE, SOLVER_FILE)):
+        raise SystemExit(f"{SOLVER_FILE} not found: pass --reference PATH or set LBM_REFERENCE_DIR")
     for name, env in CASES.items():
         if args.only and name != args.only:
             continue

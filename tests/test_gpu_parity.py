@@ -93,6 +93,27 @@ def test_gpu_tile_path_matches_oracle(variant, monkeypatch):
     assert not problems, "\n".join(problems[:20])
 
 
+def test_tile_copy_wait_timeout_reports_status_and_recovers(monkeypatch):
+    """The bounded mbarrier wait of the tile-copy kernel.  With the test
+    switch set, the first wait of every block gives up at once: the block
+    waits (bounded) for the copies it has in flight, leaves, and the launch
+    reports status bit 2.  No copy is skipped, so the GPU and the process
+    stay usable: a fresh domain then matches the oracle bit for bit."""
+    from lbm_b200.domain import Domain
+
+    env = air_wave_env(64, 64, 40, amp=3.0, level=6.0, wavelength=32.0)   # 2 x 2 tiles on tile copies
+    monkeypatch.setenv("LBM_B200_TEST_TMA_TIMEOUT", "1")
+    dom = Domain(env, device="cuda:0")
+    dom.step(3)       # steps 2 and 3 are fused steps: tile-copy launches
+    dom.synchronize()
+    flags = dom.counters()["status_flags"]
+    dom.close()
+    assert flags & 4, flags
+    monkeypatch.delenv("LBM_B200_TEST_TMA_TIMEOUT")
+    problems = _run_pair(env, chunks=(1, 3))
+    assert not problems, "\n".join(problems[:20])
+
+
 def test_gpu_step_chunking_is_invisible():
     """Ten steps in one call equal ten calls of one step."""
     from lbm_b200.domain import Domain

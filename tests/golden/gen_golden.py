@@ -102,8 +102,78 @@ CASES = {
                                  "LBM_GAUSSIAN_SIGMA_M": "2", "LBM_WATER_NU_M2S": "0.05"},
 }
 
+# VOF pool whose initial state is edited after the reference's own init
+# (inject_vof_features below) so that the rarely reached VOF kernels act in
+# the first steps: trapped-gas collapse (every step), the thin-gap bridge,
+# orphan removal, detached-cell advection and residual compression
+VOF_FEATURES = {"LBM_PHYSICS_MODE": "water", "LBM_FREE_SURFACE_TRACKING": "vof",
+                "LBM_FREE_SURFACE_INITIAL": "gaussian", "LBM_GAUSSIAN_AMPLITUDE_M": "0",
+                "LBM_X_BOUNDARY": "solid", "LBM_DX_M": "1", "LBM_LX_M": "16", "LBM_LY_M": "4", "LBM_LZ_M": "16",
+                "LBM_WATER_DEPTH_M": "4.5", "LBM_PRESSURE_FORMULATION": "vof_component_balanced",
+                "LBM_VOF_COLLAPSE_TRAPPED_GAS": "1", "LBM_VOF_COLLAPSE_INTERVAL": "1",
+                "LBM_VOF_COLLAPSE_MAX_VOLUME_M3": "64", "LBM_VOF_THIN_GAP_BRIDGE": "1",
+                "LBM_VOF_THIN_GAP_BRIDGE_STRENGTH": "4", "LBM_WATER_NU_M2S": "0.05"}
+CASES["vof_features_kbc"] = dict(VOF_FEATURES, LBM_COLLISION="kbc")
+CASES["vof_features_regularized"] = dict(VOF_FEATURES, LBM_COLLISION="regularized", LBM_X_BOUNDARY="periodic",
+                                         LBM_FREE_SURFACE_REFILL="noneq")
+# piecewise-linear bed profile from a bottom file (x_m z_m pairs)
+CASES["air_piecewise_bed"] = dict(BASE_AIR, LBM_LX_M="16", LBM_LY_M="4", LBM_LZ_M="10",
+                                  LBM_BED_PROFILE="piecewise_linear", LBM_BOTTOM_FILE="bottom_piecewise.txt",
+                                  LBM_COLLISION="regularized", LBM_BACKSCATTER="0")
+# linear-wave initial pressure (cosine modes with solid x walls, FFT modes when periodic)
+CASES["water_linear_wave_solid"] = {"LBM_PHYSICS_MODE": "water", "LBM_FREE_SURFACE_INITIAL": "gaussian",
+                                    "LBM_INITIAL_PRESSURE_MODE": "linear_wave", "LBM_DX_M": "1",
+                                    "LBM_LX_M": "16", "LBM_LY_M": "3", "LBM_LZ_M": "10", "LBM_WATER_DEPTH_M": "5",
+                                    "LBM_GAUSSIAN_AMPLITUDE_M": "1.5", "LBM_GAUSSIAN_SIGMA_M": "3",
+                                    "LBM_WATER_NU_M2S": "0.05", "LBM_PRESSURE_FORMULATION": "total_pressure"}
+CASES["water_linear_wave_periodic"] = dict(CASES["water_linear_wave_solid"], LBM_X_BOUNDARY="periodic",
+                                           LBM_PRESSURE_FORMULATION="hydrostatic_balanced")
+
 STEPS = {"air_kbc_default": 3, "air_regularized_sine": 3, "air_bed_cube_solidx": 2, "air_phi_geometry": 2,
-         "water_height_gaussian": 3, "water_height_solitary": 3, "vof_block_kbc": 4, "vof_gaussian_directional": 3}
+         "water_height_gaussian": 3, "water_height_solitary": 3, "vof_block_kbc": 4, "vof_gaussian_directional": 3,
+         "vof_features_kbc": 4, "vof_features_regularized": 4, "air_piecewise_bed": 3,
+         "water_linear_wave_solid": 2, "water_linear_wave_periodic": 2}
+
+# files a case reads, stored beside the goldens (the env holds the bare name)
+CASE_FILES = {"air_piecewise_bed": {"LBM_BOTTOM_FILE": "bottom_piecewise.txt"}}
+
+
+def inject_vof_features(mod):
+    """Edit the VOF state after the reference's init (before its first column
+    height update), in place on the reference's own fields:
+      - a trapped gas pocket one cell thick in z (2 x 1 cells at k = 2):
+        non-exterior gas, so the collapse applies; the liquid cells around it
+        stream through a one-cell gas gap, so the thin-gap bridge acts;
+      - a lone interface cell (fill 0.3) two cells above the surface layer:
+        no wet neighbour, resolved cells within reach -> orphan removal;
+      - a lone interface cell (fill 0.6) far above the pool (no resolved cell
+        within the search radius) -> detached-cell advection;
+      - a lone interface cell of fill 0.005 far above the pool -> advection,
+        then residual compression.
+    The reference's interface-layer kernel then re-establishes its invariant
+    around the edits, and the previous types follow the new ones."""
+    t = mod.free_surface_type.arr
+    fill = mod.free_surface_fill.arr
+    mass = mod.free_surface_mass.arr
+    rho = mod.rho.arr
+    gas, iface = int(mod.FS_GAS), int(mod.FS_INTERFACE)
+
+    def put(k, j, i, ctype, fl):
+        t[k, j, i] = ctype
+        fill[k, j, i] = np.float32(fl)
+        mass[k, j, i] = np.float32(np.float32(fl) * rho[k, j, i])
+
+    nx = t.shape[2]
+    put(2, 1, 5, gas, 0.0)
+    put(2, 1, 6, gas, 0.0)
+    put(6, 2, nx - 5, iface, 0.3)
+    put(12, 1, 3, iface, 0.6)
+    put(12, 2, nx - 6, iface, 0.005)
+    mod.enforce_vof_interface_layer()
+    mod.free_surface_type_prev.arr[...] = t
+
+
+INJECT = {"vof_features_kbc": inject_vof_features, "vof_features_regularized": inject_vof_features}
 
 SCALAR_FIELDS = ["rho", "ux", "uy", "uz", "omegaLoc", "phi", "obstacle", "near_obstacle", "free_surface_fill",
                  "free_surface_type", "free_surface_type_prev", "free_surface_mass", "free_surface_mass_excess",
@@ -140,6 +210,8 @@ def run_case(name: str, env: dict, seed: int = 12345) -> dict:
             if key.startswith("LBM_"):
                 del os.environ[key]
         os.environ.update(env)
+        for key, fname in CASE_FILES.get(name, {}).items():
+            os.environ[key] = os.path.join(HERE, fname)
         os.environ["LBM_TI_CACHE_DIR"] = cache
         sys.modules["taichi"] = taichi_shim
         sys.path.insert(0, REFERENCE)
@@ -168,6 +240,8 @@ def run_case(name: str, env: dict, seed: int = 12345) -> dict:
         orig_height = mod.update_free_surface_height_from_vof
 
         def height_then_snapshot():
+            if not captured["init"] and name in INJECT:
+                INJECT[name](mod)
             orig_height()
             if not captured["init"]:
                 captured["init"] = True
@@ -188,6 +262,7 @@ def run_case(name: str, env: dict, seed: int = 12345) -> dict:
             with np.errstate(all="ignore"):
                 mod.main()
         out["nsteps"] = np.array(STEPS[name])
+        out["injected"] = np.array(1 if name in INJECT else 0)
         return out
     finally:
         os.environ.clear()

@@ -30,10 +30,47 @@ EXACT = {"obstacle", "near_obstacle", "lattice_open", "lattice_wall_type", "free
          "free_surface_type_prev", "free_surface_mass_excess_dir", "vof_exterior_gas"}
 
 
+# options that name a file stored beside the goldens
+FILE_OPTIONS = ("LBM_BOTTOM_FILE",)
+
+
 def load_golden(name: str):
     data = np.load(os.path.join(GOLDEN_DIR, f"{name}.npz"))
     env = json.loads(str(data["env"]))
+    for key in FILE_OPTIONS:
+        if key in env and not os.path.isabs(env[key]):
+            env[key] = os.path.join(GOLDEN_DIR, env[key])
     return data, env
+
+
+def is_injected(data) -> bool:
+    """The case's state was edited after the reference's init; a run starts
+    from its s0 snapshot instead of its own init."""
+    return "injected" in data and bool(int(data["injected"]))
+
+
+def golden_state(data, tag: str = "s0") -> dict:
+    """ABI name -> array of the state buffers in snapshot `tag` (plus "f",
+    the current populations), in the ABI's dtypes."""
+    out = {"f": np.ascontiguousarray(data[f"{tag}_f"], dtype=np.float32)}
+    for gname, (aname, kind) in FIELD_MAP.items():
+        key = f"{tag}_{gname}"
+        if kind != "state" or key not in data:
+            continue
+        v = data[key]
+        if aname in ("fs_type", "fs_type_prev", "fs_excess_dir"):
+            v = v.astype(np.int8)
+        else:
+            v = v.astype(np.float32)
+        out[aname] = np.ascontiguousarray(v)
+    return out
+
+
+def load_state_numpy(arrays: dict, current_f: str, state: dict):
+    """Write a golden state into numpy state arrays (the oracle's)."""
+    for name, v in state.items():
+        dst = arrays[current_f] if name == "f" else arrays[name]
+        dst[...] = v.reshape(dst.shape)
 
 
 def golden_cases():

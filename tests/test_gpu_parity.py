@@ -9,48 +9,86 @@ oracle's operation order, so f32 results agree exactly.
 """
 import pytest
 
-from golden_compare import load_golden
+import numpy as np
+
+from golden_compare import golden_cases, golden_state, is_injected, load_golden, load_state_numpy
 from gpu_compare import compare_states
 from lbm_b200.config import air_wave_env, vof_block_env, water_gaussian_env
 from oracle_runner import OracleSim
 
 pytestmark = pytest.mark.gpu
 
-GOLDEN_ENVS = ["air_kbc_default", "air_regularized_sine", "air_bed_cube_solidx", "air_phi_geometry",
-               "water_height_gaussian", "water_height_solitary", "vof_block_kbc", "vof_gaussian_directional"]
+GOLDEN_ENVS = golden_cases()
+# golden cases built so that a rarely reached reference kernel acts: the
+# counters that must be non-zero in the GPU run as well
+TRIGGERED = {
+    "vof_features_kbc": ("free_surface_vof_orphan_count", "free_surface_vof_detached_advect_count",
+                         "free_surface_vof_detached_compress_count", "free_surface_vof_collapse_cell_count",
+                         "free_surface_thin_gap_bridge_count"),
+    "vof_features_regularized": ("free_surface_vof_orphan_count", "free_surface_vof_detached_advect_count",
+                                 "free_surface_vof_detached_compress_count", "free_surface_vof_collapse_cell_count",
+                                 "free_surface_thin_gap_bridge_count"),
+}
 
 
-def _run_pair(env, chunks=(1, 3, 4)):
+def load_state_torch(dom, state: dict):
+    """Write a golden state into a domain's device buffers."""
+    import torch
+
+    cur = "f1" if dom.counters()["current_f"] else "f0"
+    for name, v in state.items():
+        dst = dom.arrays[cur] if name == "f" else dom.arrays[name]
+        dst.copy_(torch.from_numpy(np.ascontiguousarray(v.reshape(tuple(dst.shape)))).to(dst.dtype))
+    torch.cuda.synchronize(dom.device)
+
+
+def _run_pair(env, chunks=(1, 3, 4), state=None, watch=()):
+    """Run the CUDA library and the oracle from the same inputs (or from
+    `state`, a golden snapshot written into both after init) and compare
+    after each call; `watch` counters are summed over the calls."""
     from lbm_b200.domain import Domain
 
     ref = OracleSim(env)
     dom = Domain(env, device="cuda:0", noise=ref.arrays["init_noise"], rho_initial=ref.arrays["rho_initial"])
+    if state is not None:
+        load_state_numpy(ref.arrays, "f1" if ref.counters()["current_f"] else "f0", state)
+        load_state_torch(dom, state)
     problems = compare_states(dom, ref, "init")
+    seen = {k: 0 for k in watch}
     for n in chunks:
-        ref.step(n)
-        dom.step(n)
-        dom.synchronize()
+        for _ in range(n if watch else 1):
+            k = 1 if watch else n
+            ref.step(k)
+            dom.step(k)
+            dom.synchronize()
+            c = dom.counters()
+            for key in watch:
+                seen[key] += c[key]
         problems += compare_states(dom, ref, f"after+{n}")
     dom.close()
     ref.close()
-    return problems
+    return problems, seen
 
 
 @pytest.mark.parametrize("name", GOLDEN_ENVS)
 def test_gpu_matches_oracle_golden_configs(name):
-    _, env = load_golden(name)
-    problems = _run_pair(env)
+    data, env = load_golden(name)
+    state = golden_state(data, "s0") if is_injected(data) else None
+    watch = TRIGGERED.get(name, ())
+    problems, seen = _run_pair(env, state=state, watch=watch)
     assert not problems, "\n".join(problems[:20])
+    for key in watch:
+        assert seen[key] > 0, f"{key} never acted on the GPU ({seen})"
 
 
 def test_gpu_matches_oracle_air_wave_benchmark_shape():
     # the benchmark's air configuration at a small size
-    problems = _run_pair(air_wave_env(48, 16, 24, amp=3.0, level=6.0, wavelength=24.0), chunks=(1, 5, 10))
+    problems, _ = _run_pair(air_wave_env(48, 16, 24, amp=3.0, level=6.0, wavelength=24.0), chunks=(1, 5, 10))
     assert not problems, "\n".join(problems[:20])
 
 
 def test_gpu_matches_oracle_water_gaussian_benchmark_shape():
-    problems = _run_pair(water_gaussian_env(48, 8, 24, depth=12.0, amp=3.0, sigma=6.0, g_lb=1e-3),
+    problems, _ = _run_pair(water_gaussian_env(48, 8, 24, depth=12.0, amp=3.0, sigma=6.0, g_lb=1e-3),
                          chunks=(1, 4, 7))
     assert not problems, "\n".join(problems[:20])
 
@@ -60,7 +98,7 @@ def test_gpu_matches_oracle_vof_block_benchmark_shape():
     with the trapped-gas collapse every 3 steps (flood fill, FP64 sums)."""
     env = vof_block_env(32, 8, 40, storage="f32", depth=10.0, block=8.0, bottom=20.0)
     env["LBM_VOF_COLLAPSE_INTERVAL"] = "3"
-    problems = _run_pair(env, chunks=(1, 3, 5))
+    problems, _ = _run_pair(env, chunks=(1, 3, 5))
     assert not problems, "\n".join(problems[:20])
 
 
@@ -89,7 +127,7 @@ def test_gpu_tile_path_matches_oracle(variant, monkeypatch):
         monkeypatch.setenv("LBM_B200_TILE_KERNEL", "classic")
         if variant == "classic_no_les":
             env["LBM_USE_LES"] = "0"
-    problems = _run_pair(env, chunks=(1, 2, 6))
+    problems, _ = _run_pair(env, chunks=(1, 2, 6))
     assert not problems, "\n".join(problems[:20])
 
 
@@ -110,7 +148,7 @@ def test_tile_copy_wait_timeout_reports_status_and_recovers(monkeypatch):
     dom.close()
     assert flags & 4, flags
     monkeypatch.delenv("LBM_B200_TEST_TMA_TIMEOUT")
-    problems = _run_pair(env, chunks=(1, 3))
+    problems, _ = _run_pair(env, chunks=(1, 3))
     assert not problems, "\n".join(problems[:20])
 
 

@@ -47,8 +47,8 @@ if PKG_ROOT not in sys.path:
 
 NX, NY, NZ = 512, 256, 256
 CHUNK = 100                 # steps per API call (health-report cadence of the reference loop)
-B_ALG = 152                 # algorithmic bytes per cell update, FP32 populations read + written once
-WORKLOAD = "air over moving wave, LES regularized, 512x256x256, FP32 populations"
+B_ALG = 152                 # algorithmic bytes per cell update, FP32 populations read + written once (76: 16-bit)
+WORKLOAD = "air over moving wave, LES regularized, 512x256x256"
 METRIC, UNIT = "MLUPS", "MLUPS"
 # bounded CPU samples: periodic sub-blocks of the workload with its full height
 # (same bed, same vertical structure), largest first
@@ -64,16 +64,20 @@ PROFILE_TRAFFIC = {
 }
 
 
-def workload_env(nx=None, ny=None, nz=None, seed=12345):
+STORAGE = "f32"             # population storage of the plain run (--plain-storage)
+ARITH = "exact"             # arithmetic of the interior kernels (--arith)
+
+
+def workload_env(nx=None, ny=None, nz=None, seed=12345, storage=None):
     from lbm_b200.config import air_wave_env
 
-    return air_wave_env(nx or NX, ny or NY, nz or NZ, storage="f32", seed=seed)
+    return air_wave_env(nx or NX, ny or NY, nz or NZ, storage=storage or STORAGE, seed=seed)
 
 
 def base_config():
     return {
         "workload": WORKLOAD, "nx": NX, "ny": NY, "nz": NZ, "cells": NX * NY * NZ, "collision": "regularized",
-        "les": "smagorinsky Cs=0.16", "tau0": 0.52, "storage": "f32", "steps_per_call": CHUNK,
+        "les": "smagorinsky Cs=0.16", "tau0": 0.52, "storage": STORAGE, "arithmetic": ARITH, "steps_per_call": CHUNK,
         "l2": (f"inputs larger than L2 ({NX * NY * NZ * B_ALG / 1e9:.2f} GB of populations, A-B)"
                if NX * NY * NZ * B_ALG > 126e6 else "inputs fit in L2 (small profiling case)"),
         "parallelism": "replicas",
@@ -155,7 +159,7 @@ def oracle_sample_rate(budget_s: float, max_steps: int):
     from oracle_runner import OracleSim
 
     shape = CPU_SAMPLES[0]
-    sim = OracleSim(workload_env(*shape))
+    sim = OracleSim(workload_env(*shape, storage="f32"))
     t0 = time.perf_counter()
     sim.step(1)
     t1 = time.perf_counter() - t0
@@ -185,7 +189,7 @@ def reference_arm(args):
     budget = 150.0   # seconds for the whole run
     # pick the largest sample whose K + W steps fit the budget, from one probe step
     probe_shape = CPU_SAMPLES[0]
-    sim = OracleSim(workload_env(*probe_shape))
+    sim = OracleSim(workload_env(*probe_shape, storage="f32"))
     t0 = time.perf_counter()
     sim.step(1)
     t_probe = time.perf_counter() - t0
@@ -197,7 +201,7 @@ def reference_arm(args):
             break
     if shape != probe_shape:
         sim.close()
-        sim = OracleSim(workload_env(*shape))
+        sim = OracleSim(workload_env(*shape, storage="f32"))
     n = shape[0] * shape[1] * shape[2]
     if W:
         sim.step(W)
@@ -256,6 +260,7 @@ def ours(args):
     K, W = args.steps, max(args.warmup, 3)
     env = workload_env(seed=reps.seed(12345))
     dom = Domain(env, device=dev, with_diag=False)
+    dom.set_arithmetic(ARITH)
     lib = dom.lib
     s = dom.stream
     ncell = NX * NY * NZ
@@ -383,7 +388,7 @@ def ours(args):
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W + extra_warm,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
+            "dtype": "f32" if STORAGE == "f32" else f"f32 compute, {STORAGE} storage", "data": "synthetic",
             "config": dict(base_config(), tile_chunk=tuned["chunk"],
                            tile_chunk_ms={str(k): round(v, 4) for k, v in tuned["ms_per_step"].items()},
                            step_graphs=graphs, eager_ms_per_step=round(eager_ms / K, 4),
@@ -552,13 +557,21 @@ def main():
                     help="time eager step calls instead of CUDA step-graph replays")
     ap.add_argument("--tile-chunk", type=int, default=0,
                     help="planes per block of the interior kernel (default: autotuned in warm-up)")
+    ap.add_argument("--plain-storage", choices=("f32", "f16s", "bf16s"), default="f32",
+                    help="population storage of the plain run (default f32, the roofline configuration)")
+    ap.add_argument("--arith", choices=("exact", "fast"), default="exact",
+                    help="arithmetic of the interior kernels: exact (reference order, bit-equal to the oracle) "
+                         "or fast (pair-form collision with multiply-add contraction)")
     ap.add_argument("--size", type=str, default=None,
                     help="NXxNYxNZ: another domain size of the same workload (profiling of small cases)")
     args = ap.parse_args()
+    global STORAGE, ARITH, B_ALG
+    STORAGE, ARITH = args.plain_storage, args.arith
+    B_ALG = 152 if STORAGE == "f32" else 76
     if args.size:
         global NX, NY, NZ, WORKLOAD
         NX, NY, NZ = (int(v) for v in args.size.lower().split("x"))
-        WORKLOAD = f"air over moving wave, LES regularized, {NX}x{NY}x{NZ}, FP32 populations"
+        WORKLOAD = f"air over moving wave, LES regularized, {NX}x{NY}x{NZ}"
     if args.impl == "reference":
         return reference_arm(args)
     if args.mode == "batched":

@@ -305,6 +305,22 @@ int lbm_kernel_timing(lbm_ctx *ctx, double *total_ms, int64_t *launches, int64_t
    choice).  lbm_b200.tuning picks it by timing candidates.  The CPU oracle
    accepts and ignores it. */
 int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes);
+/* Arithmetic of the fused interior kernels (no counterpart in the reference).
+   LBM_ARITH_EXACT evaluates every expression in the reference's operation
+   order without multiply-add contraction, bit-equal to the CPU oracle.
+   LBM_ARITH_FAST evaluates the same collision, LES rate and moments of the
+   interior cells (every cell away from the bed and the top) in a reorganised
+   form with contraction: the regularized and BGK collisions by opposite
+   pairs of directions (shared equilibrium terms and Hermite projections),
+   approximate reciprocal and square root.  Its results differ from the
+   exact ones by rounding; geometry, flags and every near-wall cell are
+   computed exactly in both modes.  New contexts take LBM_B200_ARITH
+   (fast or exact) from the environment, else exact.  Changing the mode drops
+   captured step graphs.  The CPU oracle accepts and ignores it. */
+#define LBM_ARITH_EXACT 0
+#define LBM_ARITH_FAST 1
+int lbm_set_arithmetic(lbm_ctx *ctx, int32_t mode);
+int lbm_get_arithmetic(lbm_ctx *ctx, int32_t *mode);
 /* Step graphs (no counterpart in the reference; the reference launches
    every kernel from its Python step loop): when enabled, each lbm_step call
    of the air path runs as one CUDA graph launch.  The first call of a given

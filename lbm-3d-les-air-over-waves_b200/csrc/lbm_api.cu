@@ -74,6 +74,7 @@ struct lbm_ctx {
     float *bed_cg[2] = {nullptr, nullptr};  // per-column link-endpoint cache (bed-only geometry)
     bool use_cg = false;
     int tile_chunk = 0;   // planes per block of the interior kernel (0: heuristic)
+    int arith = LBM_ARITH_EXACT;   // arithmetic of the fused interior grids (lbm_set_arithmetic)
     // VOF scratch (VOF contexts only)
     int8_t *v_open = nullptr, *v_t0 = nullptr, *v_ba = nullptr;
     float *v_lf0 = nullptr, *v_m0 = nullptr, *v_x0 = nullptr, *v_fa = nullptr;
@@ -469,8 +470,10 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
         }
         if (R.tile) {
             if (ctx->timing) timed_mark(ctx, st);
-            if (!(tma && launch_tile_tma(A, &ctx->tmap[src][0], &ctx->tmap[src][1], st)))
-                launch_step_kernel(KER_TILE_FUSED, A, st);
+            const CUtensorMap *m24 = &ctx->tmap[src][0], *m20 = &ctx->tmap[src][1];
+            const bool done = tma && (ctx->arith == LBM_ARITH_FAST ? launch_tile_tma_fast(A, m24, m20, st)
+                                                                   : launch_tile_tma(A, m24, m20, st));
+            if (!done) launch_step_kernel(KER_TILE_FUSED, A, st);
             CK_LAUNCH("tile fused");
             if (ctx->timing) {
                 timed_mark(ctx, st);
@@ -618,6 +621,11 @@ int lbm_create(const lbm_params *params, lbm_ctx **out) {
     if (ctx->D.n > 0x7fffffffULL) {
         delete ctx;
         return LBM_ERR_BAD_ARG;
+    }
+    {
+        // LBM_B200_ARITH=fast|exact: the default arithmetic of new contexts
+        const char *ar = getenv("LBM_B200_ARITH");
+        ctx->arith = (ar && strcmp(ar, "fast") == 0) ? LBM_ARITH_FAST : LBM_ARITH_EXACT;
     }
     ctx->slot = acquire_slot();
     if (ctx->slot < 0) {
@@ -936,6 +944,19 @@ int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes) {
     if (!ctx || planes < 0 || planes > 4096) return LBM_ERR_BAD_ARG;
     if (planes != ctx->tile_chunk) drop_graphs(ctx);
     ctx->tile_chunk = planes;
+    return LBM_OK;
+}
+
+int lbm_set_arithmetic(lbm_ctx *ctx, int32_t mode) {
+    if (!ctx || (mode != LBM_ARITH_EXACT && mode != LBM_ARITH_FAST)) return LBM_ERR_BAD_ARG;
+    if (mode != ctx->arith) drop_graphs(ctx);
+    ctx->arith = mode;
+    return LBM_OK;
+}
+
+int lbm_get_arithmetic(lbm_ctx *ctx, int32_t *mode) {
+    if (!ctx || !mode) return LBM_ERR_BAD_ARG;
+    *mode = ctx->arith;
     return LBM_OK;
 }
 

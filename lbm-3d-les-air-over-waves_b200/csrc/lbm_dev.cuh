@@ -28,6 +28,10 @@ namespace lbm {
 #define LBM_MAX_SLOTS 1024
 #ifdef LBM_DEVICE_TU
 __device__ lbm_params c_params[LBM_MAX_SLOTS];
+#elif defined(LBM_AUX_TU)
+// translation units without near-wall paths: the out-of-line helpers that
+// name c_params are compiled but never called there
+__device__ lbm_params c_params[1];
 #endif
 
 // f32 constants of the collision kernels (CODEX.py:3165-3171, 3326-3328),

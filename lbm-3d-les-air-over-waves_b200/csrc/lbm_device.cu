@@ -1070,65 +1070,11 @@ static bool pipe16_smem_ready() {
     return ok[dev];
 }
 
-#ifndef LBM_EDGE_CHUNK_DIV
-#define LBM_EDGE_CHUNK_DIV 2
-#endif
-template <int S>
-static bool tma_smem_ready() {
-    static bool done[64] = {false}, ok[64] = {false};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
-    if (!done[dev]) {
-        done[dev] = true;
-        const int edge_bytes = S == LBM_STORE_F32 ? PIPE_SMEM_BYTES : P16_SMEM_BYTES;
-        ok[dev] = cudaFuncSetAttribute(k_tile_tma<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       tma_smem_bytes<S>()) == cudaSuccess &&
-                  cudaFuncSetAttribute(k_tile_edges<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, edge_bytes) ==
-                      cudaSuccess;
-    }
-    return ok[dev];
-}
-
-template <int S>
-static bool launch_tile_tma_s(const StepArgs &A, const CUtensorMap *m24, const CUtensorMap *m20, cudaStream_t st) {
-    const int ni = A.zi1 - A.zi0 + 1;
-    if (ni <= 0 || A.chunk <= 0) return true;
-    const int TX = A.D.nx / LBM_TILE, TY = A.D.ny / LBM_TILE;
-    if (TX < 3 || TY < 3 || !tma_smem_ready<S>()) return false;   // no tile off the edge
-    const unsigned zc = (unsigned)((ni + A.chunk - 1) / A.chunk);
-    const int edge_bytes = S == LBM_STORE_F32 ? PIPE_SMEM_BYTES : P16_SMEM_BYTES;
-    // the edge grid marches shorter z chunks: more, shorter blocks, so that
-    // its last wave ends sooner and the grid behind it starts sooner
-    StepArgs Ae = A;
-    Ae.chunk = A.chunk / LBM_EDGE_CHUNK_DIV > 8 ? A.chunk / LBM_EDGE_CHUNK_DIV : (A.chunk < 8 ? A.chunk : 8);
-    const unsigned zce = (unsigned)((ni + Ae.chunk - 1) / Ae.chunk);
-    k_tile_edges<S><<<dim3(2 * TX + 2 * TY - 4, 1, zce), 256, edge_bytes, st>>>(Ae);
-    LAUNCHED(1);
-    // tiles off the edge: a programmatic dependent launch (it may start while
-    // the grid above drains; plain stream order when the attribute is refused)
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(TX - 2, TY - 2, zc);
-    cfg.blockDim = dim3(256, 1, 1);
-    cfg.dynamicSmemBytes = tma_smem_bytes<S>();
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if (cudaLaunchKernelEx(&cfg, k_tile_tma<S>, A, *m24, *m20) != cudaSuccess) {
-        cudaGetLastError();
-        k_tile_tma<S><<<cfg.gridDim, 256, tma_smem_bytes<S>(), st>>>(A, *m24, *m20);
-    }
-    LAUNCHED(1);
-    return true;
-}
-
 bool launch_tile_tma(const StepArgs &A, const CUtensorMap *m24, const CUtensorMap *m20, cudaStream_t st) {
     switch (A.P.pop_storage) {
-        case LBM_STORE_F32: return launch_tile_tma_s<LBM_STORE_F32>(A, m24, m20, st);
-        case LBM_STORE_F16S: return launch_tile_tma_s<LBM_STORE_F16S>(A, m24, m20, st);
-        case LBM_STORE_BF16S: return launch_tile_tma_s<LBM_STORE_BF16S>(A, m24, m20, st);
+        case LBM_STORE_F32: return launch_tile_tma_t<LBM_STORE_F32, ArExact>(A, m24, m20, st);
+        case LBM_STORE_F16S: return launch_tile_tma_t<LBM_STORE_F16S, ArExact>(A, m24, m20, st);
+        case LBM_STORE_BF16S: return launch_tile_tma_t<LBM_STORE_BF16S, ArExact>(A, m24, m20, st);
         default: return false;
     }
 }

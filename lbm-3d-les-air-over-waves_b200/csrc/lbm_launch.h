@@ -121,6 +121,8 @@ void launch_step_kernel(int which, const StepArgs &A, cudaStream_t st);
 // the source populations' tensor maps with boxes 24x18x1x1 and 20x18x1x1.
 // false: not launched (shared memory of that size unavailable)
 bool launch_tile_tma(const StepArgs &A, const CUtensorMap *m24, const CUtensorMap *m20, cudaStream_t st);
+// the same two grids with the fast arithmetic policy (lbm_fast.cu)
+bool launch_tile_tma_fast(const StepArgs &A, const CUtensorMap *m24, const CUtensorMap *m20, cudaStream_t st);
 void launch_column_flux(const StepArgs &A, float *qx, float *qy, cudaStream_t st);
 void launch_advect(const lbm_params &P, const Dom &D, const float *bed_h, const float *qx, const float *qy,
                    const float *h_in, float *h_out, float *h_last, float t, cudaStream_t st);

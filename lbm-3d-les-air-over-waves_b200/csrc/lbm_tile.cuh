@@ -54,6 +54,27 @@ LBM_DEV float les_interior(const lbm_params &P, float uxp, float uxm, float uyp,
     return 1.0f / tau_eff;
 }
 
+// Arithmetic of the interior kernels' per-cell stages (moments, LES rate,
+// collision).  ArExact: the reference's operation order (the stages shared
+// with the general kernels), bit-equal to the CPU oracle.  A faster policy
+// with the same interface lives in lbm_fast.cuh.
+struct ArExact {
+    static LBM_DEV void macro(const lbm_params &P, const Dom &D, const float f[19], int k, float &r, float &vx,
+                              float &vy, float &vz) {
+        lbm::macro(P, D, f, k, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
+    }
+    static LBM_DEV float les(const lbm_params &P, float uxp, float uxm, float uyp, float uym, float uzp, float uzm,
+                             float vxp, float vxm, float vyp, float vym, float vzp, float vzm, float wxp, float wxm,
+                             float wyp, float wym, float wzp, float wzm) {
+        return les_interior(P, uxp, uxm, uyp, uym, uzp, uzm, vxp, vxm, vyp, vym, vzp, vzm, wxp, wxm, wyp, wym, wzp,
+                            wzm);
+    }
+    static LBM_DEV void collide(const StepArgs &A, int c, int k, float r, float vx, float vy, float vz, float om,
+                                float f[19]) {
+        lbm::collide(A, c, k, false, false, false, 0.0f, r, vx, vy, vz, om, f);
+    }
+};
+
 // populations entering the collide step for an interior cell
 template <int S, int IN>
 LBM_DEV void interior_front(const StepArgs &A, int k, int j, int i, float f[19]) {
@@ -240,7 +261,7 @@ LBM_DEV void cp_async4(float *smem, const float *gmem) {
 LBM_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 LBM_DEV void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-template <int IN, bool LES>
+template <int IN, bool LES, class Ar = ArExact>
 LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by) {
     float *sf = smem;                                   // [slot][q][256] own-cell populations
     float *sr = smem + PIPE_SLOTS * 19 * 256;           // [slot][q][64] ring populations
@@ -337,7 +358,7 @@ LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by) {
         }
         issue(p + 2);           // into the slot consumed before the barrier above
         if (interior) {
-            macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
+            Ar::macro(P, D, fc, p, r, vx, vy, vz);
             if (LES) {
                 su[sl][0][tx + 1][ty + 1] = vx;
                 su[sl][1][tx + 1][ty + 1] = vy;
@@ -347,7 +368,7 @@ LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by) {
                     float fr[19], rr, a, b, d;
 #pragma unroll
                     for (int q = 0; q < 19; ++q) fr[q] = rs[q * 64];
-                    macro(P, D, fr, p, false, LBM_FS_LIQUID, 0.0f, rr, a, b, d);
+                    Ar::macro(P, D, fr, p, rr, a, b, d);
                     su[sl][0][rx + 1][ry + 1] = a;
                     su[sl][1][rx + 1][ry + 1] = b;
                     su[sl][2][rx + 1][ry + 1] = d;
@@ -377,7 +398,7 @@ LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by) {
             if (LES) {
                 const int sm = (p + 1) % 3, s0 = (p + 2) % 3, sp = sl;  // planes k-1, k, k+1
                 const int y = ty + 1, x = tx + 1;
-                om = les_interior(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
+                om = Ar::les(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
                                   su[s0][0][x][y - 1], su[sp][0][x][y], su[sm][0][x][y], su[s0][1][x + 1][y],
                                   su[s0][1][x - 1][y], su[s0][1][x][y + 1], su[s0][1][x][y - 1], su[sp][1][x][y],
                                   su[sm][1][x][y], su[s0][2][x + 1][y], su[s0][2][x - 1][y], su[s0][2][x][y + 1],
@@ -395,7 +416,7 @@ LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by) {
                 A.rho[c] = rp; A.ux[c] = vxp; A.uy[c] = vyp; A.uz[c] = vzp;
             }
             if (!(rp == rp) || fabsf(rp) > 3.0e38f) atomicOr(A.status, 1u);
-            collide(A, c, k, false, false, false, 0.0f, rp, vxp, vyp, vzp, om, fp);
+            Ar::collide(A, c, k, rp, vxp, vyp, vzp, om, fp);
 #pragma unroll
             for (int q = 0; q < 19; ++q) fdst[q * n + c] = fp[q];
         }
@@ -434,7 +455,7 @@ LBM_DEV void cp_async4v(void *smem, const void *gmem) {
 }
 LBM_DEV int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
-template <int S, int IN, bool LES>
+template <int S, int IN, bool LES, class Ar = ArExact>
 LBM_DEV void tile_pipe16_body(const StepArgs &A, float *smem, int bx, int by) {
     typedef typename Store<S>::T T;
     uint32_t *sw = (uint32_t *)smem;                     // [slot][P16_MAIN] words
@@ -550,14 +571,14 @@ LBM_DEV void tile_pipe16_body(const StepArgs &A, float *smem, int bx, int by) {
         }
         issue(p + 2);           // into the slot consumed before the barrier above
         if (interior) {
-            macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
+            Ar::macro(P, D, fc, p, r, vx, vy, vz);
             if (LES) {
                 su[sl][0][tx + 1][ty + 1] = vx;
                 su[sl][1][tx + 1][ty + 1] = vy;
                 su[sl][2][tx + 1][ty + 1] = vz;
                 if (ring) {
                     float rr2, a, b, d;
-                    macro(P, D, frr, p, false, LBM_FS_LIQUID, 0.0f, rr2, a, b, d);
+                    Ar::macro(P, D, frr, p, rr2, a, b, d);
                     su[sl][0][rx + 1][ry + 1] = a;
                     su[sl][1][rx + 1][ry + 1] = b;
                     su[sl][2][rx + 1][ry + 1] = d;
@@ -584,7 +605,7 @@ LBM_DEV void tile_pipe16_body(const StepArgs &A, float *smem, int bx, int by) {
             if (LES) {
                 const int sm = (p + 1) % 3, s0 = (p + 2) % 3, sp = sl;  // planes k-1, k, k+1
                 const int y = ty + 1, x = tx + 1;
-                om = les_interior(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
+                om = Ar::les(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
                                   su[s0][0][x][y - 1], su[sp][0][x][y], su[sm][0][x][y], su[s0][1][x + 1][y],
                                   su[s0][1][x - 1][y], su[s0][1][x][y + 1], su[s0][1][x][y - 1], su[sp][1][x][y],
                                   su[sm][1][x][y], su[s0][2][x + 1][y], su[s0][2][x - 1][y], su[s0][2][x][y + 1],
@@ -600,7 +621,7 @@ LBM_DEV void tile_pipe16_body(const StepArgs &A, float *smem, int bx, int by) {
                 A.rho[c] = rp; A.ux[c] = vxp; A.uy[c] = vyp; A.uz[c] = vzp;
             }
             if (!(rp == rp) || fabsf(rp) > 3.0e38f) atomicOr(A.status, 1u);
-            collide(A, c, k, false, false, false, 0.0f, rp, vxp, vyp, vzp, om, fp);
+            Ar::collide(A, c, k, rp, vxp, vyp, vzp, om, fp);
 #pragma unroll
             for (int q = 0; q < 19; ++q) Store<S>::st(fdst, (size_t)q * n + (size_t)c, fp[q], q, P.rho0);
         }
@@ -721,7 +742,7 @@ LBM_DEV void tma_load_4d(unsigned dst, const CUtensorMap *map, int x, int y, int
         : "memory");
 }
 
-template <int S>
+template <int S, class Ar = ArExact>
 __global__ void __launch_bounds__(256, 2)
     k_tile_tma(StepArgs A, const __grid_constant__ CUtensorMap m24, const __grid_constant__ CUtensorMap m20) {
     typedef TmaTile<S> L;
@@ -827,7 +848,7 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
                 for (int q = 0; q < 19; ++q)
                     fr[q] = Store<S>::ld_rw(L::wide(q) ? bA : bB, (size_t)(L::base(q) + L::shift(q)), q, P.rho0);
-                macro(P, D, fr, p, false, LBM_FS_LIQUID, 0.0f, rr, a, b, d);
+                Ar::macro(P, D, fr, p, rr, a, b, d);
                 su[sl][0][rx + 1][ry + 1] = a;
                 su[sl][1][rx + 1][ry + 1] = b;
                 su[sl][2][rx + 1][ry + 1] = d;
@@ -838,7 +859,7 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
             for (int q = 0; q < 19; ++q)
                 fc[q] = Store<S>::ld_rw(L::wide(q) ? bA : bB, (size_t)(L::base(q) + L::shift(q)), q, P.rho0);
-            macro(P, D, fc, p, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
+            Ar::macro(P, D, fc, p, r, vx, vy, vz);
             su[sl][0][tx + 1][ty + 1] = vx;
             su[sl][1][tx + 1][ty + 1] = vy;
             su[sl][2][tx + 1][ty + 1] = vz;
@@ -861,7 +882,7 @@ __global__ void __launch_bounds__(256, 2)
             const int c = k * nxy + col;
             const int sm = (p + 1) % 3, s0 = (p + 2) % 3, sp = sl;  // planes k-1, k, k+1
             const int y = ty + 1, x = tx + 1;
-            const float om = les_interior(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
+            const float om = Ar::les(P, su[s0][0][x + 1][y], su[s0][0][x - 1][y], su[s0][0][x][y + 1],
                                           su[s0][0][x][y - 1], su[sp][0][x][y], su[sm][0][x][y], su[s0][1][x + 1][y],
                                           su[s0][1][x - 1][y], su[s0][1][x][y + 1], su[s0][1][x][y - 1],
                                           su[sp][1][x][y], su[sm][1][x][y], su[s0][2][x + 1][y], su[s0][2][x - 1][y],
@@ -885,7 +906,7 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
             for (int q = 0; q < 19; ++q)
                 fp[q] = Store<S>::ld_rw(L::wide(q) ? bA : bB, (size_t)(L::base(q) + L::shift(q)), q, P.rho0);
-            collide(A, c, k, false, false, false, 0.0f, rp, vxp, vyp, vzp, om, fp);
+            Ar::collide(A, c, k, rp, vxp, vyp, vzp, om, fp);
 #pragma unroll
             for (int q = 0; q < 19; ++q) Store<S>::st(fdst, (size_t)(q * n + c), fp[q], q, P.rho0);
         }
@@ -913,14 +934,73 @@ LBM_DEV void edge_tile(int e, int TX, int TY, int &bx, int &by) {
 // count), cp.async-staged (k_tile_pipe's or k_tile_pipe16's body).  k_tile_tma is launched after it as a
 // programmatic dependent: it may start as soon as every block of this grid
 // is running (the two grids share no output)
-template <int S>
+template <int S, class Ar = ArExact>
 __global__ void __launch_bounds__(256, 2) k_tile_edges(StepArgs A) {
     extern __shared__ __align__(16) float smem[];
     asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     int bx = 0, by = 0;
     edge_tile(blockIdx.x, A.D.nx / LBM_TILE, A.D.ny / LBM_TILE, bx, by);
-    if constexpr (S == LBM_STORE_F32) tile_pipe_body<1, true>(A, smem, bx, by);
-    else tile_pipe16_body<S, 1, true>(A, smem, bx, by);
+    if constexpr (S == LBM_STORE_F32) tile_pipe_body<1, true, Ar>(A, smem, bx, by);
+    else tile_pipe16_body<S, 1, true, Ar>(A, smem, bx, by);
+}
+
+// ----------------------------------------------- launch of the fused interior
+#ifndef LBM_EDGE_CHUNK_DIV
+#define LBM_EDGE_CHUNK_DIV 2
+#endif
+// the two interior grids take more than 48 KB of shared memory: raise the
+// per-kernel limits once per device and arithmetic policy
+template <int S, class Ar>
+static bool tma_smem_ready_t() {
+    static bool done[64] = {false}, ok[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    if (!done[dev]) {
+        done[dev] = true;
+        const int edge_bytes = S == LBM_STORE_F32 ? PIPE_SMEM_BYTES : P16_SMEM_BYTES;
+        ok[dev] = cudaFuncSetAttribute(k_tile_tma<S, Ar>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       tma_smem_bytes<S>()) == cudaSuccess &&
+                  cudaFuncSetAttribute(k_tile_edges<S, Ar>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       edge_bytes) == cudaSuccess;
+    }
+    return ok[dev];
+}
+
+// The fused interior step with LES: the edge tiles (cp.async staging), then
+// the tiles off the edge (tile copies) as a programmatic dependent launch.
+// false: not launched (no tile off the edge, or shared memory refused).
+template <int S, class Ar>
+static bool launch_tile_tma_t(const StepArgs &A, const CUtensorMap *m24, const CUtensorMap *m20, cudaStream_t st) {
+    const int ni = A.zi1 - A.zi0 + 1;
+    if (ni <= 0 || A.chunk <= 0) return true;
+    const int TX = A.D.nx / LBM_TILE, TY = A.D.ny / LBM_TILE;
+    if (TX < 3 || TY < 3 || !tma_smem_ready_t<S, Ar>()) return false;
+    const unsigned zc = (unsigned)((ni + A.chunk - 1) / A.chunk);
+    const int edge_bytes = S == LBM_STORE_F32 ? PIPE_SMEM_BYTES : P16_SMEM_BYTES;
+    // the edge grid marches shorter z chunks: more, shorter blocks, so that
+    // its last wave ends sooner and the grid behind it starts sooner
+    StepArgs Ae = A;
+    Ae.chunk = A.chunk / LBM_EDGE_CHUNK_DIV > 8 ? A.chunk / LBM_EDGE_CHUNK_DIV : (A.chunk < 8 ? A.chunk : 8);
+    const unsigned zce = (unsigned)((ni + Ae.chunk - 1) / Ae.chunk);
+    k_tile_edges<S, Ar><<<dim3(2 * TX + 2 * TY - 4, 1, zce), 256, edge_bytes, st>>>(Ae);
+    // tiles off the edge: a programmatic dependent launch (it may start while
+    // the grid above drains; plain stream order when the attribute is refused)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(TX - 2, TY - 2, zc);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = tma_smem_bytes<S>();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k_tile_tma<S, Ar>, A, *m24, *m20) != cudaSuccess) {
+        cudaGetLastError();
+        k_tile_tma<S, Ar><<<cfg.gridDim, 256, tma_smem_bytes<S>(), st>>>(A, *m24, *m20);
+    }
+    launch_count_add(2);
+    return true;
 }
 
 // stream only (the last pass of a call) for interior cells

@@ -21,6 +21,8 @@ LBM_ERR_NOT_CONVERGED = -3
 LBM_ERR_NONFINITE = -4
 LBM_ERR_UNSUPPORTED = -5
 LBM_ERR_NOT_BOUND = -6
+LBM_ARITH_EXACT = 0
+LBM_ARITH_FAST = 1
 ERRORS = {
     -1: "bad argument", -2: "CUDA error", -3: "not converged", -4: "non-finite value",
     -5: "unsupported configuration", -6: "buffers not bound",
@@ -273,6 +275,10 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.lbm_set_tile_chunk.argtypes = [vp, C.c_int32]
     lib.lbm_set_step_graphs.restype = C.c_int
     lib.lbm_set_step_graphs.argtypes = [vp, C.c_int32]
+    lib.lbm_set_arithmetic.restype = C.c_int
+    lib.lbm_set_arithmetic.argtypes = [vp, C.c_int32]
+    lib.lbm_get_arithmetic.restype = C.c_int
+    lib.lbm_get_arithmetic.argtypes = [vp, C.POINTER(C.c_int32)]
     lib.lbm_link_geometry_noalloc.restype = C.c_int
     lib.lbm_link_geometry_noalloc.argtypes = [C.POINTER(LbmParams), vp, vp, vp, vp, vp, vp, vp, vp, C.c_char_p,
                                               C.c_size_t]
@@ -283,7 +289,7 @@ ABI_SYMBOLS = (
     "lbm_backend_name", "lbm_abi_version", "lbm_struct_size", "lbm_create", "lbm_bind", "lbm_init_geometry",
     "lbm_init_fields", "lbm_step", "lbm_export_diagnostics", "lbm_read_counters", "lbm_destroy", "lbm_last_error",
     "lbm_set_kernel_timing", "lbm_kernel_timing", "lbm_launch_count", "lbm_link_geometry_noalloc",
-    "lbm_set_tile_chunk", "lbm_set_step_graphs",
+    "lbm_set_tile_chunk", "lbm_set_step_graphs", "lbm_set_arithmetic", "lbm_get_arithmetic",
 )
 
 

@@ -2,9 +2,11 @@
 
     python -m lbm_b200.build        (from lbm-3d-les-air-over-waves_b200/)
 
-Flags: sm_100a only; -fmad=false so that every f32 expression rounds in
-source order (the CPU oracle is built with -ffp-contract=off): the GPU path
-is bit-comparable with the oracle.
+Flags: sm_100a only; -fmad=false for lbm_api.cu and lbm_device.cu, so that
+every f32 expression rounds in source order (the CPU oracle is built with
+-ffp-contract=off) and those kernels are bit-comparable with the oracle;
+lbm_fast.cu (the fast-arithmetic interior kernels) is compiled with
+multiply-add contraction.
 """
 from __future__ import annotations
 
@@ -20,14 +22,18 @@ REPO = os.path.dirname(SRC_ROOT)
 INCLUDE = os.path.join(REPO, "include")
 OUT_DIR = os.path.join(PKG, "_native")
 LIB = os.path.join(OUT_DIR, "liblbm_b200.so")
-SOURCES = ["lbm_api.cu", "lbm_device.cu"]
-HEADERS = ["lbm_dev.cuh", "lbm_geom.cuh", "lbm_stages.cuh", "lbm_tile.cuh", "lbm_vof.cuh", "lbm_launch.h"]
+SOURCES = ["lbm_api.cu", "lbm_device.cu", "lbm_fast.cu"]
+HEADERS = ["lbm_dev.cuh", "lbm_geom.cuh", "lbm_stages.cuh", "lbm_tile.cuh", "lbm_vof.cuh", "lbm_launch.h",
+           "lbm_fast.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--expt-relaxed-constexpr",
+    "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
     "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills",
 ]
+# rounding per translation unit: the reference's order everywhere except the
+# fast-arithmetic interior kernels, which contract multiply-adds
+SOURCE_FLAGS = {"lbm_api.cu": ["-fmad=false"], "lbm_device.cu": ["-fmad=false"], "lbm_fast.cu": ["-fmad=true"]}
 
 
 def nvcc() -> str:
@@ -56,7 +62,7 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     procs = []
     for src in SOURCES:
         obj = os.path.join(build_dir, src.replace(".cu", ".o"))
-        cmd = [nvcc(), *NVCC_FLAGS, *extra, "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [nvcc(), *NVCC_FLAGS, *SOURCE_FLAGS[src], *extra, "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
         procs.append((src, cmd, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
         objs.append(obj)
     failed = []

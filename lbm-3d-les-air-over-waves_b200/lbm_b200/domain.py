@@ -109,6 +109,18 @@ class Domain:
         first use per call shape, bit-identical to eager calls)."""
         self._check(self.lib.lbm_set_step_graphs(self.ctx, 1 if enable else 0), "lbm_set_step_graphs")
 
+    def set_arithmetic(self, mode: str):
+        """Arithmetic of the fused interior kernels: "exact" (the reference's
+        operation order, bit-equal to the CPU oracle) or "fast" (pair-form
+        collision with multiply-add contraction; differs by rounding)."""
+        code = {"exact": abi.LBM_ARITH_EXACT, "fast": abi.LBM_ARITH_FAST}[mode]
+        self._check(self.lib.lbm_set_arithmetic(self.ctx, code), "lbm_set_arithmetic")
+
+    def arithmetic(self) -> str:
+        v = C.c_int32()
+        self._check(self.lib.lbm_get_arithmetic(self.ctx, C.byref(v)), "lbm_get_arithmetic")
+        return "fast" if v.value == abi.LBM_ARITH_FAST else "exact"
+
     def synchronize(self):
         self.stream.synchronize()
 

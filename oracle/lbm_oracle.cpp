@@ -756,6 +756,14 @@ int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes) {
     return (ctx && planes >= 0) ? LBM_OK : LBM_ERR_BAD_ARG;
 }
 int lbm_set_step_graphs(lbm_ctx *ctx, int32_t) { return ctx ? LBM_OK : LBM_ERR_BAD_ARG; }
+int lbm_set_arithmetic(lbm_ctx *ctx, int32_t mode) {
+    return (ctx && (mode == LBM_ARITH_EXACT || mode == LBM_ARITH_FAST)) ? LBM_OK : LBM_ERR_BAD_ARG;
+}
+int lbm_get_arithmetic(lbm_ctx *ctx, int32_t *mode) {
+    if (!ctx || !mode) return LBM_ERR_BAD_ARG;
+    *mode = LBM_ARITH_EXACT;   // the oracle computes in the reference's order only
+    return LBM_OK;
+}
 int lbm_launch_count(int64_t *count) {
     if (!count) return LBM_ERR_BAD_ARG;
     *count = 0;

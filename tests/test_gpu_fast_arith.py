@@ -1,0 +1,98 @@
+"""The fast arithmetic of the interior kernels against the reference's.
+
+LBM_ARITH_FAST evaluates the interior cells' moments, LES rate and
+collision in pair form with multiply-add contraction (lbm_fast.cuh); every
+near-wall cell, the geometry and the flags stay exact.  Its results differ
+from the reference arithmetic by rounding only, and the bound on that
+difference is the north star's for the FP32 form: 1e-5 relative error
+against the reference after the configuration's full run.
+
+Error measures after N steps, over open cells:
+  density      max |rho - rho_ref| / rho_ref
+  velocity     max |u - u_ref| / max |u_ref|
+  populations  max over q of max |f_q - f_ref,q| / max |f_ref,q|
+Flags and link geometry must stay bit-equal.
+"""
+import json
+
+import numpy as np
+import pytest
+
+from gpu_compare import populations
+from lbm_b200.config import air_wave_env
+from oracle_runner import OracleSim
+
+pytestmark = pytest.mark.gpu
+
+BOUND = 1e-5
+
+
+def _errors(dom, ref):
+    open_ = ref.arrays["obstacle"] == 0
+    out = {}
+    r = dom.field("rho").cpu().numpy().astype(np.float64)
+    r0 = ref.arrays["rho"].astype(np.float64)
+    out["density"] = float((np.abs(r - r0) / np.abs(r0))[open_].max())
+    u = np.stack([dom.field(k).cpu().numpy() for k in ("ux", "uy", "uz")]).astype(np.float64)
+    u0 = np.stack([ref.arrays[k] for k in ("ux", "uy", "uz")]).astype(np.float64)
+    out["velocity"] = float(np.abs(u - u0).max(0)[open_].max() / np.sqrt((u0 ** 2).sum(0))[open_].max())
+    f = populations(dom).astype(np.float64)
+    f0 = ref.f().astype(np.float64)
+    out["populations"] = float(max(np.abs(f[q] - f0[q])[open_].max() / np.abs(f0[q])[open_].max() for q in range(19)))
+    return out
+
+
+@pytest.mark.parametrize("collision", ["regularized", "kbc"])
+def test_fast_arithmetic_interior_matches_reference_small(collision):
+    """Tile path of a small domain (inner tiles on tile copies), 60 steps."""
+    from lbm_b200.domain import Domain
+
+    env = air_wave_env(64, 64, 40, amp=3.0, level=6.0, wavelength=32.0)
+    env["LBM_COLLISION"] = collision
+    ref = OracleSim(env)
+    dom = Domain(env, device="cuda:0", noise=ref.arrays["init_noise"], rho_initial=ref.arrays["rho_initial"])
+    dom.set_arithmetic("fast")
+    assert dom.arithmetic() == "fast"
+    for n in (1, 9, 50):
+        dom.step(n)
+        ref.step(n)
+    dom.synchronize()
+    dom.export_diagnostics()
+    ref.export()
+    dom.synchronize()
+    for name in ("obstacle", "near_obstacle", "lattice_open", "lattice_wall_type"):
+        assert np.array_equal(dom.field(name).cpu().numpy(), ref.arrays[name]), name
+    errs = _errors(dom, ref)
+    print(json.dumps({"case": f"air 64x64x40 {collision}, 60 steps, fast arithmetic", "errors": errs}))
+    assert dom.counters()["status_flags"] == 0
+    for key, v in errs.items():
+        assert v <= BOUND, (key, errs)
+    dom.close()
+    ref.close()
+
+
+def test_fast_arithmetic_c1_air_1000_steps():
+    """The plain air configuration at its stated size and length (128x64x64,
+    1000 steps): the fast interior arithmetic stays within 1e-5 of the
+    reference arithmetic."""
+    from lbm_b200.domain import Domain
+
+    env = air_wave_env(128, 64, 64, amp=4.0, level=8.0, wavelength=64.0, speed=0.02, inflow=0.05)
+    ref = OracleSim(env)
+    dom = Domain(env, device="cuda:0", noise=ref.arrays["init_noise"], rho_initial=ref.arrays["rho_initial"])
+    dom.set_arithmetic("fast")
+    history = {}
+    done = 0
+    for n in (10, 90, 900):
+        dom.step(n)
+        ref.step(n)
+        done += n
+        dom.synchronize()
+        ref.export()
+        history[done] = _errors(dom, ref)
+    print(json.dumps({"case": "air 128x64x64 regularized, fast arithmetic", "errors_by_step": history}))
+    assert dom.counters()["status_flags"] == 0
+    for key, v in history[1000].items():
+        assert v <= BOUND, (key, history)
+    dom.close()
+    ref.close()

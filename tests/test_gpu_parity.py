@@ -102,6 +102,36 @@ def test_gpu_matches_oracle_vof_block_benchmark_shape():
     assert not problems, "\n".join(problems[:20])
 
 
+def test_gpu_matches_oracle_c1_air_1000_steps():
+    """The plain air configuration at its stated size and length: 128x64x64,
+    regularized + Smagorinsky, moving sinusoidal bed z = 8 + 4 sin(2 pi (x -
+    0.02 t)/64), uniform u = (0.05, 0, 0) plus seeded noise of 1e-3, 1000
+    steps.  Populations, moments, flags and counters bit-equal to the oracle
+    after steps 1, 10, 100 and 1000."""
+    env = air_wave_env(128, 64, 64, amp=4.0, level=8.0, wavelength=64.0, speed=0.02, inflow=0.05)
+    problems, _ = _run_pair(env, chunks=(1, 9, 90, 900))
+    assert not problems, "\n".join(problems[:20])
+
+
+def test_gpu_matches_oracle_vof_falling_block_400_steps():
+    """A falling-block VOF case shaped like the benchmark's (KBC, component-
+    balanced pressure, solid x walls, thin-gap bridge 4), reduced so that the
+    block reaches the pool within the run: 48x16x64, pool depth 16, block of
+    8 cells from 24, g = 1e-3, trapped-gas collapse every 20 steps, 400 steps.
+    The collapse applies, orphans are removed, detached cells are advected and
+    the bridge acts (counters summed over the run); flags, fills, masses,
+    flood-fill labels and populations are bit-equal to the oracle after steps
+    1, 10, 100, 200 and 400."""
+    env = vof_block_env(48, 16, 64, storage="f32", depth=16.0, block=8.0, bottom=24.0, g_lb=1e-3)
+    env["LBM_VOF_COLLAPSE_INTERVAL"] = "20"
+    watch = ("free_surface_vof_collapse_cell_count", "free_surface_vof_orphan_count",
+             "free_surface_vof_detached_advect_count", "free_surface_thin_gap_bridge_count")
+    problems, seen = _run_pair(env, chunks=(1, 9, 90, 100, 200), watch=watch)
+    assert not problems, "\n".join(problems[:20])
+    for key in watch:
+        assert seen[key] > 0, f"{key} never acted ({seen})"
+
+
 @pytest.mark.parametrize("variant", ["les", "no_les", "kbc", "small_chunks", "classic", "classic_no_les", "tile_copies",
                                      "tile_copies_kbc", "cp_async"])
 def test_gpu_tile_path_matches_oracle(variant, monkeypatch):

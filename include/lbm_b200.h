@@ -253,13 +253,56 @@ typedef struct lbm_counters {
     int32_t flood_sweeps_used;           /* last collapse pass: sweeps until the marks stopped changing */
 } lbm_counters;
 
+/* Inputs of lbm_diagnostics that are not solver constants. */
+typedef struct lbm_diag_inputs {
+    double rho_phys;        /* fluid density [kg/m^3]: pressures are reported in Pa */
+    double gravity_phys;    /* [m/s^2] */
+    int32_t slice_j;        /* y index of the xz slice (the reference uses Ny / 2) */
+    int32_t pad;
+} lbm_diag_inputs;
+
+/* The per-plot metric row of run_ab_case.py (make_visualize,
+   run_ab_case.py:283-679) and the health line of main() (CODEX.py:3930-3937),
+   reduced on the device.  NaN (or -1 for counts) where the reference writes
+   NaN / -1 for the mode.  Sums are FP64; the reference's float32 numpy sums
+   agree to rounding. */
+typedef struct lbm_diag {
+    /* maximum speed over active cells (not solid, and not gas with a free surface) */
+    double max_speed_lb;               /* lattice units (the health line's Max |U|) */
+    double max_speed_phys;             /* m/s */
+    double max_speed_x, max_speed_y, max_speed_z;   /* cell centre of the first maximum in C order */
+    int32_t max_k, max_j, max_i;
+    int32_t max_speed_fs_type;         /* free-surface state there (-1 without a free surface) */
+    double max_speed_fs_fill;
+    int32_t max_speed_wet_neighbors, max_speed_full_neighbors, max_speed_gas_neighbors;
+    int32_t pad0;
+    int64_t active_cells;
+    /* volumes and VOF accounting (run_ab_case.py:299-347) */
+    double water_volume;               /* m^3: fill summed over open cells times dx^3 */
+    double vof_mass_total;
+    double vof_min_interface_fill;
+    int64_t vof_tiny_interface_count;
+    double vof_pending_excess_mass;
+    int64_t vof_pending_excess_count;
+    /* free-surface line: mean over y of the surface elevation (run_ab_case.py:348-363) */
+    double surface_min, surface_max;
+    double surface_symmetry_l2, surface_eta_hp_rms, surface_left_max, surface_right_max;
+    /* xz slice at slice_j: pressure [Pa] and vorticity statistics over the near-wall band
+       0 < phi <= 10 dx and over the free-surface band (run_ab_case.py:431-596); the
+       linear-wave residual columns are not computed here */
+    double p_rms, p_hp_rms, p_total_rms, p_total_hp_rms, vort_rms, vort_hp_rms;
+    double fs_p_rms, fs_p_hp_rms, fs_p_total_rms, fs_p_total_hp_rms, fs_vort_rms, fs_vort_hp_rms;
+    int64_t band_cells, fs_band_cells;
+} lbm_diag;
+
 typedef struct lbm_ctx lbm_ctx;
 
 /* Library identity: "cuda-sm100a" or "cpu-oracle". */
 const char *lbm_backend_name(void);
 int lbm_abi_version(void);
-/* sizeof(lbm_params), sizeof(lbm_buffers), sizeof(lbm_counters) for
-   which = 0, 1, 2: lets a binding check its struct layout. */
+/* sizeof(lbm_params), sizeof(lbm_buffers), sizeof(lbm_counters),
+   sizeof(lbm_diag), sizeof(lbm_diag_inputs) for which = 0 .. 4: lets a
+   binding check its struct layout. */
 int64_t lbm_struct_size(int32_t which);
 
 /* Create a context from constants; replaces module import + field
@@ -291,6 +334,16 @@ int lbm_export_diagnostics(lbm_ctx *ctx, void *stream);
 
 /* Copy scalar counters to the host (synchronises the stream). */
 int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out);
+
+/* Device-side metrics of the current state, in place of the host reductions
+   of run_ab_case.py:283-679 (its per-plot metric row) and of the health line
+   (CODEX.py:3930-3937), which both pull whole fields to the host.  The
+   reductions run on stream and only the lbm_diag record comes back; the call
+   synchronises stream.  Obstacle and phi are recomputed from the current
+   step's geometry, so no diagnostic buffer needs to be bound.  The first call
+   allocates a small scratch (a few slice-sized arrays).  The CPU oracle
+   returns LBM_ERR_UNSUPPORTED. */
+int lbm_diagnostics(lbm_ctx *ctx, const lbm_diag_inputs *in, lbm_diag *out, void *stream);
 
 /* Measurement hook (no counterpart in the reference): when enabled, the
    library brackets every launch of its dominant step kernel (the interior

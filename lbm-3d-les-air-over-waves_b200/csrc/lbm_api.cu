@@ -104,6 +104,14 @@ struct lbm_ctx {
     float *stash = nullptr;     // FP32 post-condition populations of the general planes (16-bit storage)
     size_t stash_cells = 0;
     std::vector<StepGraph> graph_cache;
+    // scratch of lbm_diagnostics (allocated by its first call)
+    DiagCellPart *d_cellp = nullptr;
+    DiagSlicePart *d_slp = nullptr;
+    double *d_col_eta = nullptr;
+    float *d_col_mm = nullptr;
+    double *d_slice = nullptr;
+    uint8_t *d_mask = nullptr;
+    lbm_diag *d_out = nullptr;
     // tensor maps of f[0] and f[1] for the tile-copy interior kernel: boxes 24x18 and 20x18
     CUtensorMap tmap[2][2];
     void *tmap_src[2] = {nullptr, nullptr};   // buffers the maps were encoded for
@@ -601,6 +609,8 @@ int64_t lbm_struct_size(int32_t which) {
         case 0: return (int64_t)sizeof(lbm_params);
         case 1: return (int64_t)sizeof(lbm_buffers);
         case 2: return (int64_t)sizeof(lbm_counters);
+        case 3: return (int64_t)sizeof(lbm_diag);
+        case 4: return (int64_t)sizeof(lbm_diag_inputs);
         default: return -1;
     }
 }
@@ -915,6 +925,62 @@ int lbm_read_counters(lbm_ctx *ctx, lbm_counters *out) {
     out->status_flags = (int32_t)status;
     out->step = ctx->nstep;
     out->current_f = ctx->cur;
+    return LBM_OK;
+}
+
+int lbm_diagnostics(lbm_ctx *ctx, const lbm_diag_inputs *in, lbm_diag *out, void *stream) {
+    if (!ctx || !in || !out) return LBM_ERR_BAD_ARG;
+    if (!ctx->bound) return LBM_ERR_NOT_BOUND;
+    if (in->slice_j < 0 || in->slice_j >= ctx->P.ny) return fail(ctx, LBM_ERR_BAD_ARG, "lbm_diagnostics: slice_j out of range");
+    cudaStream_t st = (cudaStream_t)stream;
+    ctx->last_stream = st;
+    const int ncellp = 4 * 148, nslp = 148;
+    const size_t nx = (size_t)ctx->P.nx, nzx = (size_t)ctx->P.nz * nx;
+    int s;
+    if (!ctx->d_out) {
+        if ((s = alloc(ctx, (void **)&ctx->d_cellp, ncellp * sizeof(DiagCellPart))) ||
+            (s = alloc(ctx, (void **)&ctx->d_slp, 2 * nslp * sizeof(DiagSlicePart) + 12 * sizeof(double))) ||
+            (s = alloc(ctx, (void **)&ctx->d_col_eta, nx * sizeof(double))) ||
+            (s = alloc(ctx, (void **)&ctx->d_col_mm, 2 * nx * sizeof(float))) ||
+            (s = alloc(ctx, (void **)&ctx->d_slice, 3 * nzx * sizeof(double))) ||
+            (s = alloc(ctx, (void **)&ctx->d_mask, nzx)) || (s = alloc(ctx, (void **)&ctx->d_out, sizeof(lbm_diag))))
+            return s;
+    }
+    if ((s = load_bed_slot(ctx, (int)(ctx->nstep & 1), st)) != LBM_OK) return s;
+    DiagArgs G;
+    memset(&G, 0, sizeof G);
+    const lbm_buffers &b = ctx->b;
+    G.P = ctx->P;
+    G.slot = ctx->slot;
+    G.D = ctx->D;
+    G.bed = slot_view(ctx, (int)(ctx->nstep & 1));
+    G.bed.cg = nullptr;
+    G.rho = b.rho; G.ux = b.ux; G.uy = b.uy; G.uz = b.uz;
+    G.fill = b.fs_fill; G.mass = b.fs_mass; G.excess = b.fs_mass_excess; G.fs_h = b.fs_h;
+    G.type = b.fs_type; G.type_prev = b.fs_type_prev;
+    G.types_are_prev = ctx->nstep > 0 ? 1 : 0;
+    G.fs = ctx->P.fs_mode != LBM_FS_NONE ? 1 : 0;
+    G.vof = is_vof(ctx->P) ? 1 : 0;
+    G.slice_j = in->slice_j;
+    G.rho_phys = in->rho_phys;
+    G.gravity_phys = in->gravity_phys;
+    G.cellp = ctx->d_cellp;
+    G.ncellp = ncellp;
+    G.col_eta = ctx->d_col_eta;
+    G.col_min = ctx->d_col_mm;
+    G.col_max = ctx->d_col_mm + nx;
+    G.sl_p = ctx->d_slice;
+    G.sl_pt = ctx->d_slice + nzx;
+    G.sl_v = ctx->d_slice + 2 * nzx;
+    G.sl_mask = ctx->d_mask;
+    G.slp = ctx->d_slp;
+    G.nslp = nslp;
+    G.slice_mean = (double *)(ctx->d_slp + 2 * nslp);
+    G.out = ctx->d_out;
+    launch_diagnostics(G, st);
+    CK_LAUNCH("diagnostics");
+    CK(cudaMemcpyAsync(out, ctx->d_out, sizeof(lbm_diag), cudaMemcpyDeviceToHost, st), "diagnostics copy");
+    CK(cudaStreamSynchronize(st), "synchronize");
     return LBM_OK;
 }
 

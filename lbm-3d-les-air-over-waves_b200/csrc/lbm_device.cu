@@ -29,6 +29,7 @@
 #include "lbm_stages.cuh"
 #include "lbm_tile.cuh"
 #include "lbm_vof.cuh"
+#include "lbm_diag.cuh"
 
 namespace lbm {
 
@@ -1376,6 +1377,18 @@ void launch_vof_coalesce(const VofArgs &V, cudaStream_t st) {
     }
     LAUNCHED(1);
 }
+void launch_diagnostics(const DiagArgs &G, cudaStream_t st) {
+    k_diag_cells<<<G.ncellp, DIAG_THREADS, 0, st>>>(G); LAUNCHED(1);
+    if (G.fs) {
+        k_diag_columns<<<blocks_for(G.D.nx, 128), 128, 0, st>>>(G); LAUNCHED(1);
+    }
+    k_diag_slice<<<blocks_for((size_t)G.D.nz * G.D.nx, 256), 256, 0, st>>>(G); LAUNCHED(1);
+    k_diag_slice_sum<<<G.nslp, DIAG_SLICE_THREADS, 0, st>>>(G, 0); LAUNCHED(1);
+    k_diag_slice_mean<<<1, 32, 0, st>>>(G); LAUNCHED(1);
+    k_diag_slice_sum<<<G.nslp, DIAG_SLICE_THREADS, 0, st>>>(G, 1); LAUNCHED(1);
+    k_diag_final<<<1, 32, 0, st>>>(G); LAUNCHED(1);
+}
+
 void launch_vof_exterior(const Dom &D, const int *dist, int32_t *out, cudaStream_t st) {
     k_vof_exterior<<<blocks_for(D.n, 256), 256, 0, st>>>((int)D.n, dist, out); LAUNCHED(1);
 }

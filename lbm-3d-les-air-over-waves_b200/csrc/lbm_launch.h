@@ -5,6 +5,7 @@
 #include <cuda.h>   // CUtensorMap (the type only)
 #include <cuda_runtime.h>
 
+#include "lbm_b200.h"
 #include "lbm_dev.cuh"
 
 namespace lbm {
@@ -143,5 +144,48 @@ void launch_vof_height(const VofArgs &V, cudaStream_t st);
 cudaError_t vof_sequence(const VofArgs &V, bool collapse_due, double *tree, cudaStream_t st);
 void launch_vof_coalesce(const VofArgs &V, cudaStream_t st);
 void launch_vof_exterior(const Dom &D, const int *dist, int32_t *out, cudaStream_t st);
+
+// ---- device reductions of the harness metrics (lbm_diag.cuh)
+struct DiagCellPart {
+    unsigned long long max_key;   // (speed bits << 32) | (0xffffffff - cell): the first maximum wins ties
+    long long active, tiny, excess_count;
+    double fill_sum, mass_sum, excess_sum;
+    float min_iface;
+    int pad;
+};
+// masked sums of the slice: quantities p, p_hp, pt, pt_hp, v, v_hp over the
+// wall band and over the free-surface band
+struct DiagSlicePart {
+    double s[2][6], s2[2][6];
+    long long n[2];
+};
+
+struct DiagArgs {
+    lbm_params P;
+    int slot;
+    Dom D;
+    BedView bed;                 // geometry of the current step (no column cache)
+    const float *rho, *ux, *uy, *uz, *fill, *mass, *excess, *fs_h;
+    const int8_t *type, *type_prev;
+    int types_are_prev;          // the pressure reference of the last step used the previous types
+    int fs, vof;                 // free surface enabled, VOF tracking
+    int slice_j;
+    double rho_phys, gravity_phys;
+    DiagCellPart *cellp;         // [gridDim of k_diag_cells]
+    int ncellp;
+    double *col_eta;             // [nx] sum over y of the surface height
+    float *col_min, *col_max;    // [nx]
+    double *sl_p, *sl_pt, *sl_v; // [nz][nx] slice fields
+    uint8_t *sl_mask;            // [nz][nx] bit 0 inactive, bit 1 wall band, bit 2 free-surface band
+    DiagSlicePart *slp;          // [2][nslp]: partials of the two passes of k_diag_slice_sum
+    int nslp;
+    double *slice_mean;          // [2][6] band means of the first pass
+    lbm_diag *out;
+};
+
+constexpr int DIAG_THREADS = 256;
+constexpr int DIAG_SLICE_THREADS = 128;   // 128 slice partials of 208 bytes fit static shared memory
+
+void launch_diagnostics(const DiagArgs &G, cudaStream_t st);
 
 }  // namespace lbm

@@ -67,6 +67,34 @@ PARAM_FIELDS = [
 ]
 
 
+class LbmDiagInputs(C.Structure):
+    _fields_ = [("rho_phys", C.c_double), ("gravity_phys", C.c_double), ("slice_j", C.c_int32), ("pad", C.c_int32)]
+
+
+_D, _I64 = C.c_double, C.c_int64
+DIAG_FIELDS = [
+    ("max_speed_lb", _D), ("max_speed_phys", _D), ("max_speed_x", _D), ("max_speed_y", _D), ("max_speed_z", _D),
+    ("max_k", _I), ("max_j", _I), ("max_i", _I), ("max_speed_fs_type", _I), ("max_speed_fs_fill", _D),
+    ("max_speed_wet_neighbors", _I), ("max_speed_full_neighbors", _I), ("max_speed_gas_neighbors", _I),
+    ("pad0", _I), ("active_cells", _I64),
+    ("water_volume", _D), ("vof_mass_total", _D), ("vof_min_interface_fill", _D),
+    ("vof_tiny_interface_count", _I64), ("vof_pending_excess_mass", _D), ("vof_pending_excess_count", _I64),
+    ("surface_min", _D), ("surface_max", _D), ("surface_symmetry_l2", _D), ("surface_eta_hp_rms", _D),
+    ("surface_left_max", _D), ("surface_right_max", _D),
+    ("p_rms", _D), ("p_hp_rms", _D), ("p_total_rms", _D), ("p_total_hp_rms", _D), ("vort_rms", _D),
+    ("vort_hp_rms", _D), ("fs_p_rms", _D), ("fs_p_hp_rms", _D), ("fs_p_total_rms", _D), ("fs_p_total_hp_rms", _D),
+    ("fs_vort_rms", _D), ("fs_vort_hp_rms", _D), ("band_cells", _I64), ("fs_band_cells", _I64),
+]
+
+
+class LbmDiag(C.Structure):
+    """lbm_diag: the harness metrics reduced on the device."""
+    _fields_ = DIAG_FIELDS
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("pad")}
+
+
 class LbmParams(C.Structure):
     _fields_ = PARAM_FIELDS
 
@@ -275,6 +303,8 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.lbm_set_tile_chunk.argtypes = [vp, C.c_int32]
     lib.lbm_set_step_graphs.restype = C.c_int
     lib.lbm_set_step_graphs.argtypes = [vp, C.c_int32]
+    lib.lbm_diagnostics.restype = C.c_int
+    lib.lbm_diagnostics.argtypes = [vp, C.POINTER(LbmDiagInputs), C.POINTER(LbmDiag), vp]
     lib.lbm_set_arithmetic.restype = C.c_int
     lib.lbm_set_arithmetic.argtypes = [vp, C.c_int32]
     lib.lbm_get_arithmetic.restype = C.c_int
@@ -289,13 +319,13 @@ ABI_SYMBOLS = (
     "lbm_backend_name", "lbm_abi_version", "lbm_struct_size", "lbm_create", "lbm_bind", "lbm_init_geometry",
     "lbm_init_fields", "lbm_step", "lbm_export_diagnostics", "lbm_read_counters", "lbm_destroy", "lbm_last_error",
     "lbm_set_kernel_timing", "lbm_kernel_timing", "lbm_launch_count", "lbm_link_geometry_noalloc",
-    "lbm_set_tile_chunk", "lbm_set_step_graphs", "lbm_set_arithmetic", "lbm_get_arithmetic",
+    "lbm_set_tile_chunk", "lbm_set_step_graphs", "lbm_set_arithmetic", "lbm_get_arithmetic", "lbm_diagnostics",
 )
 
 
 def check_layout(lib: C.CDLL) -> None:
     """Raise if the library's struct sizes differ from this binding's."""
-    for which, cls in enumerate((LbmParams, LbmBuffers, LbmCounters)):
+    for which, cls in enumerate((LbmParams, LbmBuffers, LbmCounters, LbmDiag, LbmDiagInputs)):
         got = lib.lbm_struct_size(which)
         if got != C.sizeof(cls):
             raise RuntimeError(f"ABI layout mismatch for {cls.__name__}: library {got} vs binding {C.sizeof(cls)}")

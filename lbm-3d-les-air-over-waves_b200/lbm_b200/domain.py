@@ -91,6 +91,20 @@ class Domain:
         self._check(self.lib.lbm_read_counters(self.ctx, C.byref(c)), "lbm_read_counters")
         return c.as_dict()
 
+    def diagnostics(self, slice_j: int | None = None) -> dict:
+        """The harness metrics of the current state reduced on the device
+        (lbm_diagnostics): the health line's maximum speed with its location,
+        water volume and VOF accounting, surface-line and mid-slice band
+        statistics.  Only this record comes back to the host."""
+        cfg = self.cfg
+        inp = abi.LbmDiagInputs()
+        inp.rho_phys = float(cfg.rho_phys)
+        inp.gravity_phys = float(cfg.gravity_phys)
+        inp.slice_j = int(cfg.Ny // 2 if slice_j is None else slice_j)
+        out = abi.LbmDiag()
+        self._check(self.lib.lbm_diagnostics(self.ctx, C.byref(inp), C.byref(out), self._sp()), "lbm_diagnostics")
+        return out.as_dict()
+
     def set_kernel_timing(self, enable: bool):
         self._check(self.lib.lbm_set_kernel_timing(self.ctx, 1 if enable else 0), "lbm_set_kernel_timing")
 

@@ -18,8 +18,13 @@ module namespace with:
     `[None]`;
   - main(): the reference's initialisation and time loop (CODEX.py:3757-3954):
     `visualize(step, time_phys, Re_phys_air, Re_lb_base)` every plot_freq
-    steps after plot_step_start, the health line every 100 steps.  Steps
-    between those events run as one call of the engine.
+    steps after plot_step_start, the health line every 100 steps (its
+    maximum speed reduced on the device).  Steps between those events run as
+    one call of the engine;
+  - device_metrics(): the run_ab_case.py metric row of the current state,
+    reduced on the device (lbm_diagnostics), for harnesses that do not want
+    to pull whole fields; save_render_snapshot(): the render-snapshot npz of
+    run_ab_case.py:140-202.
 
 The engine itself (buffers on the device, kernels) is created on first use.
 """
@@ -186,15 +191,72 @@ def install(ns: dict, environ=None) -> None:
 
     ns["main"] = main
 
+    def device_metrics(slice_j=None) -> dict:
+        """The metric row of run_ab_case.py's make_visualize for the current
+        state (max speed and location, volume and VOF accounting, surface
+        line and mid-slice band statistics), reduced on the device."""
+        return eng.domain().diagnostics(slice_j)
+
+    ns["device_metrics"] = device_metrics
+
+    def save_render_snapshot(label, step, time_phys, output_dir):
+        """Write <output_dir>/<label>_render_<step:05d>.npz in the format of
+        run_ab_case.py:140-202 (grid, bed, obstacle mask, free-surface height
+        and fill, cube description).  Returns the path."""
+        return write_render_snapshot(ns, label=label, step=step, time_phys=time_phys, output_dir=output_dir)
+
+    ns["save_render_snapshot"] = save_render_snapshot
+
+
+def write_render_snapshot(ns, *, label: str, step: int, time_phys: float, output_dir) -> str:
+    """The render-snapshot writer of run_ab_case.py:140-202: one compressed
+    npz per call with the arrays a renderer needs, in the reference's names,
+    dtypes and shapes.  Only the format is reproduced; nothing is rendered."""
+    from pathlib import Path
+
+    out = Path(output_dir)
+    out.mkdir(parents=True, exist_ok=True)
+    fs_enabled = int(ns.get("water_free_surface_enabled", 0)) == 1
+    tracking = str(ns.get("free_surface_tracking_mode", "height"))
+    water_h = ns["water_h"].to_numpy()
+    obstacle = ns["obstacle"].to_numpy()
+    side = float(ns.get("cube_side_m", 0.0))
+    data = {
+        "time_phys": np.array(time_phys, dtype=np.float64),
+        "dx": np.array(ns["dx"], dtype=np.float64),
+        "lx_m": np.array(ns["Lx_m"], dtype=np.float64),
+        "ly_m": np.array(ns["Ly_m"], dtype=np.float64),
+        "lz_m": np.array(ns["Lz_m"], dtype=np.float64),
+        "x_phys": np.asarray(ns["x_phys"]).astype(np.float32),
+        "y_phys": np.asarray(ns["y_phys"]).astype(np.float32),
+        "z_phys": np.asarray(ns["z_phys"]).astype(np.float32),
+        "water_h": water_h.astype(np.float32),
+        "obstacle": obstacle.astype(np.uint8),
+        "free_surface_enabled": np.array(int(fs_enabled), dtype=np.int8),
+        "tracking_mode": np.array(tracking),
+        "include_cube_geometry": np.array(int(ns.get("include_cube_geometry", 0)), dtype=np.int8),
+        "cube_size_m": np.array([float(ns.get("cube_size_x_m", side)), float(ns.get("cube_size_y_m", side)),
+                                 float(ns.get("cube_size_z_m", side))], dtype=np.float32),
+        "cube_center_m": np.array([float(ns.get("cube_center_x_m", 0.0)), float(ns.get("cube_center_y_m", 0.0)),
+                                   float(ns.get("cube_center_z_m", 0.0))], dtype=np.float32),
+        "cube_yaw_pitch_deg": np.array([float(ns.get("cube_yaw_deg", 0.0)), float(ns.get("cube_pitch_deg", 0.0))],
+                                       dtype=np.float32),
+    }
+    if fs_enabled:
+        data["free_surface_h"] = ns["free_surface_h"].to_numpy().astype(np.float32)
+        data["free_surface_fill"] = ns["free_surface_fill"].to_numpy().astype(np.float32)
+    else:
+        data["free_surface_h"] = water_h.astype(np.float32)
+    path = out / f"{label}_render_{int(step):05d}.npz"
+    np.savez_compressed(path, **data)
+    return str(path)
+
 
 def _health(ns, dom, step):
-    """The reference's periodic health line (CODEX.py:3930-3954)."""
-    ux, uy, uz = (ns[k].to_numpy() for k in ("ux", "uy", "uz"))
-    active = ns["obstacle"].to_numpy() == 0
-    if ns["water_free_surface_enabled"] == 1:
-        active &= ns["free_surface_type"].to_numpy() != 0
-    speed = np.sqrt(ux ** 2 + uy ** 2 + uz ** 2)
-    max_u = float(np.nanmax(speed[active])) if active.any() else float("nan")
+    """The reference's periodic health line (CODEX.py:3930-3954).  The
+    maximum speed over active cells is reduced on the device
+    (lbm_diagnostics); only scalars come back to the host."""
+    max_u = float(dom.diagnostics()["max_speed_lb"])
     c = dom.counters()
     print(
         f"Time Step {step}, Max |U| (LB units) = {max_u:.4f}, "

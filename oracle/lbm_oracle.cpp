@@ -708,6 +708,8 @@ int64_t lbm_struct_size(int32_t which) {
         case 0: return (int64_t)sizeof(lbm_params);
         case 1: return (int64_t)sizeof(lbm_buffers);
         case 2: return (int64_t)sizeof(lbm_counters);
+        case 3: return (int64_t)sizeof(lbm_diag);
+        case 4: return (int64_t)sizeof(lbm_diag_inputs);
         default: return -1;
     }
 }
@@ -756,6 +758,10 @@ int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes) {
     return (ctx && planes >= 0) ? LBM_OK : LBM_ERR_BAD_ARG;
 }
 int lbm_set_step_graphs(lbm_ctx *ctx, int32_t) { return ctx ? LBM_OK : LBM_ERR_BAD_ARG; }
+int lbm_diagnostics(lbm_ctx *ctx, const lbm_diag_inputs *in, lbm_diag *out, void *) {
+    if (!ctx || !in || !out) return LBM_ERR_BAD_ARG;
+    return LBM_ERR_UNSUPPORTED;   // device reductions only; the oracle's fields are on the host
+}
 int lbm_set_arithmetic(lbm_ctx *ctx, int32_t mode) {
     return (ctx && (mode == LBM_ARITH_EXACT || mode == LBM_ARITH_FAST)) ? LBM_OK : LBM_ERR_BAD_ARG;
 }

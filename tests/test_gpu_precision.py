@@ -12,12 +12,17 @@ Error measures (over open, non-gas cells, after N steps):
   pressure      max |p' - p'64| / max |p'64|
   elevation     max |h - h64| / max |h64 - mean initial h| (height path)
 
-The FP32 form itself is bit-equal to the FP32 oracle (test_gpu_parity); its
-distance to FP64 is the reference algorithm's own rounding sensitivity
-(threshold branches next to the moving bed: link flips, the positivity
-limiter, the wall model), about 2.4e-3 max / 1.4e-4 rms in the air case.
-Bounds: FP32 max 5e-3, rms 5e-4; shifted FP16 rms 1.5e-3, max 5e-3;
-BF16 (8 mantissa bits) rms 5e-3, max 2e-2.
+The FP32 form itself is bit-equal to the FP32 oracle (test_gpu_parity).  Its
+distance to FP64 is the arithmetic's rounding, provided no link's open flag
+sits on a tie: the reference decides "open" by the sign of the gap between a
+link endpoint and the bed (CODEX.py:2604-2640), a discontinuous test, and a
+bed whose extremes fall exactly on link-endpoint heights (level 6, amplitude
+3 with dx = 1) gets hundreds of flags that FP32 and FP64 round to opposite
+sides (test_oracle_precision.py).  The air case here therefore uses level 6.3.
+Bounds: FP32 max 1e-4; shifted FP16 max 1e-3 (the north star's bound for the
+16-bit form); BF16 (8 mantissa bits) max 2e-2, rms 5e-3.  The water case runs
+at the water configuration's own shape (256x128x96, depth 48, Gaussian ridge
+amplitude 8, sigma 16, g = 1e-5, tau = 0.51) for 60 of its 10,000 steps.
 """
 import json
 
@@ -29,8 +34,9 @@ from oracle_runner import OracleSim
 
 pytestmark = pytest.mark.gpu
 
-VEL_MAX = {"f32": 5e-3, "f16s": 5e-3, "bf16s": 2e-2}
-VEL_RMS = {"f32": 5e-4, "f16s": 1.5e-3, "bf16s": 5e-3}
+VEL_MAX = {"f32": 1e-4, "f16s": 1e-3, "bf16s": 2e-2}
+VEL_RMS = {"f32": 1e-5, "f16s": 2.5e-4, "bf16s": 5e-3}
+PRESSURE_MAX = {"f32": 1e-4, "f16s": 2e-3, "bf16s": 5e-2}
 
 
 def _rel(a, b, mask, scale=None):
@@ -39,15 +45,28 @@ def _rel(a, b, mask, scale=None):
     return float(d.max() / s) if s > 0 else float(d.max())
 
 
+_REF = {}
+
+
+def _reference(env, steps):
+    """The FP64 oracle run of a case (kept for the storage variants)."""
+    key = (tuple(sorted(env.items())), steps)
+    if key not in _REF:
+        _REF.clear()
+        ref = OracleSim(env, fp64=True)
+        h0 = ref.arrays["fs_h"].astype(np.float64).copy()
+        ref.step(steps)
+        _REF[key] = (ref, h0)
+    return _REF[key]
+
+
 def _errors(env, storage, steps):
     from lbm_b200.domain import Domain
 
-    ref = OracleSim(env, fp64=True)
+    ref, h0 = _reference(env, steps)
     e = dict(env)
     e["LBM_B200_POP_STORAGE"] = storage
     dom = Domain(e, device="cuda:0", noise=ref.arrays["init_noise"], rho_initial=ref.arrays["rho_initial"])
-    h0 = ref.arrays["fs_h"].astype(np.float64).copy()
-    ref.step(steps)
     dom.step(steps)
     dom.synchronize()
     dom.export_diagnostics()
@@ -76,7 +95,6 @@ def _errors(env, storage, steps):
         amp = np.abs(h64 - h0.mean()).max()
         out["elevation"] = float(np.abs(h - h64).max() / amp) if amp > 0 else float(np.abs(h - h64).max())
     dom.close()
-    ref.close()
     return out
 
 
@@ -87,18 +105,20 @@ def _record(case, storage, errs):
 
 @pytest.mark.parametrize("storage", ["f32", "f16s", "bf16s"])
 def test_air_storage_error_vs_fp64(storage):
-    env = air_wave_env(64, 32, 40, amp=3.0, level=6.0, wavelength=32.0)
+    env = air_wave_env(64, 32, 40, amp=3.0, level=6.3, wavelength=32.0)
     errs = _errors(env, storage, steps=60)
-    _record("air 64x32x40, 60 steps", storage, errs)
+    _record("air 64x32x40, bed 6.3 + 3 sin, 60 steps", storage, errs)
     assert errs["velocity"] <= VEL_MAX[storage], errs
     assert errs["velocity_rms"] <= VEL_RMS[storage], errs
+    assert errs["pressure"] <= PRESSURE_MAX[storage], errs
 
 
 @pytest.mark.parametrize("storage", ["f32", "f16s", "bf16s"])
 def test_water_height_storage_error_vs_fp64(storage):
-    env = water_gaussian_env(64, 8, 32, depth=16.0, amp=3.0, sigma=8.0, g_lb=1e-3)
+    """The water configuration at its own shape, 60 steps."""
+    env = water_gaussian_env(256, 128, 96, depth=48.0, amp=8.0, sigma=16.0, g_lb=1e-5, tau0=0.51)
     errs = _errors(env, storage, steps=60)
-    _record("water height 64x8x32, 60 steps", storage, errs)
+    _record("water height 256x128x96, 60 steps", storage, errs)
     assert errs["velocity"] <= VEL_MAX[storage], errs
-    assert errs["velocity_rms"] <= VEL_RMS[storage], errs
-    assert errs["elevation"] <= VEL_RMS[storage], errs
+    assert errs["pressure"] <= PRESSURE_MAX[storage], errs
+    assert errs["elevation"] <= VEL_MAX[storage], errs

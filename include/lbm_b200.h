@@ -364,8 +364,8 @@ int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes);
    LBM_ARITH_FAST evaluates the same collision, LES rate and moments of the
    interior cells (every cell away from the bed and the top) in a reorganised
    form with contraction: the regularized and BGK collisions by opposite
-   pairs of directions (shared equilibrium terms and Hermite projections),
-   approximate reciprocal and square root.  Its results differ from the
+   pairs of directions (shared equilibrium terms and Hermite projections).
+   Its results differ from the
    exact ones by rounding; geometry, flags and every near-wall cell are
    computed exactly in both modes.  New contexts take LBM_B200_ARITH
    (fast or exact) from the environment, else exact.  Changing the mode drops
@@ -431,6 +431,27 @@ int lbm_link_geometry_noalloc(const lbm_params *params, const float *bed_h, floa
 
 int lbm_destroy(lbm_ctx *ctx);
 const char *lbm_last_error(lbm_ctx *ctx);
+
+/* Ensembles (no counterpart in the reference, which runs one domain per
+   process; replaces running run_ab_case.py once per ensemble member):
+   independent air contexts stepped together with one launch per phase of
+   the step for all of them.  The interior planes of every domain form one
+   work queue of (domain, tile, z chunk) items taken by a grid of resident
+   blocks, so domains of uneven size share the SMs; the planes next to the
+   bed and the top, the bed and the final stream run as single grids over
+   block maps of all domains.  Results equal those of stepping each context
+   with lbm_step, bit for bit.  Requirements: every context bound and
+   initialised, air mode with bed-only geometry and periodic x, nx and ny
+   multiples of 16, one population storage, LES on for all or none, all at
+   the same step; else LBM_ERR_UNSUPPORTED (message in lbm_last_error of the
+   offending context).  lbm_batch_step advances every context by nsteps on
+   stream (the contexts' own calls may be used between batch calls, keeping
+   them at one step).  The CPU oracle returns LBM_ERR_UNSUPPORTED. */
+typedef struct lbm_batch lbm_batch;
+int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out);
+int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream);
+int lbm_batch_destroy(lbm_batch *b);
+const char *lbm_batch_last_error(lbm_batch *b);
 
 #ifdef __cplusplus
 }

@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -147,8 +148,14 @@ static int cuda_check(lbm_ctx *c, cudaError_t e, const char *what) {
     } while (0)
 #define CK_LAUNCH(what) CK(cudaGetLastError(), what)
 
-static int alloc(lbm_ctx *ctx, void **p, size_t bytes) {
-    CK(cudaMalloc(p, bytes), "scratch allocation");
+// Library scratch comes from the stream-ordered allocator: allocation and
+// release are ordered on a stream and never synchronise the device, so a
+// process that creates and destroys contexts while others run (a request
+// server) does not stall their kernels.  Allocations outside a call's
+// stream (lbm_bind) are made on the legacy stream and waited for there.
+static int alloc(lbm_ctx *ctx, void **p, size_t bytes, cudaStream_t st = 0) {
+    CK(cudaMallocAsync(p, bytes, st), "scratch allocation");
+    if (st == 0) CK(cudaStreamSynchronize(0), "scratch allocation");
     ctx->owned.push_back(*p);
     return LBM_OK;
 }
@@ -437,7 +444,7 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
         const size_t ng = (size_t)(R.zcnt[0] + R.zcnt[1] + R.zcnt[2]) * P_nx(ctx) * P_ny(ctx);
         if (ctx->stash_cells < ng && !ctx->capturing) {
             float *p = nullptr;
-            if ((s = alloc(ctx, (void **)&p, 19 * ng * sizeof(float))) != LBM_OK) return s;
+            if ((s = alloc(ctx, (void **)&p, 19 * ng * sizeof(float), st)) != LBM_OK) return s;
             ctx->stash = p;
             ctx->stash_cells = ng;
         }
@@ -800,7 +807,7 @@ static int step_graph(lbm_ctx *ctx, int32_t nsteps, cudaStream_t st) {
         if (e.steps == nsteps && e.parity == par && e.cur == cur) g = &e;
     if (!g) {
         if (!ctx->dclock) {
-            int s = alloc(ctx, (void **)&ctx->dclock, sizeof(long long));
+            int s = alloc(ctx, (void **)&ctx->dclock, sizeof(long long), st);
             if (s != LBM_OK) return s;
         }
         const int64_t n0 = ctx->nstep;
@@ -938,12 +945,12 @@ int lbm_diagnostics(lbm_ctx *ctx, const lbm_diag_inputs *in, lbm_diag *out, void
     const size_t nx = (size_t)ctx->P.nx, nzx = (size_t)ctx->P.nz * nx;
     int s;
     if (!ctx->d_out) {
-        if ((s = alloc(ctx, (void **)&ctx->d_cellp, ncellp * sizeof(DiagCellPart))) ||
-            (s = alloc(ctx, (void **)&ctx->d_slp, 2 * nslp * sizeof(DiagSlicePart) + 12 * sizeof(double))) ||
-            (s = alloc(ctx, (void **)&ctx->d_col_eta, nx * sizeof(double))) ||
-            (s = alloc(ctx, (void **)&ctx->d_col_mm, 2 * nx * sizeof(float))) ||
-            (s = alloc(ctx, (void **)&ctx->d_slice, 3 * nzx * sizeof(double))) ||
-            (s = alloc(ctx, (void **)&ctx->d_mask, nzx)) || (s = alloc(ctx, (void **)&ctx->d_out, sizeof(lbm_diag))))
+        if ((s = alloc(ctx, (void **)&ctx->d_cellp, ncellp * sizeof(DiagCellPart), st)) ||
+            (s = alloc(ctx, (void **)&ctx->d_slp, 2 * nslp * sizeof(DiagSlicePart) + 12 * sizeof(double), st)) ||
+            (s = alloc(ctx, (void **)&ctx->d_col_eta, nx * sizeof(double), st)) ||
+            (s = alloc(ctx, (void **)&ctx->d_col_mm, 2 * nx * sizeof(float), st)) ||
+            (s = alloc(ctx, (void **)&ctx->d_slice, 3 * nzx * sizeof(double), st)) ||
+            (s = alloc(ctx, (void **)&ctx->d_mask, nzx, st)) || (s = alloc(ctx, (void **)&ctx->d_out, sizeof(lbm_diag), st)))
             return s;
     }
     if ((s = load_bed_slot(ctx, (int)(ctx->nstep & 1), st)) != LBM_OK) return s;
@@ -1044,12 +1051,258 @@ int lbm_destroy(lbm_ctx *ctx) {
     if (!ctx) return LBM_ERR_BAD_ARG;
     drop_graphs(ctx);
     for (cudaEvent_t e : ctx->ev) cudaEventDestroy(e);
-    for (void *p : ctx->owned) cudaFree(p);
+    // released in the order of the context's stream, after its last work
+    for (void *p : ctx->owned) cudaFreeAsync(p, ctx->last_stream);
     release_slot(ctx->slot);
     delete ctx;
     return LBM_OK;
 }
 
 const char *lbm_last_error(lbm_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ ensembles
+// An ensemble of air contexts stepped together with one launch per phase of
+// the step (lbm_batch.cuh).  The tables of block maps and work items are
+// built once; the per-domain step arguments and bed pointers (which depend on
+// the step's parity) are uploaded at the start of each call.
+struct lbm_batch {
+    std::vector<lbm_ctx *> ctx;
+    std::vector<Plan> plan;
+    std::vector<bool> stash;
+    int storage = 0;
+    bool les = false;
+    BatchLaunch L{};
+    StepArgs *d_tab = nullptr, *h_tab = nullptr;
+    BatchBed *d_bed = nullptr, *h_bed = nullptr;
+    long long *d_col0 = nullptr;
+    int4 *d_gmap = nullptr, *d_smap = nullptr, *d_items = nullptr;
+    int *d_queue = nullptr;
+    std::string err;
+};
+
+static int batch_fail(lbm_batch *b, int code, const std::string &msg) {
+    if (b) b->err = msg;
+    return code;
+}
+
+static void batch_free(lbm_batch *b) {
+    cudaFree(b->d_tab);
+    cudaFree(b->d_bed);
+    cudaFree(b->d_col0);
+    cudaFree(b->d_gmap);
+    cudaFree(b->d_smap);
+    cudaFree(b->d_items);
+    cudaFree(b->d_queue);
+    cudaFreeHost(b->h_tab);
+    cudaFreeHost(b->h_bed);
+}
+
+template <typename T>
+static cudaError_t upload_vec(T **dst, const std::vector<T> &v) {
+    cudaError_t e = cudaMalloc((void **)dst, (v.empty() ? 1 : v.size()) * sizeof(T));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+extern "C" {
+
+int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
+    if (!ctxs || n < 1 || !out) return LBM_ERR_BAD_ARG;
+    *out = nullptr;
+    lbm_batch *b = new lbm_batch();
+    lbm_ctx *c0 = ctxs[0];
+    for (int d = 0; d < n; ++d) {
+        lbm_ctx *c = ctxs[d];
+        if (!c || !c->bound) {
+            delete b;
+            return LBM_ERR_NOT_BOUND;
+        }
+        const Plan R = plan_planes(c);
+        std::string why;
+        if (c->P.fs_mode != LBM_FS_NONE) why = "air domains only";
+        else if (!c->use_cg) why = "bed-only geometry with periodic x (column-cache path) only";
+        else if (!R.tile || R.classic) why = "the interior-plane path is required (nx, ny multiples of 16)";
+        else if (c->P.pop_storage != c0->P.pop_storage) why = "one population storage for the whole ensemble";
+        else if ((c->P.use_les != 0) != (c0->P.use_les != 0)) why = "LES on for every domain or for none";
+        else if (c->nstep != c0->nstep || c->cur != c0->cur) why = "every domain at the same step";
+        if (!why.empty()) {
+            delete b;
+            return fail(c, LBM_ERR_UNSUPPORTED, "lbm_batch_create: domain " + std::to_string(d) + ": " + why);
+        }
+        b->ctx.push_back(c);
+        b->plan.push_back(R);
+    }
+    b->storage = c0->P.pop_storage;
+    b->les = c0->P.use_les != 0;
+    std::vector<long long> col0(1, 0);
+    std::vector<int4> gmap, smap, items;
+    for (int d = 0; d < n; ++d) {
+        lbm_ctx *c = b->ctx[d];
+        const Plan &R = b->plan[d];
+        const int nx = c->P.nx, ny = c->P.ny;
+        col0.push_back(col0.back() + (long long)nx * ny);
+        const int gx = (nx + 31) / 32, gy = (ny + 7) / 8, gz = R.zcnt[0] + R.zcnt[1] + R.zcnt[2];
+        for (int bz = 0; bz < gz; ++bz)
+            for (int by = 0; by < gy; ++by)
+                for (int bx = 0; bx < gx; ++bx) gmap.push_back(make_int4(d, bx, by, bz));
+        const int ni = R.zi1 - R.zi0 + 1, tx = nx / LBM_TILE, ty = ny / LBM_TILE;
+        for (int bz = 0; bz < ni; ++bz)
+            for (int by = 0; by < ty; ++by)
+                for (int bx = 0; bx < tx; ++bx) smap.push_back(make_int4(d, bx, by, bz));
+        const int nc = (ni + R.chunk - 1) / R.chunk;
+        for (int cz = 0; cz < nc; ++cz)
+            for (int by = 0; by < ty; ++by)
+                for (int bx = 0; bx < tx; ++bx) items.push_back(make_int4(d, bx, by, cz));
+        // 16-bit storage with LES: the general pre-pass hands its FP32 populations to the collide through the stash
+        bool st = false;
+        if (b->les && b->storage != LBM_STORE_F32) {
+            const size_t ng = (size_t)gz * nx * ny;
+            if (c->stash_cells < ng) {
+                float *p = nullptr;
+                if (alloc(c, (void **)&p, 19 * ng * sizeof(float)) != LBM_OK) {
+                    delete b;
+                    return LBM_ERR_CUDA;
+                }
+                c->stash = p;
+                c->stash_cells = ng;
+            }
+            st = true;
+        } else if (b->les) {
+            st = true;   // FP32: the pre-pass leaves them in the destination slots
+        }
+        b->stash.push_back(st);
+    }
+    // longest items first: the last items of the queue are the short ones
+    std::stable_sort(items.begin(), items.end(), [&](const int4 &x, const int4 &y) {
+        const Plan &Rx = b->plan[x.x], &Ry = b->plan[y.x];
+        const int px = std::min(Rx.chunk, Rx.zi1 + 1 - (Rx.zi0 + x.w * Rx.chunk));
+        const int py = std::min(Ry.chunk, Ry.zi1 + 1 - (Ry.zi0 + y.w * Ry.chunk));
+        return px > py;
+    });
+    cudaError_t e = cudaSuccess;
+    if ((e = upload_vec(&b->d_col0, col0)) != cudaSuccess || (e = upload_vec(&b->d_gmap, gmap)) != cudaSuccess ||
+        (e = upload_vec(&b->d_smap, smap)) != cudaSuccess || (e = upload_vec(&b->d_items, items)) != cudaSuccess ||
+        (e = cudaMalloc((void **)&b->d_queue, sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc((void **)&b->d_tab, 2 * n * sizeof(StepArgs))) != cudaSuccess ||
+        (e = cudaMalloc((void **)&b->d_bed, 2 * n * sizeof(BatchBed))) != cudaSuccess ||
+        (e = cudaMallocHost((void **)&b->h_tab, 2 * n * sizeof(StepArgs))) != cudaSuccess ||
+        (e = cudaMallocHost((void **)&b->h_bed, 2 * n * sizeof(BatchBed))) != cudaSuccess) {
+        batch_free(b);
+        delete b;
+        return fail(c0, LBM_ERR_CUDA, std::string("lbm_batch_create: ") + cudaGetErrorString(e));
+    }
+    BatchLaunch &L = b->L;
+    L.tab = b->d_tab;
+    L.bed = b->d_bed;
+    L.col0 = b->d_col0;
+    L.ndom = n;
+    L.ncols = col0.back();
+    L.gmap = b->d_gmap;
+    L.ngen = (int)gmap.size();
+    L.smap = b->d_smap;
+    L.nsi = (int)smap.size();
+    L.items = b->d_items;
+    L.nitems = (int)items.size();
+    L.queue = b->d_queue;
+    L.tile_blocks = batch_tile_blocks(b->storage);
+    if (L.tile_blocks <= 0) {
+        batch_free(b);
+        delete b;
+        return fail(c0, LBM_ERR_UNSUPPORTED, "lbm_batch_create: the interior grid's shared memory was refused");
+    }
+    *out = b;
+    return LBM_OK;
+}
+
+int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
+    if (!b || nsteps < 0) return LBM_ERR_BAD_ARG;
+    if (nsteps == 0) return LBM_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int n = (int)b->ctx.size();
+    const int64_t n0 = b->ctx[0]->nstep;
+    const int cur0 = b->ctx[0]->cur;
+    for (lbm_ctx *c : b->ctx)
+        if (c->nstep != n0 || c->cur != cur0) return batch_fail(b, LBM_ERR_BAD_ARG, "lbm_batch_step: domains out of step");
+    // the bound bed state into the slots of step n0; the step arguments of the call
+    for (int d = 0; d < n; ++d) {
+        lbm_ctx *c = b->ctx[d];
+        c->last_stream = st;
+        const int s = load_bed_slot(c, (int)(n0 & 1), st);
+        if (s != LBM_OK) return batch_fail(b, s, c->err);
+        for (int q = 0; q < 2; ++q) {
+            StepArgs A = step_args(c);
+            apply_plan(A, b->plan[d]);
+            const int src = cur0 ^ q;
+            A.fsrc = c->b.f[src];
+            A.fdst = c->b.f[1 - src];
+            A.bed_s = slot_view(c, (int)((n0 + q) & 1));
+            A.bed_c = slot_view(c, (int)((n0 + 1 + q) & 1));
+            A.stash = c->stash;
+            b->h_tab[q * n + d] = A;
+            const int par = q;   // bed variant by the parity of the bed step
+            BatchBed &B = b->h_bed[par * n + d];
+            B.P = c->P;
+            B.D = c->D;
+            B.h_prev = c->bed_h[1 - par];
+            B.h = c->bed_h[par];
+            B.hmax = c->bed_hmax[par];
+            B.uw = c->bed_uw[par];
+            B.vw = c->bed_vw[par];
+            B.ww = c->bed_ww[par];
+            B.cg = c->use_cg ? c->bed_cg[par] : nullptr;
+            B.piecewise = c->b.piecewise_bed_z;
+        }
+    }
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(b->d_tab, b->h_tab, 2 * n * sizeof(StepArgs), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(b->d_bed, b->h_bed, 2 * n * sizeof(BatchBed), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return batch_fail(b, LBM_ERR_CUDA, cudaGetErrorString(e));
+    const BatchLaunch &L = b->L;
+    const int S = b->storage;
+    const int tflag = b->stash[0] ? F_STASH : 0;
+    const int K = nsteps;
+    // first step of the call: collide from the stored post-stream state
+    launch_batch_bed(L, n0 + 1, st);
+    int flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
+    if (b->les) launch_batch_kernel(KER_PREPASS_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st);
+    launch_batch_kernel(KER_TILE_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st);
+    launch_batch_kernel(KER_COLLIDE_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st);
+    // fused steps: stream + boundary conditions of step m, condition ... collide of step m + 1
+    for (int s = 1; s < K; ++s) {
+        const int64_t m = n0 + s;
+        launch_batch_bed(L, m + 1, st);
+        flags = ((s == K - 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
+        const int q = s & 1;
+        if (b->les) launch_batch_kernel(KER_PREPASS_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st);
+        launch_batch_kernel(KER_TILE_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st);
+        launch_batch_kernel(KER_COLLIDE_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st);
+    }
+    // the final stream back to the post-stream state
+    for (lbm_ctx *c : b->ctx)
+        if ((e = cudaMemsetAsync(c->dcount, 0, 3 * sizeof(int), st)) != cudaSuccess)
+            return batch_fail(b, LBM_ERR_CUDA, cudaGetErrorString(e));
+    launch_batch_kernel(KER_STREAM, S, L, K & 1, (unsigned long long)(n0 + K), F_COUNT, st);
+    launch_batch_kernel(KER_STREAM_INTERIOR, S, L, K & 1, (unsigned long long)(n0 + K), F_COUNT, st);
+    if ((e = cudaGetLastError()) != cudaSuccess) return batch_fail(b, LBM_ERR_CUDA, cudaGetErrorString(e));
+    const int src_final = cur0 ^ (K & 1);
+    for (lbm_ctx *c : b->ctx) {
+        c->cur = 1 - src_final;
+        c->nstep = n0 + K;
+        const int s = store_bed_slot(c, (int)((n0 + K) & 1), c->bed_h[(n0 + K - 1) & 1], st);
+        if (s != LBM_OK) return batch_fail(b, s, c->err);
+    }
+    return LBM_OK;
+}
+
+int lbm_batch_destroy(lbm_batch *b) {
+    if (!b) return LBM_ERR_BAD_ARG;
+    batch_free(b);
+    delete b;
+    return LBM_OK;
+}
+
+const char *lbm_batch_last_error(lbm_batch *b) { return b ? b->err.c_str() : "null batch"; }
 
 }  // extern "C"

@@ -1,0 +1,151 @@
+// lbm_batch.cuh - an ensemble of air domains stepped with one launch per
+// phase.
+//
+// Each phase of the air step (bed, 3x3 maximum and column cache; general
+// pre-pass; interior planes; general collide; the final stream) runs as one
+// grid over all domains of the ensemble, with each block's domain and
+// coordinates taken from device tables built when the ensemble is created:
+//   kb_bed / kb_hmax / kb_colgeo   one thread per column of the concatenated
+//                                  columns of all domains
+//   kb_general                     one block of 32 x 8 cells per map entry
+//                                  (domain, bx, by, bz): pre-pass, collide or
+//                                  stream of the planes next to the bed and
+//                                  the top
+//   kb_tile                        the interior planes as a work queue: a
+//                                  grid of resident blocks, each taking the
+//                                  next (domain, tile, z chunk) item from a
+//                                  counter until none is left, so domains of
+//                                  uneven size share the SMs without a tail
+//                                  per domain
+//   kb_stream_interior             one block per map entry
+// A block copies its domain's step arguments into shared memory and runs the
+// same per-block body as a domain's own launch (prepass_body, collide_body,
+// stream_body, tile_pipe_body / tile_pipe16_body, stream_interior_body), so
+// an ensemble steps bit for bit like its domains stepped one by one.
+#pragma once
+
+#include "lbm_tile.cuh"
+
+namespace lbm {
+
+// copy a domain's step arguments into shared memory (all threads of the block)
+LBM_DEV void batch_load_args(StepArgs &dst, const StepArgs &src) {
+    const int nw = (int)(sizeof(StepArgs) / 4);
+    const unsigned *s = (const unsigned *)&src;
+    unsigned *d = (unsigned *)&dst;
+    const int t = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
+    for (int w = t; w < nw; w += nt) d[w] = s[w];
+}
+static_assert(sizeof(StepArgs) % 4 == 0, "step arguments copy as words");
+
+// domain of concatenated column g: the last d with col0[d] <= g
+LBM_DEV int batch_domain(const long long *col0, int ndom, long long g) {
+    int lo = 0, hi = ndom - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (col0[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void kb_bed(BatchLaunch L, long long m, int par) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= L.ncols) return;
+    const int d = batch_domain(L.col0, L.ndom, g);
+    const BatchBed &B = L.bed[par * L.ndom + d];
+    const float t = (float)((double)(m + 1) * B.P.dt_phys);   // the host's step time, CODEX.py:3874
+    bed_column(B.P, B.D, B.h_prev, B.h, B.uw, B.vw, B.ww, B.piecewise, t, (int)(g - L.col0[d]));
+}
+__global__ void kb_hmax(BatchLaunch L, int par) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= L.ncols) return;
+    const int d = batch_domain(L.col0, L.ndom, g);
+    const BatchBed &B = L.bed[par * L.ndom + d];
+    hmax_column(B.D, B.h, B.hmax, (int)(g - L.col0[d]));
+}
+__global__ void kb_colgeo(BatchLaunch L, int par) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= L.ncols) return;
+    const int d = batch_domain(L.col0, L.ndom, g);
+    const BatchBed &B = L.bed[par * L.ndom + d];
+    if (!B.cg) return;
+    const int a = (int)(g - L.col0[d]), j = a / B.D.nx, i = a - j * B.D.nx;
+    BedView V;
+    V.h = B.h; V.hmax = B.hmax; V.uw = B.uw; V.vw = B.vw; V.ww = B.ww; V.cg = B.cg;
+    colgeo_column(B.P, B.D, V, j, i, B.cg);
+}
+
+// KIND 0: pre-pass, 1: collide, 2: stream (column-cache kernels)
+template <int S, int IN, int KIND>
+__global__ void __launch_bounds__(256, KIND == 0 ? LBM_CG_PRE_MINB : LBM_CG_MINB)
+    kb_general(BatchLaunch L, int q, unsigned long long step, int flags) {
+    __shared__ __align__(16) StepArgs sA;
+    const int4 m = L.gmap[blockIdx.x];
+    batch_load_args(sA, L.tab[q * L.ndom + m.x]);
+    __syncthreads();
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        sA.step = step;
+        sA.flags = flags;
+    }
+    __syncthreads();
+    const int gz = sA.zcnt[0] + sA.zcnt[1] + sA.zcnt[2];
+    if constexpr (KIND == 0) prepass_body<S, IN, true>(sA, m.y, m.z, m.w, gz);
+    else if constexpr (KIND == 1) collide_body<S, IN, true>(sA, m.y, m.z, m.w, gz);
+    else stream_body<S, true>(sA, m.y, m.z, m.w);
+}
+
+template <int S>
+__global__ void __launch_bounds__(256) kb_stream_interior(BatchLaunch L, int q, unsigned long long step, int flags) {
+    __shared__ __align__(16) StepArgs sA;
+    const int4 m = L.smap[blockIdx.x];
+    batch_load_args(sA, L.tab[q * L.ndom + m.x]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        sA.step = step;
+        sA.flags = flags;
+    }
+    __syncthreads();
+    stream_interior_body<S>(sA, m.y, m.z, m.w);
+}
+
+template <int S>
+constexpr int batch_tile_smem() {
+    return S == LBM_STORE_F32 ? PIPE_SMEM_BYTES : P16_SMEM_BYTES;
+}
+
+// the interior planes of every domain as a work queue
+template <int S, int IN>
+__global__ void __launch_bounds__(256, 2) kb_tile(BatchLaunch L, int q, unsigned long long step, int flags) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ __align__(16) StepArgs sA;
+    __shared__ int s_item;
+    int cur = -1;
+    for (;;) {
+        __syncthreads();   // every thread is done with the last item's shared memory
+        if (threadIdx.x == 0) s_item = atomicAdd(L.queue, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= L.nitems) break;
+        const int4 it = L.items[item];
+        if (it.x != cur) {
+            batch_load_args(sA, L.tab[q * L.ndom + it.x]);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                sA.step = step;
+                sA.flags = flags;
+            }
+            __syncthreads();
+            cur = it.x;
+        }
+        if constexpr (S == LBM_STORE_F32) {
+            if (sA.P.use_les) tile_pipe_body<IN, true>(sA, smem, it.y, it.z, it.w);
+            else tile_pipe_body<IN, false>(sA, smem, it.y, it.z, it.w);
+        } else {
+            if (sA.P.use_les) tile_pipe16_body<S, IN, true>(sA, smem, it.y, it.z, it.w);
+            else tile_pipe16_body<S, IN, false>(sA, smem, it.y, it.z, it.w);
+        }
+    }
+}
+
+}  // namespace lbm

@@ -46,13 +46,13 @@ long long launch_count() { return g_launches.load(); }
 void launch_count_add(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 #define LAUNCHED(n) g_launches.fetch_add((n), std::memory_order_relaxed)
 
-// 3-D launch of the general kernels: block (32, 8), grid (ceil(nx/32),
-// ceil(ny/8), planes), blockIdx.z walking the launch's z ranges
-__device__ __forceinline__ bool cell_xyz(const StepArgs &A, int &i, int &j, int &k, int &c) {
+// 3-D launch of the general kernels: block (32, 8) covering x [32 bx, 32 bx
+// + 32) and y [8 by, 8 by + 8) of the bz-th plane of the launch's z ranges
+// (a domain's own launch: grid (ceil(nx/32), ceil(ny/8), planes))
+__device__ __forceinline__ bool cell_xyz(const StepArgs &A, int bx, int by, int bz, int &i, int &j, int &k, int &c) {
     const Dom &D = A.D;
-    i = blockIdx.x * blockDim.x + threadIdx.x;
-    j = blockIdx.y * blockDim.y + threadIdx.y;
-    int bz = blockIdx.z;
+    i = bx * 32 + threadIdx.x;
+    j = by * 8 + threadIdx.y;
     if (bz < A.zcnt[0]) k = A.zlo[0] + bz;
     else if (bz < A.zcnt[0] + A.zcnt[1]) k = A.zlo[1] + (bz - A.zcnt[0]);
     else k = A.zlo[2] + (bz - A.zcnt[0] - A.zcnt[1]);
@@ -102,12 +102,11 @@ __device__ __forceinline__ float gaussian_h(const lbm_params &P, const Dom &D, f
 }
 
 // ------------------------------------------------------------- bed (2-D)
-// update_wave_bed_and_velocities, CODEX.py:1082-1162, harmonics generalised
-__global__ void k_bed(lbm_params P, Dom D, const float *__restrict__ h_prev, float *h, float *uw, float *vw,
-                      float *ww, const float *__restrict__ piecewise, float t, const long long *clock, long long off) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= (int)D.a) return;
-    if (clock) t = (float)((double)(*clock + off + 1) * P.dt_phys);  // the host's step time, CODEX.py:3874
+// update_wave_bed_and_velocities, CODEX.py:1082-1162, harmonics generalised,
+// for column a at time t
+__device__ __forceinline__ void bed_column(const lbm_params &P, const Dom &D, const float *__restrict__ h_prev,
+                                           float *h, float *uw, float *vw, float *ww,
+                                           const float *__restrict__ piecewise, float t, int a) {
     int i = a % D.nx;
     const bool moving = P.bed_profile == LBM_BED_MOVING_SINE;
     float a1 = 0.0f, a2 = 0.0f;
@@ -150,12 +149,17 @@ __global__ void k_bed(lbm_params P, Dom D, const float *__restrict__ h_prev, flo
     vw[a] = vs / P.vel_scale;
     ww[a] = ws / P.vel_scale;
 }
+__global__ void k_bed(lbm_params P, Dom D, const float *__restrict__ h_prev, float *h, float *uw, float *vw,
+                      float *ww, const float *__restrict__ piecewise, float t, const long long *clock, long long off) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (int)D.a) return;
+    if (clock) t = (float)((double)(*clock + off + 1) * P.dt_phys);  // the host's step time, CODEX.py:3874
+    bed_column(P, D, h_prev, h, uw, vw, ww, piecewise, t, a);
+}
 
 // max of the bed over the 3x3 column neighbourhood (periodic): the support
 // of every link-endpoint sample of the column
-__global__ void k_hmax(Dom D, const float *__restrict__ h, float *hmax) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= (int)D.a) return;
+__device__ __forceinline__ void hmax_column(const Dom &D, const float *__restrict__ h, float *hmax, int a) {
     int j = a / D.nx, i = a - j * D.nx;
     float m = -3.4e38f;
     for (int dj = -1; dj <= 1; ++dj)
@@ -164,6 +168,11 @@ __global__ void k_hmax(Dom D, const float *__restrict__ h, float *hmax) {
             m = fmaxf(m, h[D.col(jj, ii)]);
         }
     hmax[a] = m;
+}
+__global__ void k_hmax(Dom D, const float *__restrict__ h, float *hmax) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= (int)D.a) return;
+    hmax_column(D, h, hmax, a);
 }
 
 // per-column link-endpoint cache of one bed state (bed-only geometry)
@@ -247,9 +256,14 @@ __device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int 
     return hmin > ((float)k + 1.01f) * dx ? 2 : 0;
 }
 
+// gas_free: the caller does not read the populations of a gas cell (the
+// velocity pre-pass, whose gas velocity is zero, and the regularized
+// collision, whose gas output is the rest equilibrium), so with a free
+// surface they are not loaded for gas cells
 template <int S, int IN, bool CG>
 __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, int i, float f[19], bool &fast_c,
-                                      bool &open, int &type, float &gbf, float &r, float &vx, float &vy, float &vz) {
+                                      bool &open, int &type, float &gbf, float &r, float &vx, float &vy, float &vz,
+                                      bool gas_free = false) {
     const lbm_params &P = A.P;
     // the column cache is used in air mode only: CG kernels carry no
     // free-surface code
@@ -266,6 +280,15 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
     }
     GeoLinks Lc;
     Geo gc = geo_cell<CG>(P, A.slot, A.D, A.bed_c, k, j, i, Lc, true, P.use_link_wall_velocity && P.include_bed);
+    fast_c = gc.fast;
+    open = (gc.lo & 1u) != 0u;
+    type = LBM_FS_LIQUID;
+    float fill = 1.0f;
+    gbf = 0.0f;
+    if (water) {
+        fs_state(A, c, k, j, i, open, type, fill);
+        gbf = gbf_of(P, k, open, type);
+    }
     // A cell with every link closed in the collide geometry (air): the
     // condition stage sets f_q = frac_q f_q + (1 - frac_q) feq_q on every
     // link, with frac_q = 0 for q >= 1, so only the rest population of the
@@ -275,7 +298,11 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
     const bool solid_c = gc.lo == 0u && !water && !P.physics_water &&
                          !(P.enable_x_fringe && i < 5 && k > A.D.nz / 2) &&
                          !(P.enable_top_drive && k == A.D.nz - 1);
-    if (solid_c) {
+    if (water && gas_free && type == LBM_FS_GAS) {
+        // macro_step gives (rho0, 0) for a gas cell whatever its populations
+#pragma unroll
+        for (int q = 0; q < 19; ++q) f[q] = 0.0f;
+    } else if (solid_c) {
         f[0] = Store<S>::ld((const typename Store<S>::T *)A.fsrc, (size_t)c, 0, P.rho0);
 #pragma unroll
         for (int q = 1; q < 19; ++q) f[q] = 0.0f;
@@ -287,27 +314,24 @@ __device__ __forceinline__ void front(const StepArgs &A, int c, int k, int j, in
         int cut = 0, fscut = 0, bridge = 0;
         stream_bc<S, CG>(A, (const typename Store<S>::T *)A.fsrc, gs, Ls, k, j, i, c, f, cut, fscut, bridge);
     }
-    fast_c = gc.fast;
-    open = (gc.lo & 1u) != 0u;
-    type = LBM_FS_LIQUID;
-    float fill = 1.0f;
-    gbf = 0.0f;
-    if (water) {
-        fs_state(A, c, k, j, i, open, type, fill);
-        gbf = gbf_of(P, k, open, type);
-    }
     condition(P, A.D, A.bed_c, gc, Lc, k, j, i, f);
     macro(P, A.D, f, k, water, type, gbf, r, vx, vy, vz);
 }
 
+// Bodies of the general kernels, with the block's coordinates explicit (bz
+// walks the launch's z ranges, gz is their total), so that one body serves
+// a domain's own launch and the batched launches over many domains.
 template <int S, int IN, bool CG>
-__global__ void __launch_bounds__(256, CG ? LBM_CG_PRE_MINB : LBM_GEN_MINB) k_prepass(StepArgs A) {
+__device__ __forceinline__ void prepass_body(const StepArgs &A, int bx, int by, int bz, int gz) {
     int i, j, k, c;
-    if (!cell_xyz(A, i, j, k, c)) return;
+    if (!cell_xyz(A, bx, by, bz, i, j, k, c)) return;
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
-    front<S, IN, CG>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
+    // with the stash the collide pass reads these populations back; without
+    // it only the velocity is used
+    const bool gas_free = !(CG && (A.flags & F_STASH));
+    front<S, IN, CG>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz, gas_free);
     A.u_out[c] = vx;
     A.u_out[A.D.n + c] = vy;
     A.u_out[2 * A.D.n + c] = vz;
@@ -318,18 +342,22 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_PRE_MINB : LBM_GEN_MINB) k_pr
         if (S == LBM_STORE_F32) {
             store_cell<S>(A, c, f);
         } else {
-            const size_t ng = (size_t)gridDim.z * A.D.nx * A.D.ny;
-            const size_t g = ((size_t)blockIdx.z * A.D.ny + j) * A.D.nx + i;
+            const size_t ng = (size_t)gz * A.D.nx * A.D.ny;
+            const size_t g = ((size_t)bz * A.D.ny + j) * A.D.nx + i;
 #pragma unroll
             for (int q = 0; q < 19; ++q) A.stash[q * ng + g] = f[q];
         }
     }
 }
+template <int S, int IN, bool CG>
+__global__ void __launch_bounds__(256, CG ? LBM_CG_PRE_MINB : LBM_GEN_MINB) k_prepass(StepArgs A) {
+    prepass_body<S, IN, CG>(A, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.z);
+}
 
 template <int S, int IN, bool CG>
-__global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collide(StepArgs A) {
+__device__ __forceinline__ void collide_body(const StepArgs &A, int bx, int by, int bz, int gz) {
     int i, j, k, c;
-    if (!cell_xyz(A, i, j, k, c)) return;
+    if (!cell_xyz(A, bx, by, bz, i, j, k, c)) return;
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
@@ -342,8 +370,8 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collid
 #pragma unroll
             for (int q = 0; q < 19; ++q) f[q] = fd[(size_t)q * A.D.n + c];
         } else {
-            const size_t ng = (size_t)gridDim.z * A.D.nx * A.D.ny;
-            const size_t g = ((size_t)blockIdx.z * A.D.ny + j) * A.D.nx + i;
+            const size_t ng = (size_t)gz * A.D.nx * A.D.ny;
+            const size_t g = ((size_t)bz * A.D.ny + j) * A.D.nx + i;
 #pragma unroll
             for (int q = 0; q < 19; ++q) f[q] = A.stash[q * ng + g];
         }
@@ -355,7 +383,8 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collid
         gbf = 0.0f;
         macro(A.P, A.D, f, k, false, type, gbf, r, vx, vy, vz);
     } else {
-        front<S, IN, CG>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz);
+        front<S, IN, CG>(A, c, k, j, i, f, fast_c, open, type, gbf, r, vx, vy, vz,
+                         A.P.collision == LBM_COLLIDE_REGULARIZED);
     }
     const lbm_params &P = A.P;
     const bool water = !CG && P.fs_mode != LBM_FS_NONE;
@@ -378,12 +407,16 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collid
     collide(A, c, k, !open, water, gas, gbf, r, vx, vy, vz, om, f);
     store_cell<S>(A, c, f);
 }
+template <int S, int IN, bool CG>
+__global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collide(StepArgs A) {
+    collide_body<S, IN, CG>(A, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.z);
+}
 
 template <int S, bool CG>
-__global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream(StepArgs A) {
+__device__ __forceinline__ void stream_body(const StepArgs &A, int bx, int by, int bz) {
     int i, j, k, c;
     int cut = 0, fscut = 0, bridge = 0;
-    if (cell_xyz(A, i, j, k, c)) {
+    if (cell_xyz(A, bx, by, bz, i, j, k, c)) {
         float f[19];
         const int wcls = CG ? 0 : water_stream_class(A, k, j, i);
         if (cell_fast(A, true, false, k, j, i)) {
@@ -457,6 +490,16 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream
         }
     }
 }
+template <int S, bool CG>
+__global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream(StepArgs A) {
+    stream_body<S, CG>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+}  // namespace lbm
+
+#include "lbm_batch.cuh"
+
+namespace lbm {
 
 // -------------------------------------------- height-function free surface
 // compute_free_surface_column_flux, CODEX.py:2376-2388 (sequential in k)
@@ -1377,6 +1420,82 @@ void launch_vof_coalesce(const VofArgs &V, cudaStream_t st) {
     }
     LAUNCHED(1);
 }
+// ------------------------------------------------------ ensemble launchers
+void launch_batch_bed(const BatchLaunch &L, long long m, cudaStream_t st) {
+    const int par = (int)(m & 1);
+    const unsigned g = blocks_for((size_t)L.ncols, 256);
+    kb_bed<<<g, 256, 0, st>>>(L, m, par); LAUNCHED(1);
+    kb_hmax<<<g, 256, 0, st>>>(L, par); LAUNCHED(1);
+    kb_colgeo<<<blocks_for((size_t)L.ncols, 128), 128, 0, st>>>(L, par); LAUNCHED(1);
+}
+
+template <int S>
+static bool batch_smem_ready() {
+    static bool done[64] = {false}, ok[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    if (!done[dev]) {
+        done[dev] = true;
+        ok[dev] = cudaFuncSetAttribute(kb_tile<S, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       batch_tile_smem<S>()) == cudaSuccess &&
+                  cudaFuncSetAttribute(kb_tile<S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       batch_tile_smem<S>()) == cudaSuccess;
+    }
+    return ok[dev];
+}
+
+template <int S>
+static int batch_tile_blocks_s() {
+    if (!batch_smem_ready<S>()) return 0;
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kb_tile<S, 1>, 256, batch_tile_smem<S>()) != cudaSuccess)
+        return 0;
+    return per * sms;
+}
+int batch_tile_blocks(int storage) {
+    switch (storage) {
+        case LBM_STORE_F16S: return batch_tile_blocks_s<LBM_STORE_F16S>();
+        case LBM_STORE_BF16S: return batch_tile_blocks_s<LBM_STORE_BF16S>();
+        default: return batch_tile_blocks_s<LBM_STORE_F32>();
+    }
+}
+
+template <int S>
+static void launch_batch_kernel_s(int which, const BatchLaunch &L, int q, unsigned long long step, int flags,
+                                  cudaStream_t st) {
+    const dim3 b3(32, 8, 1);
+    switch (which) {
+        case KER_PREPASS_CANON: if (L.ngen) { kb_general<S, 0, 0><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
+        case KER_PREPASS_FUSED: if (L.ngen) { kb_general<S, 1, 0><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
+        case KER_COLLIDE_CANON: if (L.ngen) { kb_general<S, 0, 1><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
+        case KER_COLLIDE_FUSED: if (L.ngen) { kb_general<S, 1, 1><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
+        case KER_STREAM: if (L.ngen) { kb_general<S, 0, 2><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
+        case KER_STREAM_INTERIOR:
+            if (L.nsi) { kb_stream_interior<S><<<L.nsi, 256, 0, st>>>(L, q, step, flags); LAUNCHED(1); }
+            break;
+        case KER_TILE_CANON:
+        case KER_TILE_FUSED: {
+            if (!L.nitems || !L.tile_blocks) break;
+            cudaMemsetAsync(L.queue, 0, sizeof(int), st);
+            const unsigned g = (unsigned)(L.tile_blocks < L.nitems ? L.tile_blocks : L.nitems);
+            if (which == KER_TILE_CANON) kb_tile<S, 0><<<g, 256, batch_tile_smem<S>(), st>>>(L, q, step, flags);
+            else kb_tile<S, 1><<<g, 256, batch_tile_smem<S>(), st>>>(L, q, step, flags);
+            LAUNCHED(1);
+        } break;
+        default: break;
+    }
+}
+void launch_batch_kernel(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
+                         cudaStream_t st) {
+    switch (storage) {
+        case LBM_STORE_F16S: launch_batch_kernel_s<LBM_STORE_F16S>(which, L, q, step, flags, st); break;
+        case LBM_STORE_BF16S: launch_batch_kernel_s<LBM_STORE_BF16S>(which, L, q, step, flags, st); break;
+        default: launch_batch_kernel_s<LBM_STORE_F32>(which, L, q, step, flags, st); break;
+    }
+}
+
 void launch_diagnostics(const DiagArgs &G, cudaStream_t st) {
     k_diag_cells<<<G.ncellp, DIAG_THREADS, 0, st>>>(G); LAUNCHED(1);
     if (G.fs) {

@@ -3,8 +3,9 @@
 // Same physics as ArExact (macro_step, compute_LES without the wall model,
 // collide_regularized / collide_KBC of CODEX.py:2943-3416 for a plain
 // interior air cell), reorganised for fewer instructions; compiled in its
-// own translation unit with multiply-add contraction.  Results differ from
-// the reference's operation order by rounding only.
+// own translation unit with multiply-add contraction (reciprocals and square
+// roots stay correctly rounded).  Results differ from the reference's
+// operation order by rounding only.
 //
 // Pair form.  D3Q19 velocities come in nine opposite pairs (q, q') with
 // c_q' = -c_q and equal weights.  For a pair,
@@ -71,7 +72,7 @@ struct ArFast {
         const float jx = (d1 + d7) + (d11 - d8) - d12;
         const float jy = (d3 + d7) + (d8 + d15) - d16;
         const float jz = (d5 + d11) + (d12 + d15) + d16;
-        const float inv = __fdividef(1.0f, r);
+        const float inv = 1.0f / r;
         vx = jx * inv;
         vy = jy * inv;
         vz = jz * inv;
@@ -89,10 +90,10 @@ struct ArFast {
         const float diag = axx * axx + ayy * ayy + azz * azz;
         const float off = bxy * bxy + bxz * bxz + byz * byz;
         const float x = 0.5f * diag + 0.25f * off + 1e-6f;   // 2 S:S + 1e-6
-        const float smag = x * rsqrtf(x);
+        const float smag = sqrtf(x);
         const float nu_t = fminf(P.cs_delta_sq * smag, P.nu_t_max);
         const float tau = fminf(0.5f + 3.0f * (P.nu0 + nu_t), 2.0f);
-        return __fdividef(1.0f, tau);
+        return 1.0f / tau;
     }
 
     static LBM_DEV void collide(const StepArgs &A, int c, int k, float r, float vx, float vy, float vz, float om,
@@ -136,7 +137,7 @@ struct ArFast {
             h[3] = exy + 2.0f * Pxy; h[4] = exy - 2.0f * Pxy;
             h[5] = exz + 2.0f * Pxz; h[6] = exz - 2.0f * Pxz;
             h[7] = eyz + 2.0f * Pyz; h[8] = eyz - 2.0f * Pyz;
-            const float omc = (1.0f - om) * 4.5f;
+            const float omc = (1.0f - om) * LBM_INV_2CS4;   // the reference's f32 value of 1 / (2 cs^4)
             const float g1 = omc * (1.0f / 18.0f), g2 = omc * (1.0f / 36.0f);
             f[0] = A0 - (omc * (1.0f / 3.0f)) * t3;
             fe[0] = A0;

@@ -188,4 +188,36 @@ constexpr int DIAG_SLICE_THREADS = 128;   // 128 slice partials of 208 bytes fit
 
 void launch_diagnostics(const DiagArgs &G, cudaStream_t st);
 
+// ---- ensembles stepped with one launch per phase (lbm_batch.cuh)
+// One domain's 2-D bed state for the bed step of one parity.
+struct BatchBed {
+    lbm_params P;
+    Dom D;
+    const float *h_prev, *piecewise;
+    float *h, *hmax, *uw, *vw, *ww;
+    float *cg;                       // column cache of the slot (null without one)
+};
+struct BatchLaunch {
+    const StepArgs *tab;             // [2][ndom] step arguments by the step's index in the call, mod 2
+    const BatchBed *bed;             // [2][ndom] by the parity of the bed step
+    const long long *col0;           // [ndom + 1] first column of each domain in the concatenation
+    int ndom;
+    long long ncols;
+    const int4 *gmap;                // general-kernel blocks: (domain, bx, by, bz)
+    int ngen;
+    const int4 *smap;                // interior stream blocks: (domain, bx, by, bz)
+    int nsi;
+    const int4 *items;               // interior work items: (domain, tile x, tile y, z chunk)
+    int nitems;
+    int *queue;                      // next work item of the interior grid
+    int tile_blocks;                 // resident blocks of the interior grid
+};
+// bed, 3x3 maximum and column cache of every domain at step m
+void launch_batch_bed(const BatchLaunch &L, long long m, cudaStream_t st);
+// one phase for every domain (which = KER_PREPASS_*, KER_TILE_*, KER_COLLIDE_*, KER_STREAM, KER_STREAM_INTERIOR)
+void launch_batch_kernel(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
+                         cudaStream_t st);
+// resident blocks of the interior grid on this device (0: the shared memory is refused)
+int batch_tile_blocks(int storage);
+
 }  // namespace lbm

@@ -262,7 +262,7 @@ LBM_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "me
 LBM_DEV void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <int IN, bool LES, class Ar = ArExact>
-LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by) {
+LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by, int bz) {
     float *sf = smem;                                   // [slot][q][256] own-cell populations
     float *sr = smem + PIPE_SLOTS * 19 * 256;           // [slot][q][64] ring populations
     float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =        // [plane slot][component][x][y]
@@ -271,7 +271,7 @@ LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by) {
     const Dom &D = A.D;
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
     const int i = bx * LBM_TILE + tx, j = by * LBM_TILE + ty;
-    const int z0 = A.zi0 + blockIdx.z * A.chunk;
+    const int z0 = A.zi0 + bz * A.chunk;
     const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
     const int n = (int)D.n, nxy = D.nx * D.ny;
     const float *fsrc = (const float *)A.fsrc;
@@ -430,7 +430,7 @@ LBM_DEV void tile_pipe_body(const StepArgs &A, float *smem, int bx, int by) {
 template <int IN, bool LES>
 __global__ void __launch_bounds__(256, 2) k_tile_pipe(StepArgs A) {
     extern __shared__ __align__(16) float smem[];
-    tile_pipe_body<IN, LES>(A, smem, blockIdx.x, blockIdx.y);
+    tile_pipe_body<IN, LES>(A, smem, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------- pipelined 16-bit interior kernel
@@ -456,7 +456,7 @@ LBM_DEV void cp_async4v(void *smem, const void *gmem) {
 LBM_DEV int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
 template <int S, int IN, bool LES, class Ar = ArExact>
-LBM_DEV void tile_pipe16_body(const StepArgs &A, float *smem, int bx, int by) {
+LBM_DEV void tile_pipe16_body(const StepArgs &A, float *smem, int bx, int by, int bz) {
     typedef typename Store<S>::T T;
     uint32_t *sw = (uint32_t *)smem;                     // [slot][P16_MAIN] words
     uint32_t *rw = sw + PIPE_SLOTS * P16_MAIN;           // [slot][P16_RING] words
@@ -467,7 +467,7 @@ LBM_DEV void tile_pipe16_body(const StepArgs &A, float *smem, int bx, int by) {
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
     const int x0 = bx * LBM_TILE, y0 = by * LBM_TILE;
     const int i = x0 + tx, j = y0 + ty;
-    const int z0 = A.zi0 + blockIdx.z * A.chunk;
+    const int z0 = A.zi0 + bz * A.chunk;
     const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
     const int n = (int)D.n, nxy = D.nx * D.ny;
     const T *fsrc = (const T *)A.fsrc;
@@ -635,7 +635,7 @@ LBM_DEV void tile_pipe16_body(const StepArgs &A, float *smem, int bx, int by) {
 template <int S, int IN, bool LES>
 __global__ void __launch_bounds__(256, 2) k_tile_pipe16(StepArgs A) {
     extern __shared__ __align__(16) float smem[];
-    tile_pipe16_body<S, IN, LES>(A, smem, blockIdx.x, blockIdx.y);
+    tile_pipe16_body<S, IN, LES>(A, smem, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------ TMA-staged interior kernel
@@ -940,8 +940,8 @@ __global__ void __launch_bounds__(256, 2) k_tile_edges(StepArgs A) {
     asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     int bx = 0, by = 0;
     edge_tile(blockIdx.x, A.D.nx / LBM_TILE, A.D.ny / LBM_TILE, bx, by);
-    if constexpr (S == LBM_STORE_F32) tile_pipe_body<1, true, Ar>(A, smem, bx, by);
-    else tile_pipe16_body<S, 1, true, Ar>(A, smem, bx, by);
+    if constexpr (S == LBM_STORE_F32) tile_pipe_body<1, true, Ar>(A, smem, bx, by, blockIdx.z);
+    else tile_pipe16_body<S, 1, true, Ar>(A, smem, bx, by, blockIdx.z);
 }
 
 // ----------------------------------------------- launch of the fused interior
@@ -1005,10 +1005,10 @@ static bool launch_tile_tma_t(const StepArgs &A, const CUtensorMap *m24, const C
 
 // stream only (the last pass of a call) for interior cells
 template <int S>
-__global__ void __launch_bounds__(256) k_stream_interior(StepArgs A) {
+LBM_DEV void stream_interior_body(const StepArgs &A, int bx, int by, int bz) {
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-    const int i = blockIdx.x * LBM_TILE + tx, j = blockIdx.y * LBM_TILE + ty;
-    const int k = A.zi0 + blockIdx.z;
+    const int i = bx * LBM_TILE + tx, j = by * LBM_TILE + ty;
+    const int k = A.zi0 + bz;
     if (k > A.zi1) return;
     const int c = A.D.cell(k, j, i);
     check_far(A, true, k, j, i);
@@ -1017,6 +1017,10 @@ __global__ void __launch_bounds__(256) k_stream_interior(StepArgs A) {
     typename Store<S>::T *dst = (typename Store<S>::T *)A.fdst;
 #pragma unroll
     for (int q = 0; q < 19; ++q) Store<S>::st(dst, (size_t)q * A.D.n + (size_t)c, f[q], q, A.P.rho0);
+}
+template <int S>
+__global__ void __launch_bounds__(256) k_stream_interior(StepArgs A) {
+    stream_interior_body<S>(A, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 }  // namespace lbm

@@ -303,6 +303,14 @@ def declare(lib: C.CDLL) -> C.CDLL:
     lib.lbm_set_tile_chunk.argtypes = [vp, C.c_int32]
     lib.lbm_set_step_graphs.restype = C.c_int
     lib.lbm_set_step_graphs.argtypes = [vp, C.c_int32]
+    lib.lbm_batch_create.restype = C.c_int
+    lib.lbm_batch_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]
+    lib.lbm_batch_step.restype = C.c_int
+    lib.lbm_batch_step.argtypes = [vp, C.c_int32, vp]
+    lib.lbm_batch_destroy.restype = C.c_int
+    lib.lbm_batch_destroy.argtypes = [vp]
+    lib.lbm_batch_last_error.restype = C.c_char_p
+    lib.lbm_batch_last_error.argtypes = [vp]
     lib.lbm_diagnostics.restype = C.c_int
     lib.lbm_diagnostics.argtypes = [vp, C.POINTER(LbmDiagInputs), C.POINTER(LbmDiag), vp]
     lib.lbm_set_arithmetic.restype = C.c_int
@@ -320,6 +328,7 @@ ABI_SYMBOLS = (
     "lbm_init_fields", "lbm_step", "lbm_export_diagnostics", "lbm_read_counters", "lbm_destroy", "lbm_last_error",
     "lbm_set_kernel_timing", "lbm_kernel_timing", "lbm_launch_count", "lbm_link_geometry_noalloc",
     "lbm_set_tile_chunk", "lbm_set_step_graphs", "lbm_set_arithmetic", "lbm_get_arithmetic", "lbm_diagnostics",
+    "lbm_batch_create", "lbm_batch_step", "lbm_batch_destroy", "lbm_batch_last_error",
 )
 
 

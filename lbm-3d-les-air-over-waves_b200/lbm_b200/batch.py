@@ -102,13 +102,24 @@ def domain_bytes(cfg, with_diag: bool = False) -> int:
 
 
 class Batch:
-    """Domains stepped together, each on its own stream.  With graphs (the
-    default) each air domain's step calls run as CUDA graph replays
-    (lbm_set_step_graphs): after the first eager call, one graph per call
-    shape is captured, then a call costs two launches instead of about
-    seven per step."""
+    """Domains stepped together.
 
-    def __init__(self, envs, device="cuda:0", chunk: int = 25, graphs: bool = True):
+    queue=True (air ensembles): one launch per phase of the step for all
+    domains (lbm_batch_*): the interior planes of every domain form one work
+    queue of (domain, tile, z chunk) items taken by a grid of resident
+    blocks; the planes next to the bed and the top, the bed and the final
+    stream are single grids over all domains.  Steps run on the batch's own
+    stream; results equal stepping each domain alone, bit for bit.
+
+    queue=False: each domain on its own stream, its calls interleaved so that
+    kernels of different domains overlap.  With graphs (the default) each air
+    domain's step calls run as CUDA graph replays (lbm_set_step_graphs):
+    after the first eager call, one graph per call shape is captured, then a
+    call costs two launches instead of about seven per step."""
+
+    def __init__(self, envs, device="cuda:0", chunk: int = 25, graphs: bool = True, queue: bool = False):
+        import ctypes as C
+
         import torch
 
         from .domain import Domain
@@ -117,12 +128,29 @@ class Batch:
         self.chunk = int(chunk)
         self.domains = [Domain(env, device=self.device, stream=torch.cuda.Stream(self.device), with_diag=False)
                         for env in envs]
+        self.graphs = graphs
         if graphs:
             for d in self.domains:
                 if d.cfg.physics_mode == "air":
                     d.set_step_graphs(True)
+        self.handle = None
+        self.stream = None
+        if queue:
+            lib = self.domains[0].lib
+            self.stream = torch.cuda.Stream(self.device)
+            ctxs = (C.c_void_p * len(self.domains))(*[d.ctx.value for d in self.domains])
+            h = C.c_void_p()
+            status = lib.lbm_batch_create(ctxs, len(self.domains), C.byref(h))
+            if status != 0:
+                why = [lib.lbm_last_error(d.ctx).decode() for d in self.domains if lib.lbm_last_error(d.ctx)]
+                raise RuntimeError(f"lbm_batch_create failed ({status}): {why[0] if why else ''}")
+            self.handle = h
 
-    mode = "one stream and one step graph per domain"
+    @property
+    def mode(self) -> str:
+        if self.handle is not None:
+            return "one launch per phase over all domains (interior planes as one work queue)"
+        return "one stream and one step graph per domain" if self.graphs else "one stream per domain"
 
     @property
     def cells(self) -> int:
@@ -130,9 +158,33 @@ class Batch:
 
     def streams(self) -> list:
         """The CUDA streams the ensemble's work runs on."""
+        if self.handle is not None:
+            return [self.stream]
         return [d.stream for d in self.domains]
 
     def step(self, n: int):
+        import ctypes as C
+
+        if self.handle is not None:
+            lib = self.domains[0].lib
+            for d in self.domains:          # after work the domains queued on their own streams
+                self.stream.wait_stream(d.stream)
+            status = lib.lbm_batch_step(self.handle, int(n), C.c_void_p(self.stream.cuda_stream))
+            if status != 0:
+                raise RuntimeError(f"lbm_batch_step failed ({status}): {lib.lbm_batch_last_error(self.handle).decode()}")
+            return
+        done = 0
+        while done < n:
+            k = min(self.chunk, n - done)
+            for d in self.domains:
+                d.step(k)
+            done += k
+
+    def step_each(self, n: int):
+        """Advance every domain with its own calls (graphs where enabled),
+        even in queue mode."""
+        if self.handle is not None:
+            self.stream.synchronize()
         done = 0
         while done < n:
             k = min(self.chunk, n - done)
@@ -141,10 +193,16 @@ class Batch:
             done += k
 
     def synchronize(self):
+        if self.stream is not None:
+            self.stream.synchronize()
         for d in self.domains:
             d.synchronize()
 
     def close(self):
+        if self.handle is not None:
+            self.stream.synchronize()
+            self.domains[0].lib.lbm_batch_destroy(self.handle)
+            self.handle = None
         for d in self.domains:
             d.close()
         self.domains = []

@@ -34,8 +34,12 @@ class Domain:
         self.lib = native.load()
         self.stream = stream if stream is not None else torch.cuda.Stream(self.device)
         self.params = abi.make_params(cfg)
-        self.arrays = state.allocate_torch(cfg, self.device, with_diag=with_diag)
-        self.arrays["piecewise_bed_z"].copy_(torch.as_tensor(np.asarray(cfg.piecewise_bed_z_np, dtype=np.float32)))
+        # buffers belong to the domain's stream (allocation, fills, every library call)
+        with torch.cuda.stream(self.stream):
+            self.arrays = state.allocate_torch(cfg, self.device, with_diag=with_diag)
+            self.arrays["piecewise_bed_z"].copy_(
+                torch.as_tensor(np.asarray(cfg.piecewise_bed_z_np, dtype=np.float32)).to(self.device))
+        self.stream.synchronize()
         self.ctx = C.c_void_p()
         self._check(self.lib.lbm_create(C.byref(self.params), C.byref(self.ctx)), "lbm_create")
         self.bufs = state.make_buffers(self.arrays)
@@ -59,24 +63,26 @@ class Domain:
         prepare_initial_density_field restatement with a free surface."""
         import torch
 
-        torch.cuda.synchronize(self.device)
-        self._check(self.lib.lbm_init_geometry(self.ctx, self._sp()), "lbm_init_geometry")
+        # everything on the domain's own stream: no device-wide synchronisation,
+        # so domains can be set up while others step
         self.stream.synchronize()
+        self._check(self.lib.lbm_init_geometry(self.ctx, self._sp()), "lbm_init_geometry")
         a = self.arrays
-        if noise is None:
-            # seeded uniform [-1, 1) draws made on the device
-            g = torch.Generator(device=self.device)
-            g.manual_seed(int(self.cfg.random_seed))
-            a["init_noise"].copy_(torch.rand(a["init_noise"].shape, generator=g, device=self.device) * 2.0 - 1.0)
-        else:
-            a["init_noise"].copy_(torch.as_tensor(np.ascontiguousarray(noise)))
-        if rho_initial is None and self.cfg.water_free_surface_enabled != 1:
-            a["rho_initial"].fill_(float(np.float32(self.cfg.rho0)))
-        else:
-            if rho_initial is None:
-                rho_initial = prepare_initial_density(self.cfg, a["fs_h"].cpu().numpy(), a["water_h"].cpu().numpy())
-            a["rho_initial"].copy_(torch.as_tensor(np.ascontiguousarray(rho_initial)))
-        torch.cuda.synchronize(self.device)
+        with torch.cuda.stream(self.stream):
+            if noise is None:
+                # seeded uniform [-1, 1) draws made on the device
+                g = torch.Generator(device=self.device)
+                g.manual_seed(int(self.cfg.random_seed))
+                a["init_noise"].copy_(torch.rand(a["init_noise"].shape, generator=g, device=self.device) * 2.0 - 1.0)
+            else:
+                a["init_noise"].copy_(torch.as_tensor(np.ascontiguousarray(noise)).to(self.device))
+            if rho_initial is None and self.cfg.water_free_surface_enabled != 1:
+                a["rho_initial"].fill_(float(np.float32(self.cfg.rho0)))
+            else:
+                if rho_initial is None:
+                    rho_initial = prepare_initial_density(self.cfg, a["fs_h"].cpu().numpy(),
+                                                          a["water_h"].cpu().numpy())
+                a["rho_initial"].copy_(torch.as_tensor(np.ascontiguousarray(rho_initial)).to(self.device))
         self._check(self.lib.lbm_init_fields(self.ctx, self._sp()), "lbm_init_fields")
         self.stream.synchronize()
 

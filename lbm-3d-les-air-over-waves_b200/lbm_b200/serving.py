@@ -3,12 +3,13 @@
 A request is a solve: a configuration (LBM_* options) and a number of
 steps.  The server admits requests in arrival order while their device
 memory fits the HBM budget, keeps every admitted solve's populations
-resident, and advances all active solves together in rounds of `chunk`
-steps, each solve on its own CUDA stream so that their kernels overlap on
-the device.  Requests that arrive while others run are admitted at the next
-round boundary as soon as memory frees up; a finished solve returns its
-result (the final velocity and density fields on the host) and releases its
-memory.  Latency is completion minus arrival, in wall-clock seconds.
+resident, and advances all active solves concurrently, each on its own CUDA
+stream with a few calls of `chunk` steps queued, so that their kernels
+overlap on the device.  Requests that arrive while others run are admitted
+as soon as memory frees up and are set up on a worker thread while the GPU
+keeps stepping the others; a finished solve returns its result (the final
+velocity and density fields on the host) and releases its memory.  Latency
+is completion minus arrival, in wall-clock seconds.
 
     reqs = poisson_trace(24, rate_hz=20, seed=3)
     report = Server(budget_bytes=150e9).run(reqs)
@@ -72,11 +73,23 @@ def poisson_trace(n: int, rate_hz: float = 20.0, seed: int = 3, cells_range=(1e5
 
 
 class Server:
+    """Continuous batching of solves on one GPU.
+
+    Admission runs in arrival order while the requests' device memory fits
+    the budget; a solve is built (buffers, initial state) on a worker thread,
+    so setting it up overlaps the steps of the solves already on the GPU.
+    Every active solve keeps `depth` calls of `chunk` steps queued on its own
+    stream; a CUDA event per call tells the host loop when to queue the next
+    one, so no step of the loop waits for the whole device.  A finished
+    solve's result (density and velocity) is copied to pinned host memory on
+    its stream, and the request completes when that copy has landed."""
+
     def __init__(self, device="cuda:0", budget_bytes: float = 150e9, chunk: int = 50, domain_factory=None,
-                 clock=time.perf_counter):
+                 clock=time.perf_counter, depth: int = 2):
         self.device = device
         self.budget = float(budget_bytes)
         self.chunk = int(chunk)
+        self.depth = max(1, int(depth))
         self.clock = clock
         self._factory = domain_factory
 
@@ -90,73 +103,136 @@ class Server:
 
         dom = Domain(env, device=self.device, stream=torch.cuda.Stream(torch.device(self.device)), with_diag=False)
         if dom.cfg.physics_mode == "air":
-            dom.set_step_graphs(True)   # rounds of `chunk` steps replay one captured graph per call shape
+            dom.set_step_graphs(True)   # calls of `chunk` steps replay one captured graph per call shape
         return dom
 
+    def _build(self, env):
+        t = time.perf_counter()
+        dom = self._make_domain(env)
+        return dom, time.perf_counter() - t
+
     @staticmethod
-    def _result(dom) -> dict:
-        if hasattr(dom, "field"):
-            return {k: dom.field(k).detach().cpu().numpy() for k in ("rho", "ux", "uy", "uz")}
-        return dom.result()
+    def _issue(dom, k):
+        """Queue k steps; returns an event that completes with them (None for
+        stand-in domains without a stream)."""
+        dom.step(k)
+        stream = getattr(dom, "stream", None)
+        if stream is None:
+            return None
+        import torch
+
+        ev = torch.cuda.Event()
+        ev.record(stream)
+        return ev
+
+    @staticmethod
+    def _done(ev) -> bool:
+        return ev is None or ev.query()
+
+    @staticmethod
+    def _start_result(dom):
+        """Queue the result's copy to the host: (host arrays, completion event)."""
+        if not hasattr(dom, "field"):
+            return dom.result(), None
+        import torch
+
+        host = {}
+        with torch.cuda.stream(dom.stream):
+            for k in ("rho", "ux", "uy", "uz"):
+                src = dom.field(k)
+                dst = torch.empty(src.shape, dtype=src.dtype, pin_memory=True)
+                dst.copy_(src, non_blocking=True)
+                host[k] = dst
+            ev = torch.cuda.Event()
+            ev.record(dom.stream)
+        return host, ev
 
     def run(self, requests, idle_sleep_s: float = 0.0005) -> dict:
-        pending = sorted(requests, key=lambda q: (q.arrival_s, q.rid))
+        from collections import deque
+        from concurrent.futures import ThreadPoolExecutor
+
+        pending = deque(sorted(requests, key=lambda q: (q.arrival_s, q.rid)))
         need = {q.rid: domain_bytes(load_config(q.env)) for q in pending}
         for q in pending:
             if need[q.rid] > self.budget:
                 raise ValueError(f"request {q.rid} needs {need[q.rid] / 1e9:.1f} GB, over the budget")
-        active = []          # [request, domain, remaining steps]
+        building = deque()   # (request, future) in admission order
+        active = []          # {"q", "dom", "rem", "ev": deque of events}
+        finishing = []       # (request, domain, host result, event)
         used = 0.0
         finished = []
         lups = 0
-        t0 = self.clock()
-        rounds = 0
+        chunks = 0
         peak_active = 0
         setup_s = 0.0
-        while pending or active:
-            now = self.clock() - t0
-            # admission in arrival order, by HBM budget
-            while pending and pending[0].arrival_s <= now and used + need[pending[0].rid] <= self.budget:
-                q = pending.pop(0)
-                ts = self.clock()
-                dom = self._make_domain(q.env)
-                q.admitted_s = self.clock() - t0
-                setup_s += self.clock() - ts
-                used += need[q.rid]
-                active.append([q, dom, q.steps])
-            if not active:
-                if pending:
-                    wait = pending[0].arrival_s - (self.clock() - t0)
-                    if wait > 0:
-                        time.sleep(min(wait, 0.01) if idle_sleep_s else 0)
-                continue
-            peak_active = max(peak_active, len(active))
-            # one round: every active solve advances up to `chunk` steps
-            for item in active:
-                k = min(self.chunk, item[2])
-                item[1].step(k)
-                item[2] -= k
-            for item in active:
-                item[1].synchronize()
-            rounds += 1
-            still = []
-            for item in active:
-                q, dom, rem = item
-                if rem > 0:
-                    still.append(item)
-                    continue
-                q.result = self._result(dom)
-                q.done_s = self.clock() - t0
-                cfg = dom.cfg
-                lups += cfg.Nx * cfg.Ny * cfg.Nz * q.steps
-                dom.close()
-                used -= need[q.rid]
-                finished.append(q)
-            active = still
+        pool = ThreadPoolExecutor(max_workers=1)
+        t0 = self.clock()
+        try:
+            while pending or building or active or finishing:
+                progress = False
+                now = self.clock() - t0
+                # admission in arrival order, by HBM budget
+                while pending and pending[0].arrival_s <= now and used + need[pending[0].rid] <= self.budget:
+                    q = pending.popleft()
+                    q.admitted_s = self.clock() - t0
+                    used += need[q.rid]
+                    building.append((q, pool.submit(self._build, q.env)))
+                    progress = True
+                # solves whose set-up finished join the active set, in admission order
+                while building and building[0][1].done():
+                    q, fut = building.popleft()
+                    dom, build_s = fut.result()
+                    setup_s += build_s
+                    active.append({"q": q, "dom": dom, "rem": q.steps, "ev": deque()})
+                    progress = True
+                peak_active = max(peak_active, len(active))
+                # keep `depth` calls queued per solve
+                still = []
+                for it in active:
+                    while it["ev"] and self._done(it["ev"][0]):
+                        it["ev"].popleft()
+                    while it["rem"] > 0 and len(it["ev"]) < self.depth:
+                        k = min(self.chunk, it["rem"])
+                        it["ev"].append(self._issue(it["dom"], k))
+                        it["rem"] -= k
+                        chunks += 1
+                        progress = True
+                    if it["rem"] == 0 and not it["ev"]:
+                        host, ev = self._start_result(it["dom"])
+                        finishing.append((it["q"], it["dom"], host, ev))
+                        progress = True
+                    else:
+                        still.append(it)
+                active = still
+                # results on the host: the request is complete, its memory is released
+                rest = []
+                for q, dom, host, ev in finishing:
+                    if not self._done(ev):
+                        rest.append((q, dom, host, ev))
+                        continue
+                    q.result = {k: (v.numpy() if hasattr(v, "numpy") else v) for k, v in host.items()} \
+                        if isinstance(host, dict) else host
+                    q.done_s = self.clock() - t0
+                    cfg = dom.cfg
+                    lups += cfg.Nx * cfg.Ny * cfg.Nz * q.steps
+                    dom.close()
+                    used -= need[q.rid]
+                    finished.append(q)
+                    progress = True
+                finishing = rest
+                if not progress:
+                    if pending and not (building or active or finishing):
+                        wait = pending[0].arrival_s - (self.clock() - t0)
+                        if wait > 0 and idle_sleep_s:
+                            time.sleep(min(wait, 0.01))
+                    elif idle_sleep_s:
+                        time.sleep(idle_sleep_s)
+        finally:
+            pool.shutdown(wait=True)
         wall = self.clock() - t0
         lat = np.array([q.latency_s for q in finished]) if finished else np.zeros(1)
         return {
             "requests": len(finished), "wall_s": wall, "mlups": lups / wall / 1e6 if wall > 0 else 0.0,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "rounds": rounds, "peak_active": peak_active, "setup_s": setup_s, "finished": finished,
+            "rounds": chunks, "peak_active": peak_active, "setup_s": setup_s, "finished": finished,
         }

@@ -758,6 +758,13 @@ int lbm_set_tile_chunk(lbm_ctx *ctx, int32_t planes) {
     return (ctx && planes >= 0) ? LBM_OK : LBM_ERR_BAD_ARG;
 }
 int lbm_set_step_graphs(lbm_ctx *ctx, int32_t) { return ctx ? LBM_OK : LBM_ERR_BAD_ARG; }
+int lbm_batch_create(lbm_ctx *const *, int32_t, lbm_batch **out) {
+    if (out) *out = nullptr;
+    return LBM_ERR_UNSUPPORTED;   // ensembles are a device-side feature
+}
+int lbm_batch_step(lbm_batch *, int32_t, void *) { return LBM_ERR_UNSUPPORTED; }
+int lbm_batch_destroy(lbm_batch *) { return LBM_ERR_BAD_ARG; }
+const char *lbm_batch_last_error(lbm_batch *) { return "the CPU oracle has no ensembles"; }
 int lbm_diagnostics(lbm_ctx *ctx, const lbm_diag_inputs *in, lbm_diag *out, void *) {
     if (!ctx || !in || !out) return LBM_ERR_BAD_ARG;
     return LBM_ERR_UNSUPPORTED;   // device reductions only; the oracle's fields are on the host

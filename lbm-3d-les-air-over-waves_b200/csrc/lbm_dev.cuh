@@ -100,7 +100,14 @@ LBM_DEV int pymod(int a, int n) {
 
 // ------------------------------------------------------- population storage
 // F32: plain.  F16S / BF16S: shifted populations f - w_q*rho0 stored in 16
-// bits, arithmetic in f32.
+// bits, arithmetic in f32.  FP16 stores the shifted value times 2^8: the
+// shifted values of slow or nearly hydrostatic flow (w_q (rho - rho0) of
+// order 1e-5) would otherwise fall below FP16's normal range (6.1e-5) and
+// lose relative precision; scaling by a power of two is exact both ways and
+// still leaves |f - w_q rho0| up to 255 representable.  BF16 has FP32's
+// exponent range and is stored unscaled.
+#define LBM_F16_SCALE 256.0f
+#define LBM_F16_UNSCALE 0.00390625f
 template <int S> struct Store;
 template <> struct Store<LBM_STORE_F32> {
     typedef float T;
@@ -111,13 +118,13 @@ template <> struct Store<LBM_STORE_F32> {
 template <> struct Store<LBM_STORE_F16S> {
     typedef __half T;
     static LBM_DEV float ld(const __half *p, size_t i, int q, float rho0) {
-        return __half2float(__ldg(p + i)) + wq(q) * rho0;
+        return __half2float(__ldg(p + i)) * LBM_F16_UNSCALE + wq(q) * rho0;
     }
     static LBM_DEV float ld_rw(const __half *p, size_t i, int q, float rho0) {
-        return __half2float(p[i]) + wq(q) * rho0;
+        return __half2float(p[i]) * LBM_F16_UNSCALE + wq(q) * rho0;
     }
     static LBM_DEV void st(__half *p, size_t i, float v, int q, float rho0) {
-        p[i] = __float2half_rn(v - wq(q) * rho0);
+        p[i] = __float2half_rn((v - wq(q) * rho0) * LBM_F16_SCALE);
     }
 };
 template <> struct Store<LBM_STORE_BF16S> {

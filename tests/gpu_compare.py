@@ -32,7 +32,10 @@ def populations(dom):
     if f.dtype == torch.float32:
         return f.detach().cpu().numpy()
     w = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, dtype=np.float32)
-    return f.detach().float().cpu().numpy() + (w * np.float32(dom.cfg.rho0))[:, None, None, None]
+    v = f.detach().float().cpu().numpy()
+    if f.dtype == torch.float16:
+        v = v * np.float32(1.0 / 256.0)   # FP16 holds the shifted value times 2^8
+    return v + (w * np.float32(dom.cfg.rho0))[:, None, None, None]
 
 
 def compare_states(dom, ref: OracleSim, tag: str, diag: bool = True, exact: bool = True, rtol=0.0, atol=0.0):

@@ -454,7 +454,7 @@ def run_batched(domains: int, K: int, W: int, storage: str, graphs: bool = True)
     from lbm_b200.batch import Batch, stable_ensemble_envs
 
     envs = stable_ensemble_envs(domains, seed=7, storage=storage)
-    b = Batch(envs, chunk=25, graphs=graphs, queue=True)
+    b = Batch(envs, chunk=25, graphs=graphs, queue=True, arith=ARITH)
     W = max(W, 3)
     b.step(W)
     b.synchronize()
@@ -474,7 +474,7 @@ def run_batched(domains: int, K: int, W: int, storage: str, graphs: bool = True)
     out = {
         "value": cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "steps": K, "warmup": W, "ms_per_step": ms / K,
         "domains": len(envs), "cells": cells, "storage": storage, "bytes_per_cell": bytes_cell,
-        "launch": b.mode, "gpu_launches": launches,
+        "launch": b.mode, "arithmetic": ARITH, "gpu_launches": launches,
         "roofline_step_frac": bytes_cell * cells * K / (ms * 1e-3) / (measured_hbm_peak()[0] * 1e9),
         "per_domain_streams": {"value": cells * K / (ms_streams * 1e-3) / 1e6, "ms_per_step": ms_streams / K,
                                "step_graphs": graphs, "warmup": Wd},
@@ -491,11 +491,11 @@ def run_serving(requests: int, min_steps: int, max_steps: int, storage: str) -> 
 
     reqs = poisson_trace(requests, rate_hz=20.0, seed=3, cells_range=(1e5, 2e7),
                          steps_range=(min_steps, max_steps), storage=storage)
-    rep = Server(budget_bytes=150e9, chunk=50).run(reqs)
+    rep = Server(budget_bytes=150e9, chunk=50, arith=ARITH).run(reqs)
     return {
         "value": rep["mlups"], "unit": UNIT, "p50_s": rep["p50_s"], "p99_s": rep["p99_s"], "wall_s": rep["wall_s"],
         "requests": rep["requests"], "rounds": rep["rounds"], "peak_active": rep["peak_active"],
-        "setup_s": rep["setup_s"], "storage": storage, "steps_range": [min_steps, max_steps],
+        "setup_s": rep["setup_s"], "storage": storage, "arithmetic": ARITH, "steps_range": [min_steps, max_steps],
         "workload": f"Poisson(20/s) arrivals, {requests} requests, half air-over-wave, half water Gaussian, cells "
                     f"log-uniform [1e5, 2e7], steps uniform [{min_steps}, {max_steps}], seed 3, HBM budget 150 GB",
     }

@@ -440,10 +440,11 @@ const char *lbm_last_error(lbm_ctx *ctx);
    blocks, so domains of uneven size share the SMs; the planes next to the
    bed and the top, the bed and the final stream run as single grids over
    block maps of all domains.  Results equal those of stepping each context
-   with lbm_step, bit for bit.  Requirements: every context bound and
+   with lbm_step, bit for bit (with fast arithmetic, those of its
+   cp.async-staged tiles).  Requirements: every context bound and
    initialised, air mode with bed-only geometry and periodic x, nx and ny
-   multiples of 16, one population storage, LES on for all or none, all at
-   the same step; else LBM_ERR_UNSUPPORTED (message in lbm_last_error of the
+   multiples of 16, one population storage, one arithmetic
+   (lbm_set_arithmetic), LES on for all or none, all at the same step; else LBM_ERR_UNSUPPORTED (message in lbm_last_error of the
    offending context).  lbm_batch_step advances every context by nsteps on
    stream (the contexts' own calls may be used between batch calls, keeping
    them at one step).  The CPU oracle returns LBM_ERR_UNSUPPORTED. */

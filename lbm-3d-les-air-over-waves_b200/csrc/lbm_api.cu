@@ -1072,6 +1072,7 @@ struct lbm_batch {
     std::vector<Plan> plan;
     std::vector<bool> stash;
     int storage = 0;
+    int arith = LBM_ARITH_EXACT;   // of the interior planes, uniform over the ensemble
     bool les = false;
     BatchLaunch L{};
     StepArgs *d_tab = nullptr, *h_tab = nullptr;
@@ -1126,6 +1127,7 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
         else if (!R.tile || R.classic) why = "the interior-plane path is required (nx, ny multiples of 16)";
         else if (c->P.pop_storage != c0->P.pop_storage) why = "one population storage for the whole ensemble";
         else if ((c->P.use_les != 0) != (c0->P.use_les != 0)) why = "LES on for every domain or for none";
+        else if (c->arith != c0->arith) why = "one arithmetic (lbm_set_arithmetic) for the whole ensemble";
         else if (c->nstep != c0->nstep || c->cur != c0->cur) why = "every domain at the same step";
         if (!why.empty()) {
             delete b;
@@ -1135,6 +1137,7 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
         b->plan.push_back(R);
     }
     b->storage = c0->P.pop_storage;
+    b->arith = c0->arith;
     b->les = c0->P.use_les != 0;
     std::vector<long long> col0(1, 0);
     std::vector<int4> gmap, smap, items;
@@ -1206,7 +1209,7 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
     L.items = b->d_items;
     L.nitems = (int)items.size();
     L.queue = b->d_queue;
-    L.tile_blocks = batch_tile_blocks(b->storage);
+    L.tile_blocks = batch_tile_blocks(b->storage, b->arith);
     if (L.tile_blocks <= 0) {
         batch_free(b);
         delete b;
@@ -1267,7 +1270,7 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
     launch_batch_bed(L, n0 + 1, st);
     int flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
     if (b->les) launch_batch_kernel(KER_PREPASS_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st);
-    launch_batch_kernel(KER_TILE_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st);
+    launch_batch_kernel(KER_TILE_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st, b->arith);
     launch_batch_kernel(KER_COLLIDE_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st);
     // fused steps: stream + boundary conditions of step m, condition ... collide of step m + 1
     for (int s = 1; s < K; ++s) {
@@ -1276,7 +1279,7 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
         flags = ((s == K - 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
         const int q = s & 1;
         if (b->les) launch_batch_kernel(KER_PREPASS_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st);
-        launch_batch_kernel(KER_TILE_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st);
+        launch_batch_kernel(KER_TILE_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st, b->arith);
         launch_batch_kernel(KER_COLLIDE_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st);
     }
     // the final stream back to the post-stream state

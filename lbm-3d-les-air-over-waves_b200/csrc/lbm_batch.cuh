@@ -24,19 +24,9 @@
 // an ensemble steps bit for bit like its domains stepped one by one.
 #pragma once
 
-#include "lbm_tile.cuh"
+#include "lbm_batch_tile.cuh"
 
 namespace lbm {
-
-// copy a domain's step arguments into shared memory (all threads of the block)
-LBM_DEV void batch_load_args(StepArgs &dst, const StepArgs &src) {
-    const int nw = (int)(sizeof(StepArgs) / 4);
-    const unsigned *s = (const unsigned *)&src;
-    unsigned *d = (unsigned *)&dst;
-    const int t = threadIdx.x + threadIdx.y * blockDim.x, nt = blockDim.x * blockDim.y;
-    for (int w = t; w < nw; w += nt) d[w] = s[w];
-}
-static_assert(sizeof(StepArgs) % 4 == 0, "step arguments copy as words");
 
 // domain of concatenated column g: the last d with col0[d] <= g
 LBM_DEV int batch_domain(const long long *col0, int ndom, long long g) {
@@ -107,45 +97,6 @@ __global__ void __launch_bounds__(256) kb_stream_interior(BatchLaunch L, int q, 
     }
     __syncthreads();
     stream_interior_body<S>(sA, m.y, m.z, m.w);
-}
-
-template <int S>
-constexpr int batch_tile_smem() {
-    return S == LBM_STORE_F32 ? PIPE_SMEM_BYTES : P16_SMEM_BYTES;
-}
-
-// the interior planes of every domain as a work queue
-template <int S, int IN>
-__global__ void __launch_bounds__(256, 2) kb_tile(BatchLaunch L, int q, unsigned long long step, int flags) {
-    extern __shared__ __align__(16) float smem[];
-    __shared__ __align__(16) StepArgs sA;
-    __shared__ int s_item;
-    int cur = -1;
-    for (;;) {
-        __syncthreads();   // every thread is done with the last item's shared memory
-        if (threadIdx.x == 0) s_item = atomicAdd(L.queue, 1);
-        __syncthreads();
-        const int item = s_item;
-        if (item >= L.nitems) break;
-        const int4 it = L.items[item];
-        if (it.x != cur) {
-            batch_load_args(sA, L.tab[q * L.ndom + it.x]);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                sA.step = step;
-                sA.flags = flags;
-            }
-            __syncthreads();
-            cur = it.x;
-        }
-        if constexpr (S == LBM_STORE_F32) {
-            if (sA.P.use_les) tile_pipe_body<IN, true>(sA, smem, it.y, it.z, it.w);
-            else tile_pipe_body<IN, false>(sA, smem, it.y, it.z, it.w);
-        } else {
-            if (sA.P.use_les) tile_pipe16_body<S, IN, true>(sA, smem, it.y, it.z, it.w);
-            else tile_pipe16_body<S, IN, false>(sA, smem, it.y, it.z, it.w);
-        }
-    }
 }
 
 }  // namespace lbm

@@ -184,10 +184,13 @@ __global__ void k_colgeo(lbm_params P, Dom D, BedView B, float *cg) {
 }
 
 // ------------------------------------------------------- step kernels
-// resident blocks per SM requested for the general (near-wall) kernels:
-// one, so that their long near-wall paths run without register spills
+// resident blocks per SM requested for the general kernels without the
+// column cache (water, VOF, cube, phi geometry, solid x walls): three, which
+// spills some registers of their long near-wall paths but triples the warps
+// that hide their load latency (water height 256x128x96: 2,251 -> 2,939
+// MLUPS, VOF 128x64x128: 334 -> 444 MLUPS, against one block per SM)
 #ifndef LBM_GEN_MINB
-#define LBM_GEN_MINB 1
+#define LBM_GEN_MINB 3
 #endif
 #ifndef LBM_CG_PRE_MINB
 #define LBM_CG_PRE_MINB 3   // the column-cache pre-pass: 3 blocks of 256 per SM (85 registers)
@@ -1429,36 +1432,12 @@ void launch_batch_bed(const BatchLaunch &L, long long m, cudaStream_t st) {
     kb_colgeo<<<blocks_for((size_t)L.ncols, 128), 128, 0, st>>>(L, par); LAUNCHED(1);
 }
 
-template <int S>
-static bool batch_smem_ready() {
-    static bool done[64] = {false}, ok[64] = {false};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
-    if (!done[dev]) {
-        done[dev] = true;
-        ok[dev] = cudaFuncSetAttribute(kb_tile<S, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       batch_tile_smem<S>()) == cudaSuccess &&
-                  cudaFuncSetAttribute(kb_tile<S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       batch_tile_smem<S>()) == cudaSuccess;
-    }
-    return ok[dev];
-}
-
-template <int S>
-static int batch_tile_blocks_s() {
-    if (!batch_smem_ready<S>()) return 0;
-    int dev = 0, sms = 0, per = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kb_tile<S, 1>, 256, batch_tile_smem<S>()) != cudaSuccess)
-        return 0;
-    return per * sms;
-}
-int batch_tile_blocks(int storage) {
+int batch_tile_blocks(int storage, int arith) {
+    if (arith == LBM_ARITH_FAST) return batch_tile_blocks_fast(storage);
     switch (storage) {
-        case LBM_STORE_F16S: return batch_tile_blocks_s<LBM_STORE_F16S>();
-        case LBM_STORE_BF16S: return batch_tile_blocks_s<LBM_STORE_BF16S>();
-        default: return batch_tile_blocks_s<LBM_STORE_F32>();
+        case LBM_STORE_F16S: return batch_tile_blocks_t<LBM_STORE_F16S, ArExact, ArExact>();
+        case LBM_STORE_BF16S: return batch_tile_blocks_t<LBM_STORE_BF16S, ArExact, ArExact>();
+        default: return batch_tile_blocks_t<LBM_STORE_F32, ArExact, ArExact>();
     }
 }
 
@@ -1476,19 +1455,16 @@ static void launch_batch_kernel_s(int which, const BatchLaunch &L, int q, unsign
             if (L.nsi) { kb_stream_interior<S><<<L.nsi, 256, 0, st>>>(L, q, step, flags); LAUNCHED(1); }
             break;
         case KER_TILE_CANON:
-        case KER_TILE_FUSED: {
-            if (!L.nitems || !L.tile_blocks) break;
-            cudaMemsetAsync(L.queue, 0, sizeof(int), st);
-            const unsigned g = (unsigned)(L.tile_blocks < L.nitems ? L.tile_blocks : L.nitems);
-            if (which == KER_TILE_CANON) kb_tile<S, 0><<<g, 256, batch_tile_smem<S>(), st>>>(L, q, step, flags);
-            else kb_tile<S, 1><<<g, 256, batch_tile_smem<S>(), st>>>(L, q, step, flags);
-            LAUNCHED(1);
-        } break;
+        case KER_TILE_FUSED: launch_batch_tile_t<S, ArExact, ArExact>(which, L, q, step, flags, st); break;
         default: break;
     }
 }
 void launch_batch_kernel(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
-                         cudaStream_t st) {
+                         cudaStream_t st, int arith) {
+    if (arith == LBM_ARITH_FAST && (which == KER_TILE_CANON || which == KER_TILE_FUSED)) {
+        launch_batch_tile_fast(which, storage, L, q, step, flags, st);
+        return;
+    }
     switch (storage) {
         case LBM_STORE_F16S: launch_batch_kernel_s<LBM_STORE_F16S>(which, L, q, step, flags, st); break;
         case LBM_STORE_BF16S: launch_batch_kernel_s<LBM_STORE_BF16S>(which, L, q, step, flags, st); break;

@@ -9,6 +9,7 @@
 #include "lbm_stages.cuh"
 #include "lbm_tile.cuh"
 #include "lbm_fast.cuh"
+#include "lbm_batch_tile.cuh"
 
 namespace lbm {
 
@@ -24,6 +25,26 @@ bool launch_tile_tma_fast(const StepArgs &A, const CUtensorMap *m24, const CUten
         case LBM_STORE_F16S: return launch_fast_s<LBM_STORE_F16S>(A, m24, m20, st);
         case LBM_STORE_BF16S: return launch_fast_s<LBM_STORE_BF16S>(A, m24, m20, st);
         default: return false;
+    }
+}
+
+typedef ArFast<LBM_COLLIDE_KBC> ArFastK;
+typedef ArFast<LBM_COLLIDE_REGULARIZED> ArFastR;
+
+void launch_batch_tile_fast(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
+                            cudaStream_t st) {
+    switch (storage) {
+        case LBM_STORE_F16S: launch_batch_tile_t<LBM_STORE_F16S, ArFastK, ArFastR>(which, L, q, step, flags, st); break;
+        case LBM_STORE_BF16S: launch_batch_tile_t<LBM_STORE_BF16S, ArFastK, ArFastR>(which, L, q, step, flags, st); break;
+        default: launch_batch_tile_t<LBM_STORE_F32, ArFastK, ArFastR>(which, L, q, step, flags, st); break;
+    }
+}
+
+int batch_tile_blocks_fast(int storage) {
+    switch (storage) {
+        case LBM_STORE_F16S: return batch_tile_blocks_t<LBM_STORE_F16S, ArFastK, ArFastR>();
+        case LBM_STORE_BF16S: return batch_tile_blocks_t<LBM_STORE_BF16S, ArFastK, ArFastR>();
+        default: return batch_tile_blocks_t<LBM_STORE_F32, ArFastK, ArFastR>();
     }
 }
 

@@ -214,10 +214,15 @@ struct BatchLaunch {
 };
 // bed, 3x3 maximum and column cache of every domain at step m
 void launch_batch_bed(const BatchLaunch &L, long long m, cudaStream_t st);
-// one phase for every domain (which = KER_PREPASS_*, KER_TILE_*, KER_COLLIDE_*, KER_STREAM, KER_STREAM_INTERIOR)
+// one phase for every domain (which = KER_PREPASS_*, KER_TILE_*, KER_COLLIDE_*, KER_STREAM, KER_STREAM_INTERIOR);
+// arith: the arithmetic policy of the interior planes (LBM_ARITH_*)
 void launch_batch_kernel(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
-                         cudaStream_t st);
+                         cudaStream_t st, int arith = LBM_ARITH_EXACT);
 // resident blocks of the interior grid on this device (0: the shared memory is refused)
-int batch_tile_blocks(int storage);
+int batch_tile_blocks(int storage, int arith = LBM_ARITH_EXACT);
+// the fast-arithmetic interior grid of an ensemble (lbm_fast.cu)
+void launch_batch_tile_fast(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
+                            cudaStream_t st);
+int batch_tile_blocks_fast(int storage);
 
 }  // namespace lbm

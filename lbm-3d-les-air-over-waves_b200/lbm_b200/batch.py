@@ -111,13 +111,17 @@ class Batch:
     stream are single grids over all domains.  Steps run on the batch's own
     stream; results equal stepping each domain alone, bit for bit.
 
+    arith: "exact" or "fast" interior arithmetic for every domain (default:
+    each context's own, from LBM_B200_ARITH).
+
     queue=False: each domain on its own stream, its calls interleaved so that
     kernels of different domains overlap.  With graphs (the default) each air
     domain's step calls run as CUDA graph replays (lbm_set_step_graphs):
     after the first eager call, one graph per call shape is captured, then a
     call costs two launches instead of about seven per step."""
 
-    def __init__(self, envs, device="cuda:0", chunk: int = 25, graphs: bool = True, queue: bool = False):
+    def __init__(self, envs, device="cuda:0", chunk: int = 25, graphs: bool = True, queue: bool = False,
+                 arith: str | None = None):
         import ctypes as C
 
         import torch
@@ -129,6 +133,9 @@ class Batch:
         self.domains = [Domain(env, device=self.device, stream=torch.cuda.Stream(self.device), with_diag=False)
                         for env in envs]
         self.graphs = graphs
+        if arith is not None:
+            for d in self.domains:
+                d.set_arithmetic(arith)   # exact or fast interior arithmetic, before any graph capture
         if graphs:
             for d in self.domains:
                 if d.cfg.physics_mode == "air":

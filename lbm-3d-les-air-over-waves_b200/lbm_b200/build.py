@@ -24,7 +24,7 @@ OUT_DIR = os.path.join(PKG, "_native")
 LIB = os.path.join(OUT_DIR, "liblbm_b200.so")
 SOURCES = ["lbm_api.cu", "lbm_device.cu", "lbm_fast.cu"]
 HEADERS = ["lbm_dev.cuh", "lbm_geom.cuh", "lbm_stages.cuh", "lbm_tile.cuh", "lbm_vof.cuh", "lbm_launch.h",
-           "lbm_fast.cuh"]
+           "lbm_fast.cuh", "lbm_batch.cuh", "lbm_batch_tile.cuh", "lbm_diag.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

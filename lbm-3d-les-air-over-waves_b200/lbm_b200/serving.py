@@ -85,8 +85,9 @@ class Server:
     its stream, and the request completes when that copy has landed."""
 
     def __init__(self, device="cuda:0", budget_bytes: float = 150e9, chunk: int = 50, domain_factory=None,
-                 clock=time.perf_counter, depth: int = 2):
+                 clock=time.perf_counter, depth: int = 2, arith: str | None = None):
         self.device = device
+        self.arith = arith        # "exact" / "fast" interior arithmetic of air solves (None: the library default)
         self.budget = float(budget_bytes)
         self.chunk = int(chunk)
         self.depth = max(1, int(depth))
@@ -103,6 +104,8 @@ class Server:
 
         dom = Domain(env, device=self.device, stream=torch.cuda.Stream(torch.device(self.device)), with_diag=False)
         if dom.cfg.physics_mode == "air":
+            if self.arith is not None:
+                dom.set_arithmetic(self.arith)
             dom.set_step_graphs(True)   # calls of `chunk` steps replay one captured graph per call shape
         return dom
 

@@ -36,7 +36,7 @@ pytestmark = pytest.mark.gpu
 
 VEL_MAX = {"f32": 1e-4, "f16s": 1e-3, "bf16s": 2e-2}
 VEL_RMS = {"f32": 1e-5, "f16s": 5e-4, "bf16s": 5e-3}
-PRESSURE_MAX = {"f32": 1e-4, "f16s": 2e-3, "bf16s": 0.15}
+PRESSURE_MAX = {"f32": 1e-4, "f16s": 1.5e-2, "bf16s": 0.15}
 # water at its own shape after 60 of its 10,000 steps: the flow has barely
 # started (velocities of order g t), and the hydrostatic density steps between
 # cells are a few FP32 ulps of rho, so even the FP32 form is ~1e-2 from FP64 in

@@ -27,6 +27,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1064,22 +1065,38 @@ const char *lbm_last_error(lbm_ctx *ctx) { return ctx ? ctx->err.c_str() : "null
 
 // ------------------------------------------------------------------ ensembles
 // An ensemble of air contexts stepped together with one launch per phase of
-// the step (lbm_batch.cuh).  The tables of block maps and work items are
-// built once; the per-domain step arguments and bed pointers (which depend on
-// the step's parity) are uploaded at the start of each call.
-struct lbm_batch {
-    std::vector<lbm_ctx *> ctx;
-    std::vector<Plan> plan;
-    std::vector<bool> stash;
-    int storage = 0;
-    int arith = LBM_ARITH_EXACT;   // of the interior planes, uniform over the ensemble
-    bool les = false;
-    BatchLaunch L{};
-    StepArgs *d_tab = nullptr, *h_tab = nullptr;
-    BatchBed *d_bed = nullptr, *h_bed = nullptr;
+// the step and group of domains (lbm_batch.cuh).  Domains are ordered by
+// collision model and split into groups of at most BATCH_GROUP; each group has
+// its block maps and work items (built once), a stream and an event, and its
+// steps are issued on that stream, interleaved with the other groups', so the
+// phases of different groups overlap on the device.  The per-domain step
+// arguments travel in each launch's parameters; the bed tables (which depend
+// on the step's parity) are uploaded at the start of each call.
+struct BatchGroupPlan {
+    int d0 = 0, nd = 0;                 // the group's domains: [d0, d0 + nd) of lbm_batch::ctx
+    int collision = LBM_COLLIDE_REGULARIZED;
+    int tile_blocks = 0;
+    BatchLaunch L{};                    // bed phase
     long long *d_col0 = nullptr;
     int4 *d_gmap = nullptr, *d_smap = nullptr, *d_items = nullptr;
+    int ngen = 0, nsi = 0, nitems = 0;
     int *d_queue = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+};
+
+struct lbm_batch {
+    std::vector<lbm_ctx *> ctx;         // grouped order (by collision model, then the caller's order)
+    std::vector<Plan> plan;
+    std::vector<bool> stash;
+    std::vector<BatchGroupPlan> groups;
+    int storage = 0;
+    int arith = LBM_ARITH_EXACT;        // of the interior planes, uniform over the ensemble
+    bool les = false;
+    std::vector<StepArgs> h_tab;        // [2][n] step arguments by the step's index in the call, mod 2
+    BatchBed *d_bed = nullptr, *h_bed = nullptr;
+    std::unique_ptr<BatchGroup> G;      // parameters of the launch being issued
+    cudaEvent_t start = nullptr;
     std::string err;
 };
 
@@ -1089,15 +1106,22 @@ static int batch_fail(lbm_batch *b, int code, const std::string &msg) {
 }
 
 static void batch_free(lbm_batch *b) {
-    cudaFree(b->d_tab);
+    for (BatchGroupPlan &g : b->groups) {
+        cudaFree(g.d_col0);
+        cudaFree(g.d_gmap);
+        cudaFree(g.d_smap);
+        cudaFree(g.d_items);
+        cudaFree(g.d_queue);
+        if (g.done) cudaEventDestroy(g.done);
+        if (g.stream) cudaStreamDestroy(g.stream);
+    }
+    b->groups.clear();
+    if (b->start) cudaEventDestroy(b->start);
+    b->start = nullptr;
     cudaFree(b->d_bed);
-    cudaFree(b->d_col0);
-    cudaFree(b->d_gmap);
-    cudaFree(b->d_smap);
-    cudaFree(b->d_items);
-    cudaFree(b->d_queue);
-    cudaFreeHost(b->h_tab);
     cudaFreeHost(b->h_bed);
+    b->d_bed = nullptr;
+    b->h_bed = nullptr;
 }
 
 template <typename T>
@@ -1107,6 +1131,31 @@ static cudaError_t upload_vec(T **dst, const std::vector<T> &v) {
     return cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
 
+// One phase of one group: the group's step arguments for the step's parity q,
+// with the step number and flags of the launch, into the launch parameters.
+static void batch_issue(lbm_batch *b, const BatchGroupPlan &g, int which, int q, unsigned long long step, int flags) {
+    const int n = (int)b->ctx.size();
+    BatchGroup &G = *b->G;
+    G.ndom = g.nd;
+    for (int d = 0; d < g.nd; ++d) {
+        G.a[d] = b->h_tab[(size_t)q * n + g.d0 + d];
+        G.a[d].step = step;
+        G.a[d].flags = flags;
+    }
+    G.queue = g.d_queue;
+    if (which == KER_TILE_CANON || which == KER_TILE_FUSED) {
+        G.map = g.d_items;
+        G.nmap = g.nitems;
+    } else if (which == KER_STREAM_INTERIOR) {
+        G.map = g.d_smap;
+        G.nmap = g.nsi;
+    } else {
+        G.map = g.d_gmap;
+        G.nmap = g.ngen;
+    }
+    launch_batch_group(which, b->storage, G, b->les, g.collision, b->arith, g.tile_blocks, g.stream);
+}
+
 extern "C" {
 
 int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
@@ -1114,6 +1163,7 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
     *out = nullptr;
     lbm_batch *b = new lbm_batch();
     lbm_ctx *c0 = ctxs[0];
+    std::vector<Plan> plans(n);
     for (int d = 0; d < n; ++d) {
         lbm_ctx *c = ctxs[d];
         if (!c || !c->bound) {
@@ -1133,38 +1183,108 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
             delete b;
             return fail(c, LBM_ERR_UNSUPPORTED, "lbm_batch_create: domain " + std::to_string(d) + ": " + why);
         }
-        b->ctx.push_back(c);
-        b->plan.push_back(R);
+        plans[d] = R;
     }
     b->storage = c0->P.pop_storage;
     b->arith = c0->arith;
     b->les = c0->P.use_les != 0;
-    std::vector<long long> col0(1, 0);
-    std::vector<int4> gmap, smap, items;
-    for (int d = 0; d < n; ++d) {
+    // domains by collision model (regularized, then KBC), each in the caller's order
+    std::vector<int> order(n);
+    for (int d = 0; d < n; ++d) order[d] = d;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return (ctxs[x]->P.collision == LBM_COLLIDE_KBC) < (ctxs[y]->P.collision == LBM_COLLIDE_KBC);
+    });
+    for (int d : order) {
+        b->ctx.push_back(ctxs[d]);
+        b->plan.push_back(plans[d]);
+    }
+    // groups: runs of one collision model, split evenly into at most BATCH_GROUP
+    // domains each (LBM_B200_BATCH_GROUP lowers the bound)
+    int gmax = BATCH_GROUP;
+    if (const char *gv = getenv("LBM_B200_BATCH_GROUP")) {
+        const int v = atoi(gv);
+        if (v >= 1 && v < gmax) gmax = v;
+    }
+    for (int r0 = 0; r0 < n;) {
+        int r1 = r0;
+        while (r1 < n && b->ctx[r1]->P.collision == b->ctx[r0]->P.collision) ++r1;
+        const int len = r1 - r0, ng = (len + gmax - 1) / gmax;
+        for (int k = 0, d = r0; k < ng; ++k) {
+            BatchGroupPlan g;
+            g.d0 = d;
+            g.nd = len / ng + (k < len % ng ? 1 : 0);
+            g.collision = b->ctx[r0]->P.collision;
+            d += g.nd;
+            b->groups.push_back(g);
+        }
+        r0 = r1;
+    }
+    cudaError_t e = cudaSuccess;
+    std::string where;
+    for (BatchGroupPlan &g : b->groups) {
+        std::vector<long long> col0(1, 0);
+        std::vector<int4> gmap, smap, items;
+        std::vector<int> len;
+        for (int ld = 0; ld < g.nd; ++ld) {
+            const int d = g.d0 + ld;
+            lbm_ctx *c = b->ctx[d];
+            const Plan &R = b->plan[d];
+            const int nx = c->P.nx, ny = c->P.ny;
+            col0.push_back(col0.back() + (long long)nx * ny);
+            const int gx = (nx + 31) / 32, gy = (ny + 7) / 8, gz = R.zcnt[0] + R.zcnt[1] + R.zcnt[2];
+            for (int bz = 0; bz < gz; ++bz)
+                for (int by = 0; by < gy; ++by)
+                    for (int bx = 0; bx < gx; ++bx) gmap.push_back(make_int4(ld, bx, by, bz));
+            const int ni = R.zi1 - R.zi0 + 1, tx = nx / LBM_TILE, ty = ny / LBM_TILE;
+            for (int bz = 0; bz < ni; ++bz)
+                for (int by = 0; by < ty; ++by)
+                    for (int bx = 0; bx < tx; ++bx) smap.push_back(make_int4(ld, bx, by, bz));
+            const int nc = (ni + R.chunk - 1) / R.chunk;
+            for (int cz = 0; cz < nc; ++cz)
+                for (int by = 0; by < ty; ++by)
+                    for (int bx = 0; bx < tx; ++bx) items.push_back(make_int4(ld, bx, by, cz));
+        }
+        // longest items first: the last items of the queue are the short ones
+        std::stable_sort(items.begin(), items.end(), [&](const int4 &x, const int4 &y) {
+            const Plan &Rx = b->plan[g.d0 + x.x], &Ry = b->plan[g.d0 + y.x];
+            const int px = std::min(Rx.chunk, Rx.zi1 + 1 - (Rx.zi0 + x.w * Rx.chunk));
+            const int py = std::min(Ry.chunk, Ry.zi1 + 1 - (Ry.zi0 + y.w * Ry.chunk));
+            return px > py;
+        });
+        g.ngen = (int)gmap.size();
+        g.nsi = (int)smap.size();
+        g.nitems = (int)items.size();
+        if ((e = upload_vec(&g.d_col0, col0)) != cudaSuccess || (e = upload_vec(&g.d_gmap, gmap)) != cudaSuccess ||
+            (e = upload_vec(&g.d_smap, smap)) != cudaSuccess || (e = upload_vec(&g.d_items, items)) != cudaSuccess ||
+            (e = cudaMalloc((void **)&g.d_queue, sizeof(int))) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming)) != cudaSuccess) {
+            where = "group tables";
+            break;
+        }
+        g.L.nall = n;
+        g.L.d0 = g.d0;
+        g.L.col0 = g.d_col0;
+        g.L.ndom = g.nd;
+        g.L.ncols = col0.back();
+        g.tile_blocks = batch_tile_blocks(b->storage, b->les, g.collision, b->arith);
+        if (g.tile_blocks <= 0) {
+            batch_free(b);
+            delete b;
+            return fail(c0, LBM_ERR_UNSUPPORTED, "lbm_batch_create: the interior grid's shared memory was refused");
+        }
+    }
+    // 16-bit storage with LES: the general pre-pass hands its FP32 populations to the collide through the stash
+    for (int d = 0; d < n && e == cudaSuccess; ++d) {
         lbm_ctx *c = b->ctx[d];
         const Plan &R = b->plan[d];
-        const int nx = c->P.nx, ny = c->P.ny;
-        col0.push_back(col0.back() + (long long)nx * ny);
-        const int gx = (nx + 31) / 32, gy = (ny + 7) / 8, gz = R.zcnt[0] + R.zcnt[1] + R.zcnt[2];
-        for (int bz = 0; bz < gz; ++bz)
-            for (int by = 0; by < gy; ++by)
-                for (int bx = 0; bx < gx; ++bx) gmap.push_back(make_int4(d, bx, by, bz));
-        const int ni = R.zi1 - R.zi0 + 1, tx = nx / LBM_TILE, ty = ny / LBM_TILE;
-        for (int bz = 0; bz < ni; ++bz)
-            for (int by = 0; by < ty; ++by)
-                for (int bx = 0; bx < tx; ++bx) smap.push_back(make_int4(d, bx, by, bz));
-        const int nc = (ni + R.chunk - 1) / R.chunk;
-        for (int cz = 0; cz < nc; ++cz)
-            for (int by = 0; by < ty; ++by)
-                for (int bx = 0; bx < tx; ++bx) items.push_back(make_int4(d, bx, by, cz));
-        // 16-bit storage with LES: the general pre-pass hands its FP32 populations to the collide through the stash
         bool st = false;
         if (b->les && b->storage != LBM_STORE_F32) {
-            const size_t ng = (size_t)gz * nx * ny;
+            const size_t ng = (size_t)(R.zcnt[0] + R.zcnt[1] + R.zcnt[2]) * c->P.nx * c->P.ny;
             if (c->stash_cells < ng) {
                 float *p = nullptr;
                 if (alloc(c, (void **)&p, 19 * ng * sizeof(float)) != LBM_OK) {
+                    batch_free(b);
                     delete b;
                     return LBM_ERR_CUDA;
                 }
@@ -1177,44 +1297,20 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
         }
         b->stash.push_back(st);
     }
-    // longest items first: the last items of the queue are the short ones
-    std::stable_sort(items.begin(), items.end(), [&](const int4 &x, const int4 &y) {
-        const Plan &Rx = b->plan[x.x], &Ry = b->plan[y.x];
-        const int px = std::min(Rx.chunk, Rx.zi1 + 1 - (Rx.zi0 + x.w * Rx.chunk));
-        const int py = std::min(Ry.chunk, Ry.zi1 + 1 - (Ry.zi0 + y.w * Ry.chunk));
-        return px > py;
-    });
-    cudaError_t e = cudaSuccess;
-    if ((e = upload_vec(&b->d_col0, col0)) != cudaSuccess || (e = upload_vec(&b->d_gmap, gmap)) != cudaSuccess ||
-        (e = upload_vec(&b->d_smap, smap)) != cudaSuccess || (e = upload_vec(&b->d_items, items)) != cudaSuccess ||
-        (e = cudaMalloc((void **)&b->d_queue, sizeof(int))) != cudaSuccess ||
-        (e = cudaMalloc((void **)&b->d_tab, 2 * n * sizeof(StepArgs))) != cudaSuccess ||
-        (e = cudaMalloc((void **)&b->d_bed, 2 * n * sizeof(BatchBed))) != cudaSuccess ||
-        (e = cudaMallocHost((void **)&b->h_tab, 2 * n * sizeof(StepArgs))) != cudaSuccess ||
-        (e = cudaMallocHost((void **)&b->h_bed, 2 * n * sizeof(BatchBed))) != cudaSuccess) {
+    if (e == cudaSuccess) {
+        where = "tables";
+        if ((e = cudaMalloc((void **)&b->d_bed, 2 * n * sizeof(BatchBed))) == cudaSuccess &&
+            (e = cudaMallocHost((void **)&b->h_bed, 2 * n * sizeof(BatchBed))) == cudaSuccess)
+            e = cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
         batch_free(b);
         delete b;
-        return fail(c0, LBM_ERR_CUDA, std::string("lbm_batch_create: ") + cudaGetErrorString(e));
+        return fail(c0, LBM_ERR_CUDA, "lbm_batch_create: " + where + ": " + cudaGetErrorString(e));
     }
-    BatchLaunch &L = b->L;
-    L.tab = b->d_tab;
-    L.bed = b->d_bed;
-    L.col0 = b->d_col0;
-    L.ndom = n;
-    L.ncols = col0.back();
-    L.gmap = b->d_gmap;
-    L.ngen = (int)gmap.size();
-    L.smap = b->d_smap;
-    L.nsi = (int)smap.size();
-    L.items = b->d_items;
-    L.nitems = (int)items.size();
-    L.queue = b->d_queue;
-    L.tile_blocks = batch_tile_blocks(b->storage, b->arith);
-    if (L.tile_blocks <= 0) {
-        batch_free(b);
-        delete b;
-        return fail(c0, LBM_ERR_UNSUPPORTED, "lbm_batch_create: the interior grid's shared memory was refused");
-    }
+    for (BatchGroupPlan &g : b->groups) g.L.bed = b->d_bed;
+    b->h_tab.resize(2 * (size_t)n);
+    b->G.reset(new BatchGroup());
     *out = b;
     return LBM_OK;
 }
@@ -1243,7 +1339,7 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
             A.bed_s = slot_view(c, (int)((n0 + q) & 1));
             A.bed_c = slot_view(c, (int)((n0 + 1 + q) & 1));
             A.stash = c->stash;
-            b->h_tab[q * n + d] = A;
+            b->h_tab[(size_t)q * n + d] = A;
             const int par = q;   // bed variant by the parity of the bed step
             BatchBed &B = b->h_bed[par * n + d];
             B.P = c->P;
@@ -1259,35 +1355,44 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
         }
     }
     cudaError_t e;
-    if ((e = cudaMemcpyAsync(b->d_tab, b->h_tab, 2 * n * sizeof(StepArgs), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(b->d_bed, b->h_bed, 2 * n * sizeof(BatchBed), cudaMemcpyHostToDevice, st)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(b->d_bed, b->h_bed, 2 * n * sizeof(BatchBed), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (e = cudaEventRecord(b->start, st)) != cudaSuccess)
         return batch_fail(b, LBM_ERR_CUDA, cudaGetErrorString(e));
-    const BatchLaunch &L = b->L;
-    const int S = b->storage;
+    for (BatchGroupPlan &g : b->groups)
+        if ((e = cudaStreamWaitEvent(g.stream, b->start, 0)) != cudaSuccess)
+            return batch_fail(b, LBM_ERR_CUDA, cudaGetErrorString(e));
     const int tflag = b->stash[0] ? F_STASH : 0;
     const int K = nsteps;
-    // first step of the call: collide from the stored post-stream state
-    launch_batch_bed(L, n0 + 1, st);
-    int flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
-    if (b->les) launch_batch_kernel(KER_PREPASS_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st);
-    launch_batch_kernel(KER_TILE_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st, b->arith);
-    launch_batch_kernel(KER_COLLIDE_CANON, S, L, 0, (unsigned long long)(n0 + 1), flags, st);
-    // fused steps: stream + boundary conditions of step m, condition ... collide of step m + 1
-    for (int s = 1; s < K; ++s) {
-        const int64_t m = n0 + s;
-        launch_batch_bed(L, m + 1, st);
-        flags = ((s == K - 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
+    // step s of every group, then step s + 1: the groups' streams run side by side
+    for (int s = 0; s < K; ++s) {
+        const int64_t m = n0 + s;   // s = 0: collide from the stored post-stream state; then fused steps
+        const int flags = ((s == K - 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
         const int q = s & 1;
-        if (b->les) launch_batch_kernel(KER_PREPASS_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st);
-        launch_batch_kernel(KER_TILE_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st, b->arith);
-        launch_batch_kernel(KER_COLLIDE_FUSED, S, L, q, (unsigned long long)(m + 1), flags, st);
+        const unsigned long long step = (unsigned long long)(m + 1);
+        for (BatchGroupPlan &g : b->groups) {
+            launch_batch_bed(g.L, m + 1, g.stream);
+            if (s == 0) {
+                if (b->les) batch_issue(b, g, KER_PREPASS_CANON, 0, step, flags);
+                batch_issue(b, g, KER_TILE_CANON, 0, step, flags);
+                batch_issue(b, g, KER_COLLIDE_CANON, 0, step, flags);
+            } else {
+                if (b->les) batch_issue(b, g, KER_PREPASS_FUSED, q, step, flags);
+                batch_issue(b, g, KER_TILE_FUSED, q, step, flags);
+                batch_issue(b, g, KER_COLLIDE_FUSED, q, step, flags);
+            }
+        }
     }
     // the final stream back to the post-stream state
-    for (lbm_ctx *c : b->ctx)
-        if ((e = cudaMemsetAsync(c->dcount, 0, 3 * sizeof(int), st)) != cudaSuccess)
+    for (BatchGroupPlan &g : b->groups) {
+        for (int d = g.d0; d < g.d0 + g.nd; ++d)
+            if ((e = cudaMemsetAsync(b->ctx[d]->dcount, 0, 3 * sizeof(int), g.stream)) != cudaSuccess)
+                return batch_fail(b, LBM_ERR_CUDA, cudaGetErrorString(e));
+        batch_issue(b, g, KER_STREAM, K & 1, (unsigned long long)(n0 + K), F_COUNT);
+        batch_issue(b, g, KER_STREAM_INTERIOR, K & 1, (unsigned long long)(n0 + K), F_COUNT);
+        if ((e = cudaEventRecord(g.done, g.stream)) != cudaSuccess ||
+            (e = cudaStreamWaitEvent(st, g.done, 0)) != cudaSuccess)
             return batch_fail(b, LBM_ERR_CUDA, cudaGetErrorString(e));
-    launch_batch_kernel(KER_STREAM, S, L, K & 1, (unsigned long long)(n0 + K), F_COUNT, st);
-    launch_batch_kernel(KER_STREAM_INTERIOR, S, L, K & 1, (unsigned long long)(n0 + K), F_COUNT, st);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return batch_fail(b, LBM_ERR_CUDA, cudaGetErrorString(e));
     const int src_final = cur0 ^ (K & 1);
     for (lbm_ctx *c : b->ctx) {

@@ -505,26 +505,51 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream
 namespace lbm {
 
 // -------------------------------------------- height-function free surface
-// compute_free_surface_column_flux, CODEX.py:2376-2388 (sequential in k)
-__global__ void k_column_flux(StepArgs A, float *qx_out, float *qy_out) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= (int)A.D.a) return;
+// compute_free_surface_column_flux, CODEX.py:2376-2388.  A block covers 32
+// columns of one row (x fastest, so the velocity loads coalesce) with 8
+// warps over z: the terms fill u vel_scale dx of FLUX_KC planes are formed in
+// parallel into shared memory, then one warp per component adds them in
+// plane order, so each column's sum is the reference's sequential one.  A
+// gas or closed cell adds +0, which leaves a sum that starts at +0 unchanged.
+constexpr int FLUX_KC = 64;
+__global__ void __launch_bounds__(256) k_column_flux(StepArgs A, float *qx_out, float *qy_out) {
+    __shared__ float sq[2][FLUX_KC][33];
     const Dom &D = A.D;
-    int j = a / D.nx, i = a - j * D.nx;
-    float h = A.fs_h[a];
-    float qx = 0.0f, qy = 0.0f;
-    for (int k = 0; k < D.nz; ++k) {
-        int c = D.cell(k, j, i);
-        int type;
-        float fill;
-        classify_height(A.P, h, k, true, type, fill);
-        if (type == LBM_FS_GAS) continue;
-        if (!cell_open(A.P, A.slot, D, A.bed_s, k, j, i)) continue;
-        qx += fill * A.ux[c] * A.P.vel_scale * A.P.dx;
-        qy += fill * A.uy[c] * A.P.vel_scale * A.P.dx;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int nbx = (D.nx + 31) / 32;
+    const int j = blockIdx.x / nbx, i = (blockIdx.x - j * nbx) * 32 + tx;
+    const bool live = i < D.nx;
+    const int a = j * D.nx + i;
+    const float h = live ? A.fs_h[a] : 0.0f;
+    float q = 0.0f;   // warp 0: x flux, warp 1: y flux
+    for (int k0 = 0; k0 < D.nz; k0 += FLUX_KC) {
+        for (int kk = ty; kk < FLUX_KC; kk += 8) {
+            const int k = k0 + kk;
+            float tqx = 0.0f, tqy = 0.0f;
+            if (live && k < D.nz) {
+                int type;
+                float fill;
+                classify_height(A.P, h, k, true, type, fill);
+                if (type != LBM_FS_GAS && cell_open(A.P, A.slot, D, A.bed_s, k, j, i)) {
+                    const int c = D.cell(k, j, i);
+                    tqx = fill * A.ux[c] * A.P.vel_scale * A.P.dx;
+                    tqy = fill * A.uy[c] * A.P.vel_scale * A.P.dx;
+                }
+            }
+            sq[0][kk][tx] = tqx;
+            sq[1][kk][tx] = tqy;
+        }
+        __syncthreads();
+        if (ty < 2) {
+            const int kn = min(FLUX_KC, D.nz - k0);
+            for (int kk = 0; kk < kn; ++kk) q += sq[ty][kk][tx];
+        }
+        __syncthreads();
     }
-    qx_out[a] = qx;
-    qy_out[a] = qy;
+    if (live) {
+        if (ty == 0) qx_out[a] = q;
+        else if (ty == 1) qy_out[a] = q;
+    }
 }
 
 // advect_free_surface_height, CODEX.py:2391-2429
@@ -565,26 +590,16 @@ __global__ void k_advect(lbm_params P, Dom D, const float *__restrict__ bed_h, c
 
 // refill_new_free_surface_cells, CODEX.py:2163-2316.  Height path: the
 // before/after states come from h_last/h; VOF path: from the stored
-// type_prev/type (F_VOF_STATE).
+// type_prev/type (F_VOF_STATE).  refill_cell handles one cell and returns 1
+// if it refilled it; tp / tn are the cell's types before and after.
 template <int S>
-__global__ void __launch_bounds__(256) k_refill(StepArgs A, const int8_t *type_prev_v, int *count) {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ int refill_cell(const StepArgs &A, const int8_t *type_prev_v, int c, int k, int j, int i,
+                                           int tp, int tn) {
     int did = 0;
     const lbm_params &P = A.P;
     const Dom &D = A.D;
     const bool vofm = (A.flags & F_VOF_STATE) != 0;
-    if (c < (int)D.n) {
-        int k, j, i;
-        cell_of(D, c, k, j, i);
-        int tp, tn;
-        float fl;
-        if (vofm) {
-            tp = type_prev_v[c];
-            tn = A.fs_type[c];
-        } else {
-            classify_height(P, A.fs_h_last[D.col(j, i)], k, true, tp, fl);
-            classify_height(P, A.fs_h[D.col(j, i)], k, true, tn, fl);
-        }
+    {
         bool cand = tp == LBM_FS_GAS && tn != LBM_FS_GAS;
         if (cand && cell_open(P, A.slot, D, A.bed_s, k, j, i)) {
             typename Store<S>::T *fb = (typename Store<S>::T *)A.fdst;
@@ -728,8 +743,52 @@ __global__ void __launch_bounds__(256) k_refill(StepArgs A, const int8_t *type_p
             did = 1;
         }
     }
-    unsigned m = __activemask();
-    int s = __reduce_add_sync(m, did);
+    return did;
+}
+
+// VOF path: one thread per cell, types from the stored fields
+template <int S>
+__global__ void __launch_bounds__(256) k_refill(StepArgs A, const int8_t *type_prev_v, int *count) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    int did = 0;
+    if (c < (int)A.D.n) {
+        int k, j, i;
+        cell_of(A.D, c, k, j, i);
+        did = refill_cell<S>(A, type_prev_v, c, k, j, i, type_prev_v[c], A.fs_type[c]);
+    }
+    const int s = __reduce_add_sync(0xffffffffu, did);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(count, s);
+}
+
+// Height path: one thread per column.  A cell is refilled only if it was gas
+// under the height before advection and is not gas under the new one, which
+// needs k dx within a cell of the two heights: the planes from two below the
+// lower height to two above the higher one are tested (every plane if a
+// height is not finite); every other plane is liquid or gas under both.
+template <int S>
+__global__ void __launch_bounds__(256) k_refill_height(StepArgs A, int *count) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    int did = 0;
+    const Dom &D = A.D;
+    if (a < (int)D.a) {
+        const int j = a / D.nx, i = a - j * D.nx;
+        const float hl = A.fs_h_last[a], hn = A.fs_h[a];
+        int k0 = 0, k1 = D.nz - 1;
+        if (hl == hl && hn == hn) {
+            const float lo = fminf(fmaxf(fminf(hl, hn) / A.P.dx, -4.0f), (float)D.nz + 4.0f);
+            const float hi = fminf(fmaxf(fmaxf(hl, hn) / A.P.dx, -4.0f), (float)D.nz + 4.0f);
+            k0 = max(0, (int)floorf(lo) - 2);
+            k1 = min(D.nz - 1, (int)floorf(hi) + 2);
+        }
+        for (int k = k0; k <= k1; ++k) {
+            int tp, tn;
+            float fl;
+            classify_height(A.P, hl, k, true, tp, fl);
+            classify_height(A.P, hn, k, true, tn, fl);
+            if (tp == LBM_FS_GAS && tn != LBM_FS_GAS) did += refill_cell<S>(A, nullptr, D.cell(k, j, i), k, j, i, tp, tn);
+        }
+    }
+    const int s = __reduce_add_sync(0xffffffffu, did);
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(count, s);
 }
 
@@ -1221,13 +1280,24 @@ void launch_step_kernel(int which, const StepArgs &A, cudaStream_t st) {
     }
 }
 void launch_column_flux(const StepArgs &A, float *qx, float *qy, cudaStream_t st) {
-    k_column_flux<<<blocks_for(A.D.a, 128), 128, 0, st>>>(A, qx, qy); LAUNCHED(1);
+    const unsigned g = (unsigned)(((A.D.nx + 31) / 32) * A.D.ny);
+    k_column_flux<<<g, dim3(32, 8, 1), 0, st>>>(A, qx, qy); LAUNCHED(1);
 }
 void launch_advect(const lbm_params &P, const Dom &D, const float *bed_h, const float *qx, const float *qy,
                    const float *h_in, float *h_out, float *h_last, float t, cudaStream_t st) {
     k_advect<<<blocks_for(D.a, 256), 256, 0, st>>>(P, D, bed_h, qx, qy, h_in, h_out, h_last, t); LAUNCHED(1);
 }
 void launch_refill(const StepArgs &A, const int8_t *type_prev, int *count, cudaStream_t st) {
+    if (!(A.flags & F_VOF_STATE)) {
+        const unsigned gh = blocks_for(A.D.a, 256);
+        switch (A.P.pop_storage) {
+            case LBM_STORE_F16S: k_refill_height<LBM_STORE_F16S><<<gh, 256, 0, st>>>(A, count); break;
+            case LBM_STORE_BF16S: k_refill_height<LBM_STORE_BF16S><<<gh, 256, 0, st>>>(A, count); break;
+            default: k_refill_height<LBM_STORE_F32><<<gh, 256, 0, st>>>(A, count); break;
+        }
+        LAUNCHED(1);
+        return;
+    }
     unsigned g = blocks_for(A.D.n, 256);
     switch (A.P.pop_storage) {
         case LBM_STORE_F16S: { k_refill<LBM_STORE_F16S><<<g, 256, 0, st>>>(A, type_prev, count); LAUNCHED(1); } break;
@@ -1432,43 +1502,37 @@ void launch_batch_bed(const BatchLaunch &L, long long m, cudaStream_t st) {
     kb_colgeo<<<blocks_for((size_t)L.ncols, 128), 128, 0, st>>>(L, par); LAUNCHED(1);
 }
 
-int batch_tile_blocks(int storage, int arith) {
-    if (arith == LBM_ARITH_FAST) return batch_tile_blocks_fast(storage);
-    switch (storage) {
-        case LBM_STORE_F16S: return batch_tile_blocks_t<LBM_STORE_F16S, ArExact, ArExact>();
-        case LBM_STORE_BF16S: return batch_tile_blocks_t<LBM_STORE_BF16S, ArExact, ArExact>();
-        default: return batch_tile_blocks_t<LBM_STORE_F32, ArExact, ArExact>();
-    }
+int batch_tile_blocks(int storage, bool les, int collision, int arith) {
+    if (arith == LBM_ARITH_FAST) return batch_tile_blocks_fast(storage, les, collision);
+    return batch_tile_blocks_any<ArExact>(storage, les);
 }
 
 template <int S>
-static void launch_batch_kernel_s(int which, const BatchLaunch &L, int q, unsigned long long step, int flags,
-                                  cudaStream_t st) {
+static void launch_batch_group_s(int which, const BatchGroup &G, cudaStream_t st) {
+    if (!G.nmap) return;
     const dim3 b3(32, 8, 1);
     switch (which) {
-        case KER_PREPASS_CANON: if (L.ngen) { kb_general<S, 0, 0><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
-        case KER_PREPASS_FUSED: if (L.ngen) { kb_general<S, 1, 0><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
-        case KER_COLLIDE_CANON: if (L.ngen) { kb_general<S, 0, 1><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
-        case KER_COLLIDE_FUSED: if (L.ngen) { kb_general<S, 1, 1><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
-        case KER_STREAM: if (L.ngen) { kb_general<S, 0, 2><<<L.ngen, b3, 0, st>>>(L, q, step, flags); LAUNCHED(1); } break;
-        case KER_STREAM_INTERIOR:
-            if (L.nsi) { kb_stream_interior<S><<<L.nsi, 256, 0, st>>>(L, q, step, flags); LAUNCHED(1); }
-            break;
-        case KER_TILE_CANON:
-        case KER_TILE_FUSED: launch_batch_tile_t<S, ArExact, ArExact>(which, L, q, step, flags, st); break;
-        default: break;
+        case KER_PREPASS_CANON: kb_general<S, 0, 0><<<G.nmap, b3, 0, st>>>(G); break;
+        case KER_PREPASS_FUSED: kb_general<S, 1, 0><<<G.nmap, b3, 0, st>>>(G); break;
+        case KER_COLLIDE_CANON: kb_general<S, 0, 1><<<G.nmap, b3, 0, st>>>(G); break;
+        case KER_COLLIDE_FUSED: kb_general<S, 1, 1><<<G.nmap, b3, 0, st>>>(G); break;
+        case KER_STREAM: kb_general<S, 0, 2><<<G.nmap, b3, 0, st>>>(G); break;
+        case KER_STREAM_INTERIOR: kb_stream_interior<S><<<G.nmap, 256, 0, st>>>(G); break;
+        default: return;
     }
+    LAUNCHED(1);
 }
-void launch_batch_kernel(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
-                         cudaStream_t st, int arith) {
-    if (arith == LBM_ARITH_FAST && (which == KER_TILE_CANON || which == KER_TILE_FUSED)) {
-        launch_batch_tile_fast(which, storage, L, q, step, flags, st);
+void launch_batch_group(int which, int storage, const BatchGroup &G, bool les, int collision, int arith,
+                        int tile_blocks, cudaStream_t st) {
+    if (which == KER_TILE_CANON || which == KER_TILE_FUSED) {
+        if (arith == LBM_ARITH_FAST) launch_batch_tile_fast(which, storage, G, les, collision, tile_blocks, st);
+        else launch_batch_tile_any<ArExact>(which, storage, G, les, tile_blocks, st);
         return;
     }
     switch (storage) {
-        case LBM_STORE_F16S: launch_batch_kernel_s<LBM_STORE_F16S>(which, L, q, step, flags, st); break;
-        case LBM_STORE_BF16S: launch_batch_kernel_s<LBM_STORE_BF16S>(which, L, q, step, flags, st); break;
-        default: launch_batch_kernel_s<LBM_STORE_F32>(which, L, q, step, flags, st); break;
+        case LBM_STORE_F16S: launch_batch_group_s<LBM_STORE_F16S>(which, G, st); break;
+        case LBM_STORE_BF16S: launch_batch_group_s<LBM_STORE_BF16S>(which, G, st); break;
+        default: launch_batch_group_s<LBM_STORE_F32>(which, G, st); break;
     }
 }
 

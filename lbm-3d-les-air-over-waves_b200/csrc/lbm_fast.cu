@@ -28,24 +28,18 @@ bool launch_tile_tma_fast(const StepArgs &A, const CUtensorMap *m24, const CUten
     }
 }
 
-typedef ArFast<LBM_COLLIDE_KBC> ArFastK;
-typedef ArFast<LBM_COLLIDE_REGULARIZED> ArFastR;
-
-void launch_batch_tile_fast(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
+// the interior grid of an ensemble group: the group's collision model picks the policy
+void launch_batch_tile_fast(int which, int storage, const BatchGroup &G, bool les, int collision, int tile_blocks,
                             cudaStream_t st) {
-    switch (storage) {
-        case LBM_STORE_F16S: launch_batch_tile_t<LBM_STORE_F16S, ArFastK, ArFastR>(which, L, q, step, flags, st); break;
-        case LBM_STORE_BF16S: launch_batch_tile_t<LBM_STORE_BF16S, ArFastK, ArFastR>(which, L, q, step, flags, st); break;
-        default: launch_batch_tile_t<LBM_STORE_F32, ArFastK, ArFastR>(which, L, q, step, flags, st); break;
-    }
+    if (collision == LBM_COLLIDE_KBC)
+        launch_batch_tile_any<ArFast<LBM_COLLIDE_KBC>>(which, storage, G, les, tile_blocks, st);
+    else
+        launch_batch_tile_any<ArFast<LBM_COLLIDE_REGULARIZED>>(which, storage, G, les, tile_blocks, st);
 }
 
-int batch_tile_blocks_fast(int storage) {
-    switch (storage) {
-        case LBM_STORE_F16S: return batch_tile_blocks_t<LBM_STORE_F16S, ArFastK, ArFastR>();
-        case LBM_STORE_BF16S: return batch_tile_blocks_t<LBM_STORE_BF16S, ArFastK, ArFastR>();
-        default: return batch_tile_blocks_t<LBM_STORE_F32, ArFastK, ArFastR>();
-    }
+int batch_tile_blocks_fast(int storage, bool les, int collision) {
+    if (collision == LBM_COLLIDE_KBC) return batch_tile_blocks_any<ArFast<LBM_COLLIDE_KBC>>(storage, les);
+    return batch_tile_blocks_any<ArFast<LBM_COLLIDE_REGULARIZED>>(storage, les);
 }
 
 }  // namespace lbm

@@ -188,7 +188,7 @@ constexpr int DIAG_SLICE_THREADS = 128;   // 128 slice partials of 208 bytes fit
 
 void launch_diagnostics(const DiagArgs &G, cudaStream_t st);
 
-// ---- ensembles stepped with one launch per phase (lbm_batch.cuh)
+// ---- ensembles stepped with one launch per phase and group (lbm_batch.cuh)
 // One domain's 2-D bed state for the bed step of one parity.
 struct BatchBed {
     lbm_params P;
@@ -197,32 +197,42 @@ struct BatchBed {
     float *h, *hmax, *uw, *vw, *ww;
     float *cg;                       // column cache of the slot (null without one)
 };
+// the bed phase of one group: one thread per column of its domains
 struct BatchLaunch {
-    const StepArgs *tab;             // [2][ndom] step arguments by the step's index in the call, mod 2
-    const BatchBed *bed;             // [2][ndom] by the parity of the bed step
-    const long long *col0;           // [ndom + 1] first column of each domain in the concatenation
+    const BatchBed *bed;             // [2][nall] by the parity of the bed step, whole ensemble
+    int nall;                        // domains of the ensemble
+    int d0;                          // ensemble index of the group's first domain
+    const long long *col0;           // [ndom + 1] first column of each of the group's domains
     int ndom;
     long long ncols;
-    const int4 *gmap;                // general-kernel blocks: (domain, bx, by, bz)
-    int ngen;
-    const int4 *smap;                // interior stream blocks: (domain, bx, by, bz)
-    int nsi;
-    const int4 *items;               // interior work items: (domain, tile x, tile y, z chunk)
-    int nitems;
-    int *queue;                      // next work item of the interior grid
-    int tile_blocks;                 // resident blocks of the interior grid
 };
-// bed, 3x3 maximum and column cache of every domain at step m
+// Domains per launch of the step grids.  Their step arguments travel in the
+// kernel's parameter space (read-only, at most 32,764 bytes), so that the
+// shared bodies read them, indexed by the block's domain, as a domain's own
+// kernel reads its argument, without copies to shared memory or registers.
+constexpr int BATCH_GROUP = 36;
+struct BatchGroup {
+    const int4 *map;                 // general / stream blocks: (domain, bx, by, bz); interior grid: work
+                                     // items (domain, tile x, tile y, z chunk); domain = index in a[]
+    int nmap;
+    int ndom;
+    int *queue;                      // interior grid: next work item
+    StepArgs a[BATCH_GROUP];         // step arguments of the launch (step number and flags included)
+};
+static_assert(sizeof(BatchGroup) <= 32764, "kernel parameter space");
+
+// bed, 3x3 maximum and column cache of the group's domains at step m
 void launch_batch_bed(const BatchLaunch &L, long long m, cudaStream_t st);
-// one phase for every domain (which = KER_PREPASS_*, KER_TILE_*, KER_COLLIDE_*, KER_STREAM, KER_STREAM_INTERIOR);
-// arith: the arithmetic policy of the interior planes (LBM_ARITH_*)
-void launch_batch_kernel(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
-                         cudaStream_t st, int arith = LBM_ARITH_EXACT);
+// one phase over one group (which = KER_PREPASS_*, KER_TILE_*, KER_COLLIDE_*, KER_STREAM, KER_STREAM_INTERIOR);
+// the group's domains share storage, LES and collision model; arith: the interior planes' policy (LBM_ARITH_*);
+// tile_blocks: resident blocks of the interior grid
+void launch_batch_group(int which, int storage, const BatchGroup &G, bool les, int collision, int arith,
+                        int tile_blocks, cudaStream_t st);
 // resident blocks of the interior grid on this device (0: the shared memory is refused)
-int batch_tile_blocks(int storage, int arith = LBM_ARITH_EXACT);
-// the fast-arithmetic interior grid of an ensemble (lbm_fast.cu)
-void launch_batch_tile_fast(int which, int storage, const BatchLaunch &L, int q, unsigned long long step, int flags,
+int batch_tile_blocks(int storage, bool les, int collision, int arith);
+// the fast-arithmetic interior grid of a group (lbm_fast.cu)
+void launch_batch_tile_fast(int which, int storage, const BatchGroup &G, bool les, int collision, int tile_blocks,
                             cudaStream_t st);
-int batch_tile_blocks_fast(int storage);
+int batch_tile_blocks_fast(int storage, bool les, int collision);
 
 }  // namespace lbm

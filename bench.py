@@ -541,15 +541,70 @@ def serving(args):
     return 0
 
 
+# the stated-size configurations other than the plain roofline run: name -> (env builder, storage)
+CONFIGS = {
+    "C1": ("air over moving wave 128x64x64, regularized + LES, 1000-step case", "f32"),
+    "C2": ("water height path 256x128x96, Gaussian mound, solid x walls", "f32"),
+    "C2-f16s": ("water height path 256x128x96, Gaussian mound, solid x walls", "f16s"),
+    "C2-bf16s": ("water height path 256x128x96, Gaussian mound, solid x walls", "bf16s"),
+    "C3": ("VOF falling block 384x192x192, KBC, collapse and bridge", "f16s"),
+}
+
+
+def _config_env(name: str, storage: str) -> dict:
+    from lbm_b200.config import air_wave_env, vof_block_env, water_gaussian_env
+
+    if name == "C1":
+        return air_wave_env(128, 64, 64, storage=storage)
+    if name.startswith("C2"):
+        return water_gaussian_env(256, 128, 96, storage=storage, depth=48.0, amp=8.0, sigma=16.0, g_lb=1e-5,
+                                  tau0=0.51)
+    return vof_block_env(384, 192, 192, storage=storage)
+
+
+def configs(args):
+    """Device time per step of the stated-size configurations (eager calls,
+    CUDA events on the domain's stream, after warm-up), one JSON line."""
+    import torch
+
+    from lbm_b200.domain import Domain
+
+    names = args.only.split(",") if args.only else list(CONFIGS)
+    out = {}
+    for name in names:
+        what, storage = CONFIGS[name]
+        d = Domain(_config_env(name, storage), device="cuda:0", with_diag=False)
+        d.step(max(3, args.warmup))
+        d.synchronize()
+        K = args.steps
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(d.stream)
+        d.step(K)
+        e1.record(d.stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / K
+        cells = d.cfg.Nx * d.cfg.Ny * d.cfg.Nz
+        out[name] = {"workload": what, "storage": storage, "cells": cells, "steps": K, "ms_per_step": ms,
+                     "value": cells / ms / 1e3, "unit": UNIT, "status_flags": d.counters()["status_flags"]}
+        d.close()
+        del d
+        torch.cuda.empty_cache()
+    print(json.dumps({"metric": METRIC, "mode": "configs", "n_gpus": 1, "data": "synthetic", "configs": out}),
+          flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--mode", choices=("plain", "batched", "serving"), default="plain",
+    ap.add_argument("--mode", choices=("plain", "batched", "serving", "configs"), default="plain",
                     help="plain: the 512x256x256 step (default); batched: the 96-domain ensemble; "
-                         "serving: the request loop on a Poisson trace")
+                         "serving: the request loop on a Poisson trace; configs: the other stated-size "
+                         "configurations (C1 air, C2 water in three storages, C3 VOF)")
+    ap.add_argument("--only", type=str, default=None, help="configs mode: comma-separated subset (C1,C2,...)")
     ap.add_argument("--storage", choices=("f32", "f16s", "bf16s"), default=None,
                     help="population storage of the batched and serving modes (default f16s)")
     ap.add_argument("--domains", type=int, default=96, help="batched mode: ensemble size")
@@ -585,6 +640,8 @@ def main():
         return batched(args)
     if args.mode == "serving":
         return serving(args)
+    if args.mode == "configs":
+        return configs(args)
     return ours(args)
 
 

@@ -536,12 +536,17 @@ static int step_height(lbm_ctx *ctx, int K, cudaStream_t st) {
             launch_step_kernel(KER_PREPASS_CANON, A, st);
             CK_LAUNCH("prepass");
         }
+        // the compact kernels take the cells with local collide / plain-gather
+        // stream, the general ones the rest (disjoint cells, either order)
+        A.flags |= F_WATER_SPLIT;
+        launch_step_kernel(KER_WATER_COLLIDE, A, st);
         launch_step_kernel(KER_COLLIDE_CANON, A, st);
         CK_LAUNCH("collide");
         CK(cudaMemsetAsync(ctx->dcount, 0, 4 * sizeof(int), st), "counter reset");
         A.fsrc = ctx->b.f[1 - ctx->cur];
         A.fdst = ctx->b.f[ctx->cur];
-        A.flags = F_COUNT;
+        A.flags = F_COUNT | F_WATER_SPLIT;
+        launch_step_kernel(KER_WATER_STREAM, A, st);
         launch_step_kernel(KER_STREAM, A, st);
         CK_LAUNCH("stream");
         launch_column_flux(A, ctx->b.fs_flux_x, ctx->b.fs_flux_y, st);
@@ -1268,6 +1273,12 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
         g.L.ndom = g.nd;
         g.L.ncols = col0.back();
         g.tile_blocks = batch_tile_blocks(b->storage, b->les, g.collision, b->arith);
+        // LBM_B200_BATCH_TILE_BLOCKS: fewer resident blocks for the interior grid, leaving
+        // SM room for the other groups' kernels
+        if (const char *tb = getenv("LBM_B200_BATCH_TILE_BLOCKS")) {
+            const int v = atoi(tb);
+            if (v > 0 && v < g.tile_blocks) g.tile_blocks = v;
+        }
         if (g.tile_blocks <= 0) {
             batch_free(b);
             delete b;

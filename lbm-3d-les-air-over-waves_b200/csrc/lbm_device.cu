@@ -259,6 +259,29 @@ __device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int 
     return hmin > ((float)k + 1.01f) * dx ? 2 : 0;
 }
 
+// Height-path water cell whose collide needs no link geometry: inside the
+// domain's z range, farther than half a cell from the bed, no cube, phi
+// geometry, fringe or top drive.  Its own link (q = 0) is open, and every
+// closed link is an x wall, where the water path's condition stage applies
+// nothing (only bed links, or any link in air physics, are conditioned).
+__device__ __forceinline__ bool water_collide_local(const StepArgs &A, int k, int j, int i) {
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    if (P.fs_mode == LBM_FS_NONE || (A.flags & F_VOF_STATE) || !P.physics_water) return false;
+    if (k < 1 || k > D.nz - 2) return false;
+    if (P.enable_x_fringe || P.enable_top_drive || P.include_cube || P.use_phi_open_fraction ||
+        P.use_phi_open_flags)
+        return false;
+    if (P.include_bed) {
+        const float dx = P.dx, hdx = 0.5f * dx;
+        const float zc = ((float)k + 0.5f) * dx;
+        const float hm = __ldg(A.bed_c.hmax + D.col(j, i));
+        const float margin = 1e-4f * dx + 1e-6f * (fabsf(zc) + fabsf(hm));
+        if (!((zc - hdx) - hm >= hdx + margin)) return false;
+    }
+    return true;
+}
+
 // gas_free: the caller does not read the populations of a gas cell (the
 // velocity pre-pass, whose gas velocity is zero, and the regularized
 // collision, whose gas output is the rest equilibrium), so with a free
@@ -361,6 +384,7 @@ template <int S, int IN, bool CG>
 __device__ __forceinline__ void collide_body(const StepArgs &A, int bx, int by, int bz, int gz) {
     int i, j, k, c;
     if (!cell_xyz(A, bx, by, bz, i, j, k, c)) return;
+    if (!CG && IN == 0 && (A.flags & F_WATER_SPLIT) && water_collide_local(A, k, j, i)) return;   // k_collide_water
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
@@ -422,7 +446,9 @@ __device__ __forceinline__ void stream_body(const StepArgs &A, int bx, int by, i
     if (cell_xyz(A, bx, by, bz, i, j, k, c)) {
         float f[19];
         const int wcls = CG ? 0 : water_stream_class(A, k, j, i);
-        if (cell_fast(A, true, false, k, j, i)) {
+        if (!CG && wcls != 0 && (A.flags & F_WATER_SPLIT)) {
+            // k_stream_water
+        } else if (cell_fast(A, true, false, k, j, i)) {
             stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
             store_cell<S>(A, c, f);
         } else if (wcls != 0) {
@@ -496,6 +522,107 @@ __device__ __forceinline__ void stream_body(const StepArgs &A, int bx, int by, i
 template <int S, bool CG>
 __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream(StepArgs A) {
     stream_body<S, CG>(A, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ------------------------------------------ compact kernels of height-path water
+// The cells that water_collide_local (collide) or water_stream_class (stream)
+// admit take the same stage functions as in the general kernels, in kernels
+// that carry none of the near-wall, free-surface-cut or VOF code, so they are
+// small enough to run without register spills or instruction-cache misses.
+// The general kernels, launched with F_WATER_SPLIT, skip these cells.
+template <int S, int COLL>
+__global__ void __launch_bounds__(256, 2) k_collide_water(StepArgs A) {
+    int i, j, k, c;
+    if (!cell_xyz(A, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k, c)) return;
+    if (!water_collide_local(A, k, j, i)) return;
+    const lbm_params &P = A.P;
+    // front() for such a cell: open, no closed link to condition
+    const bool fast_c = !(P.x_solid && (i == 0 || i == A.D.nx - 1));
+    int type;
+    float fill;
+    fs_state(A, c, k, j, i, true, type, fill);
+    const float gbf = gbf_of(P, k, true, type);
+    const bool gas = type == LBM_FS_GAS;
+    float f[19];
+    if (gas && COLL == LBM_COLLIDE_REGULARIZED) {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) f[q] = 0.0f;   // macro_step gives (rho0, 0) for a gas cell
+    } else {
+        load_cell<S>(A, c, f);
+    }
+    float r, vx, vy, vz;
+    macro(P, A.D, f, k, true, type, gbf, r, vx, vy, vz);
+    if (A.flags & F_WRITE_MACRO) {
+        A.rho[c] = r; A.ux[c] = vx; A.uy[c] = vy; A.uz[c] = vz;
+    }
+    if (!(r == r) || fabsf(r) > 3.0e38f) atomicOr(A.status, 1u);
+    float om;
+    if (P.use_les) {
+        if (!gas) {
+            om = les_omega(A, k, j, i, c, vx, vy, vz);
+            if ((A.flags & F_WRITE_ALL_OMEGA) || !fast_c) A.omega[c] = om;
+        } else {
+            om = A.omega[c];
+        }
+    } else {
+        om = P.omega0;
+    }
+    collide<COLL>(A, c, k, false, true, gas, gbf, r, vx, vy, vz, om, f);
+    store_cell<S>(A, c, f);
+}
+
+template <int S>
+__global__ void __launch_bounds__(256, 2) k_stream_water(StepArgs A) {
+    int i, j, k, c;
+    int cut = 0;
+    if (cell_xyz(A, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k, c)) {
+        const int wcls = water_stream_class(A, k, j, i);
+        if (wcls != 0) {
+            // the water branch of stream_body: a gas cell takes the rest
+            // equilibrium, a cell whose sources are all wet the plain gather
+            // (links through a solid x wall carry the cell's own opposite
+            // population); then the post-stream macro step
+            float f[19];
+            const typename Store<S>::T *fs = (const typename Store<S>::T *)A.fsrc;
+            const bool xwall = A.P.x_solid && (i == 0 || i + 1 == A.D.nx);
+            if (wcls == 1) {
+                f[0] = feq<0>(A.P.rho0, 0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+                for (int q = 1; q < 19; ++q) f[q] = A.P.rho0 * wq(q) * 1.0f;
+            } else if (!xwall) {
+                stream_fast<S>(A, fs, k, j, i, c, f);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 19; ++q) {
+                    const int si = i - cxq(q);
+                    if (si < 0 || si >= A.D.nx) continue;
+                    const int sj = (j - cyq(q) + A.D.ny) % A.D.ny;
+                    f[q] = Store<S>::ld(fs, (size_t)q * A.D.n + A.D.cell(k - czq(q), sj, si), q, A.P.rho0);
+                }
+            }
+            if (xwall) {
+#pragma unroll
+                for (int q = 1; q < 19; ++q) {
+                    if ((i == 0 && cxq(q) > 0) || (i + 1 == A.D.nx && cxq(q) < 0)) {
+                        f[q] = Store<S>::ld(fs, (size_t)oppq(q) * A.D.n + c, oppq(q), A.P.rho0);
+                        if (wcls == 2) cut++;
+                    }
+                }
+            }
+            store_cell<S>(A, c, f);
+            int type;
+            float fill;
+            fs_state(A, c, k, j, i, true, type, fill);
+            const float gbf = gbf_of(A.P, k, true, type);
+            float r, vx, vy, vz;
+            macro(A.P, A.D, f, k, true, type, gbf, r, vx, vy, vz);
+            A.rho[c] = r; A.ux[c] = vx; A.uy[c] = vy; A.uz[c] = vz;
+        }
+    }
+    if (A.flags & F_COUNT) {
+        const int s0 = __reduce_add_sync(0xffffffffu, cut);
+        if ((threadIdx.x & 31) == 0 && s0) atomicAdd(A.counters + 0, s0);
+    }
 }
 
 }  // namespace lbm
@@ -1189,7 +1316,7 @@ template <int S>
 static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) {
     dim3 g = grid3(A);
     const int ni = A.zi1 - A.zi0 + 1;
-    const bool tile_kernel = which >= KER_TILE_CANON;
+    const bool tile_kernel = which == KER_TILE_CANON || which == KER_TILE_FUSED || which == KER_STREAM_INTERIOR;
     if (!tile_kernel && g.z == 0) return;
     if (tile_kernel && (ni <= 0 || A.chunk <= 0)) return;
     const unsigned tz = tile_kernel ? (unsigned)((ni + A.chunk - 1) / A.chunk) : 0u;
@@ -1230,6 +1357,15 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
         case KER_STREAM:
             if (cg) k_stream<S, true><<<g, kBlock3, 0, st>>>(A);
             else k_stream<S, false><<<g, kBlock3, 0, st>>>(A);
+            LAUNCHED(1);
+            break;
+        case KER_WATER_COLLIDE:
+            if (A.P.collision == LBM_COLLIDE_KBC) k_collide_water<S, LBM_COLLIDE_KBC><<<g, kBlock3, 0, st>>>(A);
+            else k_collide_water<S, LBM_COLLIDE_REGULARIZED><<<g, kBlock3, 0, st>>>(A);
+            LAUNCHED(1);
+            break;
+        case KER_WATER_STREAM:
+            k_stream_water<S><<<g, kBlock3, 0, st>>>(A);
             LAUNCHED(1);
             break;
         case KER_TILE_CANON:

@@ -61,8 +61,13 @@ LBM_DEV void fast_limit(const float fe[19], float f[19]) {
 
 template <int COLL>
 struct ArFast {
-    static LBM_DEV void macro(const lbm_params &, const Dom &, const float f[19], int, float &r, float &vx, float &vy,
-                              float &vz) {
+    static LBM_DEV void macro(const lbm_params &P_, const Dom &D_, const float f[19], int k_, float &r, float &vx,
+                              float &vy, float &vz) {
+#ifdef LBM_FAST_EXACT_MACRO
+        // the reference's summation order (sums only: nothing to contract)
+        ArExact::macro(P_, D_, f, k_, r, vx, vy, vz);
+        return;
+#endif
         const float d1 = f[1] - f[2], d3 = f[3] - f[4], d5 = f[5] - f[6], d7 = f[7] - f[9], d8 = f[8] - f[10];
         const float d11 = f[11] - f[13], d12 = f[12] - f[14], d15 = f[15] - f[17], d16 = f[16] - f[18];
         const float s0 = (f[0] + f[1]) + (f[2] + f[3]) + (f[4] + f[5]) + (f[6] + f[7]);
@@ -101,7 +106,7 @@ struct ArFast {
         const lbm_params &P = A.P;
         if (COLL == LBM_COLLIDE_KBC && (P.c_backscatter > 0.0f || (P.enable_top_sponge && k > A.D.nz - 3))) {
             // stochastic backscatter and the top sponge: the reference arithmetic
-            lbm::collide(A, c, k, false, false, false, 0.0f, r, vx, vy, vz, om, f);
+            lbm::collide<COLL>(A, c, k, false, false, false, 0.0f, r, vx, vy, vz, om, f);
             return;
         }
         const float u2 = vx * vx + vy * vy + vz * vz;

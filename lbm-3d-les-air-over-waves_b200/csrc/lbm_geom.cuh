@@ -154,10 +154,16 @@ static __device__ __noinline__ float sample_phi(int slot, Dom D, const float *h,
     return pxy_0 * (1.0f - fz) + pxy_1 * fz;
 }
 
+LBM_DEV bool geo_far_except_x(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i);
 // conservative "far from every wall" test
 LBM_DEV bool geo_far(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i) {
-    if (P.use_phi_open_fraction || P.use_phi_open_flags) return false;
     if (P.x_solid && (i == 0 || i == D.nx - 1)) return false;
+    return geo_far_except_x(P, D, B, k, j, i);
+}
+// the same test without the solid x walls: the cell may have links closed
+// by an x wall, but none that meets the bed, the cube or phi geometry
+LBM_DEV bool geo_far_except_x(const lbm_params &P, const Dom &D, const BedView &B, int k, int j, int i) {
+    if (P.use_phi_open_fraction || P.use_phi_open_flags) return false;
     const float dx = P.dx, hdx = 0.5f * dx;
     float zc = ((float)k + 0.5f) * dx;
     if (P.include_bed) {
@@ -391,7 +397,8 @@ static __device__ __noinline__ bool cell_open_slow(int slot, Dom D, BedView B, i
 }
 // lattice_open[0] only (cheap when far from walls)
 LBM_DEV bool cell_open(const lbm_params &P, int slot, const Dom &D, const BedView &B, int k, int j, int i) {
-    if (geo_far(P, D, B, k, j, i)) return true;
+    // a solid x wall closes links of the cells next to it, not the cells
+    if (geo_far_except_x(P, D, B, k, j, i)) return true;
     return cell_open_slow(slot, D, B, k, j, i);
 }
 

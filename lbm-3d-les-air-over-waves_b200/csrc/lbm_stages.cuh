@@ -590,6 +590,9 @@ LBM_DEV float hermite2(float Pxx, float Pyy, float Pzz, float Pxy, float Pxz, fl
 }
 
 // collide_KBC / collide_regularized for one cell (in place on f[])
+// COLL: the collision model when the caller knows it at compile time (-1:
+// from P.collision)
+template <int COLL = -1>
 LBM_DEV void collide(const StepArgs &A, int c, int k, bool solid, bool water, bool gas, float gbf, float r,
                      float vx, float vy, float vz, float om, float f[19]) {
     const lbm_params &P = A.P;
@@ -608,7 +611,7 @@ LBM_DEV void collide(const StepArgs &A, int c, int k, bool solid, bool water, bo
     }
     const bool force = water && !gas;
     const float fz = force ? -r * g_local(P, gbf) : 0.0f;
-    if (P.collision == LBM_COLLIDE_REGULARIZED) {
+    if (COLL == LBM_COLLIDE_REGULARIZED || (COLL < 0 && P.collision == LBM_COLLIDE_REGULARIZED)) {
         if (gas) {
 #pragma unroll
             for (int q = 0; q < 19; ++q) f[q] = fe[q];

@@ -1085,7 +1085,12 @@ struct BatchGroupPlan {
     long long *d_col0 = nullptr;
     int4 *d_gmap = nullptr, *d_smap = nullptr, *d_items = nullptr;
     int ngen = 0, nsi = 0, nitems = 0;
-    int *d_queue = nullptr;
+    // fused steps with LES: the tiles off the edge of the domains that allow
+    // tile copies (inner, kb_tile_tma) and all other tiles (edge, kb_tile)
+    int4 *d_edge = nullptr, *d_inner = nullptr;
+    int nedge = 0, ninner = 0;
+    int tma_blocks = 0;
+    int *d_queue = nullptr;             // [3]: all items, edge items, inner items
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
 };
@@ -1094,6 +1099,7 @@ struct lbm_batch {
     std::vector<lbm_ctx *> ctx;         // grouped order (by collision model, then the caller's order)
     std::vector<Plan> plan;
     std::vector<bool> stash;
+    std::vector<bool> tma;              // domains whose inner tiles take the tile-copy grid
     std::vector<BatchGroupPlan> groups;
     int storage = 0;
     int arith = LBM_ARITH_EXACT;        // of the interior planes, uniform over the ensemble
@@ -1116,6 +1122,8 @@ static void batch_free(lbm_batch *b) {
         cudaFree(g.d_gmap);
         cudaFree(g.d_smap);
         cudaFree(g.d_items);
+        cudaFree(g.d_edge);
+        cudaFree(g.d_inner);
         cudaFree(g.d_queue);
         if (g.done) cudaEventDestroy(g.done);
         if (g.stream) cudaStreamDestroy(g.stream);
@@ -1138,7 +1146,10 @@ static cudaError_t upload_vec(T **dst, const std::vector<T> &v) {
 
 // One phase of one group: the group's step arguments for the step's parity q,
 // with the step number and flags of the launch, into the launch parameters.
-static void batch_issue(lbm_batch *b, const BatchGroupPlan &g, int which, int q, unsigned long long step, int flags) {
+// edge: the fused interior step on the edge item list only (the inner items
+// go to the tile-copy grid, which = KER_TILE_TMA).
+static void batch_issue(lbm_batch *b, const BatchGroupPlan &g, int which, int q, unsigned long long step, int flags,
+                        bool edge = false) {
     const int n = (int)b->ctx.size();
     BatchGroup &G = *b->G;
     G.ndom = g.nd;
@@ -1148,7 +1159,23 @@ static void batch_issue(lbm_batch *b, const BatchGroupPlan &g, int which, int q,
         G.a[d].flags = flags;
     }
     G.queue = g.d_queue;
-    if (which == KER_TILE_CANON || which == KER_TILE_FUSED) {
+    int blocks = g.tile_blocks;
+    if (which == KER_TILE_TMA) {
+        for (int d = 0; d < g.nd; ++d) {
+            lbm_ctx *c = b->ctx[g.d0 + d];
+            const int src = G.a[d].fsrc == c->b.f[0] ? 0 : 1;
+            G.tmap[d][0] = c->tmap[src][0];
+            G.tmap[d][1] = c->tmap[src][1];
+        }
+        G.map = g.d_inner;
+        G.nmap = g.ninner;
+        G.queue = g.d_queue + 2;
+        blocks = g.tma_blocks;
+    } else if (edge) {
+        G.map = g.d_edge;
+        G.nmap = g.nedge;
+        G.queue = g.d_queue + 1;
+    } else if (which == KER_TILE_CANON || which == KER_TILE_FUSED) {
         G.map = g.d_items;
         G.nmap = g.nitems;
     } else if (which == KER_STREAM_INTERIOR) {
@@ -1158,7 +1185,7 @@ static void batch_issue(lbm_batch *b, const BatchGroupPlan &g, int which, int q,
         G.map = g.d_gmap;
         G.nmap = g.ngen;
     }
-    launch_batch_group(which, b->storage, G, b->les, g.collision, b->arith, g.tile_blocks, g.stream);
+    launch_batch_group(which, b->storage, G, b->les, g.collision, b->arith, blocks, g.stream);
 }
 
 extern "C" {
@@ -1226,10 +1253,13 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
     }
     cudaError_t e = cudaSuccess;
     std::string where;
+    // LBM_B200_BATCH_TMA=0: the cp.async-staged grid for every interior tile
+    const char *tv = getenv("LBM_B200_BATCH_TMA");
+    const bool tma_on = !(tv && tv[0] == '0');
+    b->tma.assign(n, false);
     for (BatchGroupPlan &g : b->groups) {
         std::vector<long long> col0(1, 0);
-        std::vector<int4> gmap, smap, items;
-        std::vector<int> len;
+        std::vector<int4> gmap, smap, items, edge, inner;
         for (int ld = 0; ld < g.nd; ++ld) {
             const int d = g.d0 + ld;
             lbm_ctx *c = b->ctx[d];
@@ -1245,23 +1275,46 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
                 for (int by = 0; by < ty; ++by)
                     for (int bx = 0; bx < tx; ++bx) smap.push_back(make_int4(ld, bx, by, bz));
             const int nc = (ni + R.chunk - 1) / R.chunk;
+            // tile copies for the tiles off this domain's edge (fused steps with LES)
+            const bool tma = tma_on && b->les && !R.classic && !R.no_tma && tx >= 3 && ty >= 3 &&
+                             19.0 * (double)c->D.n < 2147483647.0 && tile_maps_ready(c);
             for (int cz = 0; cz < nc; ++cz)
                 for (int by = 0; by < ty; ++by)
-                    for (int bx = 0; bx < tx; ++bx) items.push_back(make_int4(ld, bx, by, cz));
+                    for (int bx = 0; bx < tx; ++bx) {
+                        const int4 it = make_int4(ld, bx, by, cz);
+                        items.push_back(it);
+                        if (tma && bx >= 1 && bx <= tx - 2 && by >= 1 && by <= ty - 2) inner.push_back(it);
+                        else edge.push_back(it);
+                    }
+            b->tma[d] = tma;
         }
-        // longest items first: the last items of the queue are the short ones
-        std::stable_sort(items.begin(), items.end(), [&](const int4 &x, const int4 &y) {
-            const Plan &Rx = b->plan[g.d0 + x.x], &Ry = b->plan[g.d0 + y.x];
-            const int px = std::min(Rx.chunk, Rx.zi1 + 1 - (Rx.zi0 + x.w * Rx.chunk));
-            const int py = std::min(Ry.chunk, Ry.zi1 + 1 - (Ry.zi0 + y.w * Ry.chunk));
-            return px > py;
-        });
+        // longest items first: the last items of each queue are the short ones
+        auto longest_first = [&](std::vector<int4> &v) {
+            std::stable_sort(v.begin(), v.end(), [&](const int4 &x, const int4 &y) {
+                const Plan &Rx = b->plan[g.d0 + x.x], &Ry = b->plan[g.d0 + y.x];
+                const int px = std::min(Rx.chunk, Rx.zi1 + 1 - (Rx.zi0 + x.w * Rx.chunk));
+                const int py = std::min(Ry.chunk, Ry.zi1 + 1 - (Ry.zi0 + y.w * Ry.chunk));
+                return px > py;
+            });
+        };
+        g.tma_blocks = inner.empty() ? 0 : batch_tile_blocks(b->storage, b->les, g.collision, b->arith, true);
+        if (g.tma_blocks <= 0) {   // no tile-copy grid: every item on the cp.async grid
+            inner.clear();
+            edge = items;
+            for (int ld = 0; ld < g.nd; ++ld) b->tma[g.d0 + ld] = false;
+        }
+        longest_first(items);
+        longest_first(edge);
+        longest_first(inner);
         g.ngen = (int)gmap.size();
         g.nsi = (int)smap.size();
         g.nitems = (int)items.size();
+        g.nedge = (int)edge.size();
+        g.ninner = (int)inner.size();
         if ((e = upload_vec(&g.d_col0, col0)) != cudaSuccess || (e = upload_vec(&g.d_gmap, gmap)) != cudaSuccess ||
             (e = upload_vec(&g.d_smap, smap)) != cudaSuccess || (e = upload_vec(&g.d_items, items)) != cudaSuccess ||
-            (e = cudaMalloc((void **)&g.d_queue, sizeof(int))) != cudaSuccess ||
+            (e = upload_vec(&g.d_edge, edge)) != cudaSuccess || (e = upload_vec(&g.d_inner, inner)) != cudaSuccess ||
+            (e = cudaMalloc((void **)&g.d_queue, 3 * sizeof(int))) != cudaSuccess ||
             (e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking)) != cudaSuccess ||
             (e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming)) != cudaSuccess) {
             where = "group tables";
@@ -1339,6 +1392,9 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
     for (int d = 0; d < n; ++d) {
         lbm_ctx *c = b->ctx[d];
         c->last_stream = st;
+        // the tensor maps follow the context's population buffers
+        if (b->tma[d] && !tile_maps_ready(c))
+            return batch_fail(b, LBM_ERR_CUDA, "lbm_batch_step: tensor maps of domain " + std::to_string(d));
         const int s = load_bed_slot(c, (int)(n0 & 1), st);
         if (s != LBM_OK) return batch_fail(b, s, c->err);
         for (int q = 0; q < 2; ++q) {
@@ -1388,7 +1444,12 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
                 batch_issue(b, g, KER_COLLIDE_CANON, 0, step, flags);
             } else {
                 if (b->les) batch_issue(b, g, KER_PREPASS_FUSED, q, step, flags);
-                batch_issue(b, g, KER_TILE_FUSED, q, step, flags);
+                if (g.ninner) {
+                    batch_issue(b, g, KER_TILE_FUSED, q, step, flags, true);
+                    batch_issue(b, g, KER_TILE_TMA, q, step, flags);
+                } else {
+                    batch_issue(b, g, KER_TILE_FUSED, q, step, flags);
+                }
                 batch_issue(b, g, KER_COLLIDE_FUSED, q, step, flags);
             }
         }

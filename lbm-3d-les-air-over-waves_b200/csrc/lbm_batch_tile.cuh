@@ -35,6 +35,61 @@ __global__ void __launch_bounds__(256, 2) kb_tile(const __grid_constant__ BatchG
     }
 }
 
+// The fused interior step with LES on the tiles off each domain's edge,
+// staged by tile copies (tile_tma_body), as a work queue of (domain, tile x,
+// tile y, z chunk) items; the tensor maps of the item's domain come from the
+// launch parameters.
+template <int S, class Ar>
+__global__ void __launch_bounds__(256, 2) kb_tile_tma(const __grid_constant__ BatchGroup G) {
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    __shared__ int s_item;
+    for (;;) {
+        __syncthreads();   // every thread is done with the last item's shared memory
+        if (threadIdx.x == 0) s_item = atomicAdd(G.queue, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= G.nmap) break;
+        const int4 it = G.map[item];
+        if (!tile_tma_body<S, Ar>(G.a[it.x], &G.tmap[it.x][0], &G.tmap[it.x][1], tma_smem, it.y * LBM_TILE,
+                                  it.z * LBM_TILE, it.w))
+            break;   // a wait gave up (status bit 2 of the domain)
+    }
+}
+
+template <int S, class Ar>
+static bool batch_tma_ready_t() {
+    static bool done[64] = {false}, ok[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    if (!done[dev]) {
+        done[dev] = true;
+        ok[dev] = cudaFuncSetAttribute(kb_tile_tma<S, Ar>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       tma_smem_bytes<S>()) == cudaSuccess;
+    }
+    return ok[dev];
+}
+
+template <int S, class Ar>
+static int batch_tma_blocks_t() {
+    if (!batch_tma_ready_t<S, Ar>()) return 0;
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kb_tile_tma<S, Ar>, 256, tma_smem_bytes<S>()) !=
+            cudaSuccess)
+        return 0;
+    return per * sms;
+}
+
+template <int S, class Ar>
+static void launch_batch_tma_t(const BatchGroup &G, int tile_blocks, cudaStream_t st) {
+    if (!G.nmap || tile_blocks <= 0 || !batch_tma_ready_t<S, Ar>()) return;
+    cudaMemsetAsync(G.queue, 0, sizeof(int), st);
+    const unsigned g = (unsigned)(tile_blocks < G.nmap ? tile_blocks : G.nmap);
+    kb_tile_tma<S, Ar><<<g, 256, tma_smem_bytes<S>(), st>>>(G);
+    launch_count_add(1);
+}
+
 template <int S, bool LES, class Ar>
 static bool batch_tile_ready_t() {
     static bool done[64] = {false}, ok[64] = {false};
@@ -74,9 +129,18 @@ static void launch_batch_tile_t(int which, const BatchGroup &G, int tile_blocks,
 }
 
 // dispatch on the storage and the LES switch for one arithmetic policy
+// (KER_TILE_TMA: the tile-copy grid, LES on)
 template <class Ar>
 static void launch_batch_tile_any(int which, int storage, const BatchGroup &G, bool les, int tile_blocks,
                                   cudaStream_t st) {
+    if (which == KER_TILE_TMA) {
+        switch (storage) {
+            case LBM_STORE_F16S: launch_batch_tma_t<LBM_STORE_F16S, Ar>(G, tile_blocks, st); break;
+            case LBM_STORE_BF16S: launch_batch_tma_t<LBM_STORE_BF16S, Ar>(G, tile_blocks, st); break;
+            default: launch_batch_tma_t<LBM_STORE_F32, Ar>(G, tile_blocks, st); break;
+        }
+        return;
+    }
     switch (storage) {
         case LBM_STORE_F16S:
             if (les) launch_batch_tile_t<LBM_STORE_F16S, true, Ar>(which, G, tile_blocks, st);
@@ -93,7 +157,14 @@ static void launch_batch_tile_any(int which, int storage, const BatchGroup &G, b
     }
 }
 template <class Ar>
-static int batch_tile_blocks_any(int storage, bool les) {
+static int batch_tile_blocks_any(int storage, bool les, bool tma = false) {
+    if (tma) {
+        switch (storage) {
+            case LBM_STORE_F16S: return batch_tma_blocks_t<LBM_STORE_F16S, Ar>();
+            case LBM_STORE_BF16S: return batch_tma_blocks_t<LBM_STORE_BF16S, Ar>();
+            default: return batch_tma_blocks_t<LBM_STORE_F32, Ar>();
+        }
+    }
     switch (storage) {
         case LBM_STORE_F16S:
             return les ? batch_tile_blocks_t<LBM_STORE_F16S, true, Ar>() : batch_tile_blocks_t<LBM_STORE_F16S, false, Ar>();

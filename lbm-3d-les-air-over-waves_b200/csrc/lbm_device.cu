@@ -219,8 +219,9 @@ __device__ __forceinline__ void store_cell(const StepArgs &A, int c, const float
 // Stream-stage class of a water cell on the height path: 1 = gas cell,
 // 2 = cell whose sources are all wet, 0 = anything else; in classes 1 and 2
 // the cell is away from the bed (its link endpoints are more than half a
-// cell above the 3x3 bed maximum), away from the top and bottom rows, and
-// there is no cube, phi geometry, fringe or top drive, so stream_bc gives:
+// cell above the 3x3 bed maximum), above the bottom row, below the top row
+// (class 2), and there is no cube, phi geometry, fringe or top drive, so
+// stream_bc gives:
 // the rest equilibrium (gas) or the plain gather (wet sources) on every
 // link, except the links through a solid x wall, which carry the cell's own
 // opposite population.  Wet sources: the lowest free-surface height over
@@ -230,7 +231,7 @@ __device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int 
     const lbm_params &P = A.P;
     const Dom &D = A.D;
     if (P.fs_mode == LBM_FS_NONE || (A.flags & F_VOF_STATE)) return 0;
-    if (k < 1 || k > D.nz - 2) return 0;
+    if (k < 1 || k > D.nz - 1) return 0;
     if (P.enable_x_fringe || P.enable_top_drive || P.include_cube || P.use_phi_open_fraction ||
         P.use_phi_open_flags)
         return 0;
@@ -244,7 +245,8 @@ __device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int 
     int type;
     float fill;
     classify_height(P, __ldg(A.fs_h + D.col(j, i)), k, true, type, fill);
-    if (type == LBM_FS_GAS) return 1;
+    if (type == LBM_FS_GAS) return 1;   // the top row too: stream_bc gives a gas cell the rest equilibrium
+    if (k == D.nz - 1) return 0;
     int im = i == 0 ? D.nx - 1 : i - 1, ip = i + 1 == D.nx ? 0 : i + 1;
     if (P.x_solid) {
         if (i == 0) im = i;
@@ -259,16 +261,16 @@ __device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int 
     return hmin > ((float)k + 1.01f) * dx ? 2 : 0;
 }
 
-// Height-path water cell whose collide needs no link geometry: inside the
-// domain's z range, farther than half a cell from the bed, no cube, phi
-// geometry, fringe or top drive.  Its own link (q = 0) is open, and every
-// closed link is an x wall, where the water path's condition stage applies
-// nothing (only bed links, or any link in air physics, are conditioned).
+// Height-path water cell whose collide needs no link geometry: farther than
+// half a cell from the bed, no cube, phi geometry, fringe or top drive (the
+// top and bottom rows included: the domain's z ends close no link).  Its own
+// link (q = 0) is open, and every closed link is an x wall, where the water
+// path's condition stage applies nothing (only bed links, or any link in
+// air physics, are conditioned).
 __device__ __forceinline__ bool water_collide_local(const StepArgs &A, int k, int j, int i) {
     const lbm_params &P = A.P;
     const Dom &D = A.D;
     if (P.fs_mode == LBM_FS_NONE || (A.flags & F_VOF_STATE) || !P.physics_water) return false;
-    if (k < 1 || k > D.nz - 2) return false;
     if (P.enable_x_fringe || P.enable_top_drive || P.include_cube || P.use_phi_open_fraction ||
         P.use_phi_open_flags)
         return false;
@@ -1638,9 +1640,9 @@ void launch_batch_bed(const BatchLaunch &L, long long m, cudaStream_t st) {
     kb_colgeo<<<blocks_for((size_t)L.ncols, 128), 128, 0, st>>>(L, par); LAUNCHED(1);
 }
 
-int batch_tile_blocks(int storage, bool les, int collision, int arith) {
-    if (arith == LBM_ARITH_FAST) return batch_tile_blocks_fast(storage, les, collision);
-    return batch_tile_blocks_any<ArExact>(storage, les);
+int batch_tile_blocks(int storage, bool les, int collision, int arith, bool tma) {
+    if (arith == LBM_ARITH_FAST) return batch_tile_blocks_fast(storage, les, collision, tma);
+    return batch_tile_blocks_any<ArExact>(storage, les, tma);
 }
 
 template <int S>
@@ -1660,7 +1662,7 @@ static void launch_batch_group_s(int which, const BatchGroup &G, cudaStream_t st
 }
 void launch_batch_group(int which, int storage, const BatchGroup &G, bool les, int collision, int arith,
                         int tile_blocks, cudaStream_t st) {
-    if (which == KER_TILE_CANON || which == KER_TILE_FUSED) {
+    if (which == KER_TILE_CANON || which == KER_TILE_FUSED || which == KER_TILE_TMA) {
         if (arith == LBM_ARITH_FAST) launch_batch_tile_fast(which, storage, G, les, collision, tile_blocks, st);
         else launch_batch_tile_any<ArExact>(which, storage, G, les, tile_blocks, st);
         return;

@@ -37,9 +37,9 @@ void launch_batch_tile_fast(int which, int storage, const BatchGroup &G, bool le
         launch_batch_tile_any<ArFast<LBM_COLLIDE_REGULARIZED>>(which, storage, G, les, tile_blocks, st);
 }
 
-int batch_tile_blocks_fast(int storage, bool les, int collision) {
-    if (collision == LBM_COLLIDE_KBC) return batch_tile_blocks_any<ArFast<LBM_COLLIDE_KBC>>(storage, les);
-    return batch_tile_blocks_any<ArFast<LBM_COLLIDE_REGULARIZED>>(storage, les);
+int batch_tile_blocks_fast(int storage, bool les, int collision, bool tma) {
+    if (collision == LBM_COLLIDE_KBC) return batch_tile_blocks_any<ArFast<LBM_COLLIDE_KBC>>(storage, les, tma);
+    return batch_tile_blocks_any<ArFast<LBM_COLLIDE_REGULARIZED>>(storage, les, tma);
 }
 
 }  // namespace lbm

@@ -23,7 +23,8 @@ enum : int {
 
 enum {
     KER_PREPASS_CANON = 0, KER_PREPASS_FUSED = 1, KER_COLLIDE_CANON = 2, KER_COLLIDE_FUSED = 3, KER_STREAM = 4,
-    KER_TILE_CANON = 5, KER_TILE_FUSED = 6, KER_STREAM_INTERIOR = 7, KER_WATER_COLLIDE = 8, KER_WATER_STREAM = 9
+    KER_TILE_CANON = 5, KER_TILE_FUSED = 6, KER_STREAM_INTERIOR = 7, KER_WATER_COLLIDE = 8, KER_WATER_STREAM = 9,
+    KER_TILE_TMA = 10   // ensembles: the fused interior step with LES on the tiles off the domain edge, tile copies
 };
 // device counters of a context (int slots)
 enum { CNT_CUT = 0, CNT_FSCUT = 1, CNT_BRIDGE = 2, CNT_FS_REFILL = 3, CNT_COALESCE = 4, CNT_VOF_EXCESS = 5,
@@ -207,33 +208,35 @@ struct BatchLaunch {
     int ndom;
     long long ncols;
 };
-// Domains per launch of the step grids.  Their step arguments travel in the
-// kernel's parameter space (read-only, at most 32,764 bytes), so that the
-// shared bodies read them, indexed by the block's domain, as a domain's own
-// kernel reads its argument, without copies to shared memory or registers.
-constexpr int BATCH_GROUP = 36;
+// Domains per launch of the step grids.  Their step arguments and the
+// tensor maps of their source populations travel in the kernel's parameter
+// space (read-only, at most 32,764 bytes), so that the shared bodies read
+// them, indexed by the block's domain, as a domain's own kernel reads its
+// arguments, without copies to shared memory or registers.
+constexpr int BATCH_GROUP = 28;
 struct BatchGroup {
-    const int4 *map;                 // general / stream blocks: (domain, bx, by, bz); interior grid: work
+    CUtensorMap tmap[BATCH_GROUP][2];  // interior tile-copy grid: boxes 24 and 20 wide (one map for 16-bit storage)
+    const int4 *map;                 // general / stream blocks: (domain, bx, by, bz); interior grids: work
                                      // items (domain, tile x, tile y, z chunk); domain = index in a[]
     int nmap;
     int ndom;
-    int *queue;                      // interior grid: next work item
+    int *queue;                      // interior grids: next work item
     StepArgs a[BATCH_GROUP];         // step arguments of the launch (step number and flags included)
 };
 static_assert(sizeof(BatchGroup) <= 32764, "kernel parameter space");
 
 // bed, 3x3 maximum and column cache of the group's domains at step m
 void launch_batch_bed(const BatchLaunch &L, long long m, cudaStream_t st);
-// one phase over one group (which = KER_PREPASS_*, KER_TILE_*, KER_COLLIDE_*, KER_STREAM, KER_STREAM_INTERIOR);
-// the group's domains share storage, LES and collision model; arith: the interior planes' policy (LBM_ARITH_*);
-// tile_blocks: resident blocks of the interior grid
+// one phase over one group (which = KER_PREPASS_*, KER_TILE_*, KER_TILE_TMA, KER_COLLIDE_*, KER_STREAM,
+// KER_STREAM_INTERIOR); the group's domains share storage, LES and collision model; arith: the interior
+// planes' policy (LBM_ARITH_*); tile_blocks: resident blocks of the interior grid
 void launch_batch_group(int which, int storage, const BatchGroup &G, bool les, int collision, int arith,
                         int tile_blocks, cudaStream_t st);
-// resident blocks of the interior grid on this device (0: the shared memory is refused)
-int batch_tile_blocks(int storage, bool les, int collision, int arith);
-// the fast-arithmetic interior grid of a group (lbm_fast.cu)
+// resident blocks of the interior grid (tma: the tile-copy grid) on this device (0: the shared memory is refused)
+int batch_tile_blocks(int storage, bool les, int collision, int arith, bool tma = false);
+// the fast-arithmetic interior grids of a group (lbm_fast.cu)
 void launch_batch_tile_fast(int which, int storage, const BatchGroup &G, bool les, int collision, int tile_blocks,
                             cudaStream_t st);
-int batch_tile_blocks_fast(int storage, bool les, int collision);
+int batch_tile_blocks_fast(int storage, bool les, int collision, bool tma);
 
 }  // namespace lbm

@@ -742,12 +742,20 @@ LBM_DEV void tma_load_4d(unsigned dst, const CUtensorMap *map, int x, int y, int
         : "memory");
 }
 
-template <int S, class Ar = ArExact>
-__global__ void __launch_bounds__(256, 2)
-    k_tile_tma(StepArgs A, const __grid_constant__ CUtensorMap m24, const __grid_constant__ CUtensorMap m20) {
+LBM_DEV void mbar_inval(unsigned bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+
+// One tile (x0, y0) and z chunk bz of the fused interior step staged by tile
+// copies (the body of k_tile_tma, also run per work item by the ensemble's
+// kb_tile_tma).  m24 / m20: tensor maps of the source populations (kernel
+// parameters).  false: a wait gave up (status bit 2 set, the block's copies
+// in flight waited for); the caller leaves.
+template <int S, class Ar>
+LBM_DEV bool tile_tma_body(const StepArgs &A, const CUtensorMap *m24, const CUtensorMap *m20,
+                           unsigned char *tma_smem, int x0, int y0, int bz) {
     typedef TmaTile<S> L;
     typedef typename L::T T;
-    extern __shared__ __align__(128) unsigned char tma_smem[];
     T *sf = (T *)(tma_smem + ((128u - (smem_addr(tma_smem) & 127u)) & 127u));   // [slot][L::SLOT]
     float (*su)[3][LBM_TILE + 2][LBM_TILE + 2] =        // [plane slot][component][x][y]
         (float (*)[3][LBM_TILE + 2][LBM_TILE + 2])(sf + PIPE_SLOTS * L::SLOT);
@@ -755,9 +763,8 @@ __global__ void __launch_bounds__(256, 2)
     const lbm_params &P = A.P;
     const Dom &D = A.D;
     const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-    const int x0 = (blockIdx.x + 1) * LBM_TILE, y0 = (blockIdx.y + 1) * LBM_TILE;   // tiles off the domain edge
     const int i = x0 + tx, j = y0 + ty;
-    const int z0 = A.zi0 + blockIdx.z * A.chunk;
+    const int z0 = A.zi0 + bz * A.chunk;
     const int z1 = min(z0 + A.chunk, A.zi1 + 1);  // planes [z0, z1) are collided here
     const int n = (int)D.n, nxy = D.nx * D.ny;
     T *fdst = (T *)A.fdst;
@@ -792,7 +799,7 @@ __global__ void __launch_bounds__(256, 2)
             const unsigned b = smem_addr(bar + slot);
             if (t == 0) mbar_expect_tx(b, L::BYTES);
             for (int q = t >> 5; q < 19; q += 8) {
-                tma_load_4d(smem_addr(sf + slot * L::SLOT + L::base(q)), L::wide(q) ? &m24 : &m20,
+                tma_load_4d(smem_addr(sf + slot * L::SLOT + L::base(q)), L::wide(q) ? m24 : m20,
                             L::x_start(x0, cxq(q)), y0 - 1 - cyq(q), p - czq(q), q, b);
             }
         }
@@ -833,8 +840,7 @@ __global__ void __launch_bounds__(256, 2)
             const unsigned b = smem_addr(bar + sl);
             for (int it = 0; it < TMA_WAIT_LIMIT && !mbar_try_wait(b, (phase >> sl) & 1u); ++it) {
             }
-            asm volatile("griddepcontrol.wait;\n" ::: "memory");
-            return;
+            return false;
         }
         if (interior) phase ^= 1u << sl;
         issue(p + 1);
@@ -912,6 +918,21 @@ __global__ void __launch_bounds__(256, 2)
         }
         rp = r;
     }
+    // every copy has been waited for: retire the barriers before the shared
+    // memory is used again (the next work item of a queue)
+    __syncthreads();
+    if (t == 0)
+        for (int s = 0; s < PIPE_SLOTS; ++s) mbar_inval(smem_addr(bar + s));
+    return true;
+}
+
+template <int S, class Ar = ArExact>
+__global__ void __launch_bounds__(256, 2)
+    k_tile_tma(StepArgs A, const __grid_constant__ CUtensorMap m24, const __grid_constant__ CUtensorMap m20) {
+    extern __shared__ __align__(128) unsigned char tma_smem[];
+    // tiles off the domain edge
+    tile_tma_body<S, Ar>(A, &m24, &m20, tma_smem, (blockIdx.x + 1) * LBM_TILE, (blockIdx.y + 1) * LBM_TILE,
+                         blockIdx.z);
     // complete only after the edge-tile grid this one was launched behind,
     // so that the work after it sees both grids' results
     asm volatile("griddepcontrol.wait;\n" ::: "memory");

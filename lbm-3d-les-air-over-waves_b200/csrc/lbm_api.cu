@@ -591,12 +591,15 @@ static int step_vof(lbm_ctx *ctx, int K, cudaStream_t st) {
             launch_step_kernel(KER_PREPASS_CANON, A, st);
             CK_LAUNCH("prepass");
         }
+        A.flags |= F_WATER_SPLIT;   // compact kernels for the cells with local collide / plain-gather stream
+        launch_step_kernel(KER_WATER_COLLIDE, A, st);
         launch_step_kernel(KER_COLLIDE_CANON, A, st);
         CK_LAUNCH("collide");
         CK(cudaMemsetAsync(ctx->dcount, 0, 4 * sizeof(int), st), "counter reset");
         A.fsrc = ctx->b.f[1 - ctx->cur];
         A.fdst = ctx->b.f[ctx->cur];
-        A.flags = F_COUNT | F_VOF_STATE;
+        A.flags = F_COUNT | F_VOF_STATE | F_WATER_SPLIT;
+        launch_step_kernel(KER_WATER_STREAM, A, st);
         launch_step_kernel(KER_STREAM, A, st);
         CK_LAUNCH("stream");
         const bool due = ctx->P.vof_collapse_enabled && (m % ctx->P.vof_collapse_interval) == 0;

@@ -227,10 +227,12 @@ __device__ __forceinline__ void store_cell(const StepArgs &A, int c, const float
 // opposite population.  Wet sources: the lowest free-surface height over
 // the 3x3 columns is more than 1.01 cells above the top source plane's
 // bottom, so every source fill exceeds 1e-4.
+__device__ __forceinline__ int vof_stream_class(const StepArgs &A, int k, int j, int i);
 __device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int j, int i) {
     const lbm_params &P = A.P;
     const Dom &D = A.D;
-    if (P.fs_mode == LBM_FS_NONE || (A.flags & F_VOF_STATE)) return 0;
+    if (P.fs_mode == LBM_FS_NONE) return 0;
+    if (A.flags & F_VOF_STATE) return vof_stream_class(A, k, j, i);
     if (k < 1 || k > D.nz - 1) return 0;
     if (P.enable_x_fringe || P.enable_top_drive || P.include_cube || P.use_phi_open_fraction ||
         P.use_phi_open_flags)
@@ -261,7 +263,41 @@ __device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int 
     return hmin > ((float)k + 1.01f) * dx ? 2 : 0;
 }
 
-// Height-path water cell whose collide needs no link geometry: farther than
+// The same classes on the VOF path, from the stored cell types, away from
+// solid x walls: 1 = open gas cell (stream_bc gives the rest equilibrium and
+// no wall bounce-back), 2 = liquid cell below the top row whose 18 sources
+// are liquid (every link takes the plain gather: no free-surface link, link
+// aperture 1), 0 = anything else.
+__device__ __forceinline__ int vof_stream_class(const StepArgs &A, int k, int j, int i) {
+    const lbm_params &P = A.P;
+    const Dom &D = A.D;
+    if (k < 1 || k > D.nz - 1) return 0;
+    if (P.x_solid && (i == 0 || i == D.nx - 1)) return 0;
+    if (P.enable_x_fringe || P.enable_top_drive || P.include_cube || P.use_phi_open_fraction ||
+        P.use_phi_open_flags)
+        return 0;
+    const float dx = P.dx, hdx = 0.5f * dx;
+    if (P.include_bed) {
+        const float zc = ((float)k + 0.5f) * dx;
+        const float hm = __ldg(A.bed_s.hmax + D.col(j, i));
+        const float margin = 1e-4f * dx + 1e-6f * (fabsf(zc) + fabsf(hm));
+        if (!((zc - hdx) - hm >= hdx + margin)) return 0;
+    }
+    const int type = A.fs_type[D.cell(k, j, i)];
+    if (type == LBM_FS_GAS) return 1;
+    if (type != LBM_FS_LIQUID || k == D.nz - 1) return 0;
+    const int im = i == 0 ? D.nx - 1 : i - 1, ip = i + 1 == D.nx ? 0 : i + 1;
+    const int jm = j == 0 ? D.ny - 1 : j - 1, jp = j + 1 == D.ny ? 0 : j + 1;
+#pragma unroll
+    for (int q = 1; q < 19; ++q) {
+        const int si = cxq(q) > 0 ? im : (cxq(q) < 0 ? ip : i);
+        const int sj = cyq(q) > 0 ? jm : (cyq(q) < 0 ? jp : j);
+        if (A.fs_type[D.cell(k - czq(q), sj, si)] != LBM_FS_LIQUID) return 0;
+    }
+    return 2;
+}
+
+// Water cell (height or VOF path) whose collide needs no link geometry: farther than
 // half a cell from the bed, no cube, phi geometry, fringe or top drive (the
 // top and bottom rows included: the domain's z ends close no link).  Its own
 // link (q = 0) is open, and every closed link is an x wall, where the water
@@ -270,7 +306,7 @@ __device__ __forceinline__ int water_stream_class(const StepArgs &A, int k, int 
 __device__ __forceinline__ bool water_collide_local(const StepArgs &A, int k, int j, int i) {
     const lbm_params &P = A.P;
     const Dom &D = A.D;
-    if (P.fs_mode == LBM_FS_NONE || (A.flags & F_VOF_STATE) || !P.physics_water) return false;
+    if (P.fs_mode == LBM_FS_NONE || !P.physics_water) return false;
     if (P.enable_x_fringe || P.enable_top_drive || P.include_cube || P.use_phi_open_fraction ||
         P.use_phi_open_flags)
         return false;

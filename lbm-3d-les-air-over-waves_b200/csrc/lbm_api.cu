@@ -81,6 +81,7 @@ struct lbm_ctx {
     int8_t *v_open = nullptr, *v_t0 = nullptr, *v_ba = nullptr;
     float *v_lf0 = nullptr, *v_m0 = nullptr, *v_x0 = nullptr, *v_fa = nullptr;
     double *v_dd = nullptr, *v_tree = nullptr;
+    uint8_t *v_near = nullptr;   // coarse donor-in-reach flags of the VOF receiver passes
     int *v_dist = nullptr;
     float *u_les = nullptr;
     int *dcount = nullptr;
@@ -105,6 +106,7 @@ struct lbm_ctx {
     long long *dclock = nullptr;
     float *stash = nullptr;     // FP32 post-condition populations of the general planes (16-bit storage)
     size_t stash_cells = 0;
+    int *wlist = nullptr;       // water stream: the cells of the general path ([n]) and their count ([n])
     std::vector<StepGraph> graph_cache;
     // scratch of lbm_diagnostics (allocated by its first call)
     DiagCellPart *d_cellp = nullptr;
@@ -236,6 +238,11 @@ static VofArgs vof_args(lbm_ctx *ctx, int slot, void *f) {
     V.m0 = ctx->v_m0; V.x0 = ctx->v_x0; V.t0 = ctx->v_t0;
     V.fa = ctx->v_fa; V.ba = ctx->v_ba; V.dd = ctx->v_dd;
     V.dist = ctx->v_dist;
+    V.near = ctx->v_near;
+    V.cbx = (ctx->D.nx + VOF_CB - 1) / VOF_CB;
+    V.cby = (ctx->D.ny + VOF_CB - 1) / VOF_CB;
+    V.cbz = (ctx->D.nz + VOF_CB - 1) / VOF_CB;
+    V.near_ok = ctx->v_near && ctx->D.ny % VOF_CB == 0 && (ctx->P.x_solid || ctx->D.nx % VOF_CB == 0);
     V.count = ctx->dcount;
     V.fcount = ctx->dfcount;
     return V;
@@ -517,9 +524,16 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     return LBM_OK;
 }
 
+// the list of the water stream's general cells (one int per cell and a count)
+static int water_list(lbm_ctx *ctx, cudaStream_t st) {
+    if (ctx->wlist) return LBM_OK;
+    return alloc(ctx, (void **)&ctx->wlist, ((size_t)ctx->D.n + 1) * sizeof(int), st);
+}
+
 static int step_height(lbm_ctx *ctx, int K, cudaStream_t st) {
     const bool les = ctx->P.use_les != 0;
     int s;
+    if ((s = water_list(ctx, st)) != LBM_OK) return s;
     for (int it = 0; it < K; ++it) {
         int64_t m = ctx->nstep + 1;
         if ((s = bed_step(ctx, m, st)) != LBM_OK) return s;
@@ -545,9 +559,8 @@ static int step_height(lbm_ctx *ctx, int K, cudaStream_t st) {
         CK(cudaMemsetAsync(ctx->dcount, 0, 4 * sizeof(int), st), "counter reset");
         A.fsrc = ctx->b.f[1 - ctx->cur];
         A.fdst = ctx->b.f[ctx->cur];
-        A.flags = F_COUNT | F_WATER_SPLIT;
-        launch_step_kernel(KER_WATER_STREAM, A, st);
-        launch_step_kernel(KER_STREAM, A, st);
+        A.flags = F_COUNT;
+        launch_water_stream(A, ctx->wlist, ctx->wlist + ctx->D.n, st);
         CK_LAUNCH("stream");
         launch_column_flux(A, ctx->b.fs_flux_x, ctx->b.fs_flux_y, st);
         CK_LAUNCH("column flux");
@@ -571,6 +584,7 @@ static int step_height(lbm_ctx *ctx, int K, cudaStream_t st) {
 static int step_vof(lbm_ctx *ctx, int K, cudaStream_t st) {
     const bool les = ctx->P.use_les != 0;
     int s;
+    if ((s = water_list(ctx, st)) != LBM_OK) return s;
     for (int it = 0; it < K; ++it) {
         int64_t m = ctx->nstep + 1;
         if ((s = bed_step(ctx, m, st)) != LBM_OK) return s;
@@ -598,9 +612,8 @@ static int step_vof(lbm_ctx *ctx, int K, cudaStream_t st) {
         CK(cudaMemsetAsync(ctx->dcount, 0, 4 * sizeof(int), st), "counter reset");
         A.fsrc = ctx->b.f[1 - ctx->cur];
         A.fdst = ctx->b.f[ctx->cur];
-        A.flags = F_COUNT | F_VOF_STATE | F_WATER_SPLIT;
-        launch_step_kernel(KER_WATER_STREAM, A, st);
-        launch_step_kernel(KER_STREAM, A, st);
+        A.flags = F_COUNT | F_VOF_STATE;
+        launch_water_stream(A, ctx->wlist, ctx->wlist + ctx->D.n, st);
         CK_LAUNCH("stream");
         const bool due = ctx->P.vof_collapse_enabled && (m % ctx->P.vof_collapse_interval) == 0;
         CK(vof_sequence(V, due, ctx->v_tree, st), "vof sequence");
@@ -696,7 +709,8 @@ int lbm_bind(lbm_ctx *ctx, const lbm_buffers *bufs) {
                 (s = alloc(ctx, (void **)&ctx->v_ba, 2 * n)) || (s = alloc(ctx, (void **)&ctx->v_lf0, 4 * n)) ||
                 (s = alloc(ctx, (void **)&ctx->v_m0, 4 * n)) || (s = alloc(ctx, (void **)&ctx->v_x0, 4 * n)) ||
                 (s = alloc(ctx, (void **)&ctx->v_fa, 24 * n)) || (s = alloc(ctx, (void **)&ctx->v_dd, 8 * n)) ||
-                (s = alloc(ctx, (void **)&ctx->v_tree, 8 * nt)) || (s = alloc(ctx, (void **)&ctx->v_dist, 4 * n)))
+                (s = alloc(ctx, (void **)&ctx->v_tree, 8 * nt)) || (s = alloc(ctx, (void **)&ctx->v_dist, 4 * n)) ||
+                (s = alloc(ctx, (void **)&ctx->v_near, vof_near_bytes(ctx->D))))
                 return s;
             CK(cudaMemset(ctx->v_dist, 0xff, 4 * n), "memset");
         }

@@ -478,15 +478,11 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collid
 }
 
 template <int S, bool CG>
-__device__ __forceinline__ void stream_body(const StepArgs &A, int bx, int by, int bz) {
-    int i, j, k, c;
-    int cut = 0, fscut = 0, bridge = 0;
-    if (cell_xyz(A, bx, by, bz, i, j, k, c)) {
+__device__ __forceinline__ void stream_cell(const StepArgs &A, int k, int j, int i, int c, int wcls, int &cut,
+                                            int &fscut, int &bridge) {
+    {
         float f[19];
-        const int wcls = CG ? 0 : water_stream_class(A, k, j, i);
-        if (!CG && wcls != 0 && (A.flags & F_WATER_SPLIT)) {
-            // k_stream_water
-        } else if (cell_fast(A, true, false, k, j, i)) {
+        if (cell_fast(A, true, false, k, j, i)) {
             stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
             store_cell<S>(A, c, f);
         } else if (wcls != 0) {
@@ -547,6 +543,10 @@ __device__ __forceinline__ void stream_body(const StepArgs &A, int bx, int by, i
             }
         }
     }
+}
+
+// the stream counters of a warp (cut, free-surface cut, bridge links)
+__device__ __forceinline__ void stream_counts(const StepArgs &A, int cut, int fscut, int bridge) {
     if (A.flags & F_COUNT) {
         unsigned m = __activemask();
         int s0 = __reduce_add_sync(m, cut), s1 = __reduce_add_sync(m, fscut), s2 = __reduce_add_sync(m, bridge);
@@ -556,6 +556,18 @@ __device__ __forceinline__ void stream_body(const StepArgs &A, int bx, int by, i
             if (s2) atomicAdd(A.counters + 2, s2);
         }
     }
+}
+
+template <int S, bool CG>
+__device__ __forceinline__ void stream_body(const StepArgs &A, int bx, int by, int bz) {
+    int i, j, k, c;
+    int cut = 0, fscut = 0, bridge = 0;
+    if (cell_xyz(A, bx, by, bz, i, j, k, c)) {
+        const int wcls = CG ? 0 : water_stream_class(A, k, j, i);
+        if (CG || wcls == 0 || !(A.flags & F_WATER_SPLIT))   // else: k_stream_water
+            stream_cell<S, CG>(A, k, j, i, c, wcls, cut, fscut, bridge);
+    }
+    stream_counts(A, cut, fscut, bridge);
 }
 template <int S, bool CG>
 __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream(StepArgs A) {
@@ -609,12 +621,16 @@ __global__ void __launch_bounds__(256, 2) k_collide_water(StepArgs A) {
     store_cell<S>(A, c, f);
 }
 
+// list / count: the cells left to the general path are appended (one
+// warp-aggregated atomic per warp), for k_stream_list
 template <int S>
-__global__ void __launch_bounds__(256, 2) k_stream_water(StepArgs A) {
+__global__ void __launch_bounds__(256, 2) k_stream_water(StepArgs A, int *list, int *count) {
     int i, j, k, c;
     int cut = 0;
+    bool general = false;
     if (cell_xyz(A, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k, c)) {
         const int wcls = water_stream_class(A, k, j, i);
+        general = wcls == 0;
         if (wcls != 0) {
             // the water branch of stream_body: a gas cell takes the rest
             // equilibrium, a cell whose sources are all wet the plain gather
@@ -657,10 +673,32 @@ __global__ void __launch_bounds__(256, 2) k_stream_water(StepArgs A) {
             A.rho[c] = r; A.ux[c] = vx; A.uy[c] = vy; A.uz[c] = vz;
         }
     }
+    const unsigned lanes = __ballot_sync(0xffffffffu, general);
+    if (lanes) {
+        const int lane = threadIdx.x & 31, lead = __ffs(lanes) - 1;
+        int base = 0;
+        if (lane == lead) base = atomicAdd(count, __popc(lanes));
+        base = __shfl_sync(0xffffffffu, base, lead);
+        if (general) list[base + __popc(lanes & ((1u << lane) - 1u))] = c;
+    }
     if (A.flags & F_COUNT) {
         const int s0 = __reduce_add_sync(0xffffffffu, cut);
         if ((threadIdx.x & 31) == 0 && s0) atomicAdd(A.counters + 0, s0);
     }
+}
+
+// the general stream over the cells k_stream_water left (grid-stride over the list)
+template <int S>
+__global__ void __launch_bounds__(256, LBM_GEN_MINB) k_stream_list(StepArgs A, const int *list, const int *count) {
+    const int nl = *count;
+    int cut = 0, fscut = 0, bridge = 0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nl; e += gridDim.x * blockDim.x) {
+        const int c = list[e];
+        int k, j, i;
+        cell_of(A.D, c, k, j, i);
+        stream_cell<S, false>(A, k, j, i, c, 0, cut, fscut, bridge);
+    }
+    stream_counts(A, cut, fscut, bridge);
 }
 
 }  // namespace lbm
@@ -1402,10 +1440,7 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
             else k_collide_water<S, LBM_COLLIDE_REGULARIZED><<<g, kBlock3, 0, st>>>(A);
             LAUNCHED(1);
             break;
-        case KER_WATER_STREAM:
-            k_stream_water<S><<<g, kBlock3, 0, st>>>(A);
-            LAUNCHED(1);
-            break;
+
         case KER_TILE_CANON:
             if constexpr (S != LBM_STORE_F32) {
                 if (pipe16) {
@@ -1451,6 +1486,24 @@ void launch_step_kernel(int which, const StepArgs &A, cudaStream_t st) {
         case LBM_STORE_F16S: launch_step_kernel_s<LBM_STORE_F16S>(which, A, st); break;
         case LBM_STORE_BF16S: launch_step_kernel_s<LBM_STORE_BF16S>(which, A, st); break;
         default: launch_step_kernel_s<LBM_STORE_F32>(which, A, st); break;
+    }
+}
+template <int S>
+static void launch_water_stream_s(const StepArgs &A, int *list, int *count, cudaStream_t st) {
+    const dim3 g = grid3(A);
+    if (g.z == 0) return;
+    cudaMemsetAsync(count, 0, sizeof(int), st);
+    k_stream_water<S><<<g, kBlock3, 0, st>>>(A, list, count);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_stream_list<S><<<(unsigned)(sms * LBM_GEN_MINB), 256, 0, st>>>(A, list, count);
+    LAUNCHED(2);
+}
+void launch_water_stream(const StepArgs &A, int *list, int *count, cudaStream_t st) {
+    switch (A.P.pop_storage) {
+        case LBM_STORE_F16S: launch_water_stream_s<LBM_STORE_F16S>(A, list, count, st); break;
+        case LBM_STORE_BF16S: launch_water_stream_s<LBM_STORE_BF16S>(A, list, count, st); break;
+        default: launch_water_stream_s<LBM_STORE_F32>(A, list, count, st); break;
     }
 }
 void launch_column_flux(const StepArgs &A, float *qx, float *qy, cudaStream_t st) {
@@ -1560,6 +1613,7 @@ static cudaError_t vof_snapshot(const VofArgs &V, const float *a, float *a0, con
 static cudaError_t vof_redistribute(const VofArgs &V, cudaStream_t st) {
     cudaError_t e = vof_snapshot(V, V.mass, V.m0, V.mass_excess, V.x0, false, st);
     if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(V.near, 0, vof_near_bytes(V.D), st)) != cudaSuccess) return e;
     k_vof_redist_donor<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
     k_vof_redist_recv<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
     return cudaGetLastError();
@@ -1601,6 +1655,7 @@ cudaError_t vof_sequence(const VofArgs &V, bool collapse_due, double *tree, cuda
     if ((e = vof_interface_layer(V, st)) != cudaSuccess) return e;
     // orphans: snapshots of mass, fill and type
     if ((e = vof_snapshot(V, V.mass, V.m0, V.fill, V.x0, true, st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(V.near, 0, vof_near_bytes(V.D), st)) != cudaSuccess) return e;
     k_vof_orphan_donor<<<vblocks(V), 256, 0, st>>>(V, cnt + CNT_ORPHAN); LAUNCHED(1);
     k_vof_orphan_recv<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
     double *ping = tree, *pong = tree + (n / 256 + 2);

@@ -23,7 +23,7 @@ enum : int {
 
 enum {
     KER_PREPASS_CANON = 0, KER_PREPASS_FUSED = 1, KER_COLLIDE_CANON = 2, KER_COLLIDE_FUSED = 3, KER_STREAM = 4,
-    KER_TILE_CANON = 5, KER_TILE_FUSED = 6, KER_STREAM_INTERIOR = 7, KER_WATER_COLLIDE = 8, KER_WATER_STREAM = 9,
+    KER_TILE_CANON = 5, KER_TILE_FUSED = 6, KER_STREAM_INTERIOR = 7, KER_WATER_COLLIDE = 8,
     KER_TILE_TMA = 10   // ensembles: the fused interior step with LES on the tiles off the domain edge, tile copies
 };
 // device counters of a context (int slots)
@@ -74,6 +74,12 @@ struct InitArgs {
     int8_t *fs_type, *fs_type_prev, *fs_excess_dir;
 };
 
+// edge of the coarse blocks of the VOF receivers' donor-in-reach flags
+constexpr int VOF_CB = 4;
+inline size_t vof_near_bytes(const Dom &D) {
+    return (size_t)((D.nx + VOF_CB - 1) / VOF_CB) * ((D.ny + VOF_CB - 1) / VOF_CB) * ((D.nz + VOF_CB - 1) / VOF_CB);
+}
+
 // state and scratch of the VOF kernels
 struct VofArgs {
     lbm_params P;
@@ -93,6 +99,9 @@ struct VofArgs {
     int8_t *ba;                       // 2 n bytes
     double *dd;                       // n doubles
     int *dist;                        // flood-fill distance of the last collapse pass (-1: not reached)
+    uint8_t *near;                    // [cbz][cby][cbx] blocks of VOF_CB^3 cells with a donor within reach (vof_near_*)
+    int cbx, cby, cbz;
+    int near_ok;                      // the periodic extents are multiples of VOF_CB (else the flags are not used)
     int *count;                       // integer counters (CNT_*)
     float *fcount;                    // float counters
 };
@@ -127,6 +136,10 @@ bool launch_tile_tma(const StepArgs &A, const CUtensorMap *m24, const CUtensorMa
 // the same two grids with the fast arithmetic policy (lbm_fast.cu)
 bool launch_tile_tma_fast(const StepArgs &A, const CUtensorMap *m24, const CUtensorMap *m20, cudaStream_t st);
 void launch_column_flux(const StepArgs &A, float *qx, float *qy, cudaStream_t st);
+// the water stream (height or VOF path): the compact kernel on the cells of
+// water_stream_class, then the general stream on the cells it left, listed in
+// list[*count] (list: one int per cell)
+void launch_water_stream(const StepArgs &A, int *list, int *count, cudaStream_t st);
 void launch_advect(const lbm_params &P, const Dom &D, const float *bed_h, const float *qx, const float *qy,
                    const float *h_in, float *h_out, float *h_last, float t, cudaStream_t st);
 void launch_refill(const StepArgs &A, const int8_t *type_prev, int *count, cudaStream_t st);

@@ -60,11 +60,50 @@ LBM_DEV float rho_ref(const VofArgs &V, int c) {
 
 // lattice_open[0] and lattice_open_frac[0] of every cell for the step's
 // geometry (the VOF kernels look them up for 18 neighbours per cell)
+// Donor-in-reach flags of the receiver passes.  A donor (excess mass or an
+// orphan) marks the coarse block of VOF_CB^3 cells it lies in and the 26
+// around it (wrapping as the neighbour lookup does), so every cell within
+// VOF_CB cells of a donor sits in a marked block; a receiver in an unmarked
+// block has no donor in reach, and its loop over the donors would add
+// nothing.  Wrapped neighbours fall in the next block only when the
+// periodic extents are multiples of VOF_CB; otherwise (near_ok 0) the flags
+// are not used.
+LBM_DEV void vof_mark_near(const VofArgs &V, int k, int j, int i) {
+    if (!V.near_ok) return;
+    const int bk = k / VOF_CB, bj = j / VOF_CB, bi = i / VOF_CB;
+    for (int dk = -1; dk <= 1; ++dk) {
+        const int zk = bk + dk;
+        if (zk < 0 || zk >= V.cbz) continue;
+        for (int dj = -1; dj <= 1; ++dj) {
+            const int yj = (bj + dj + V.cby) % V.cby;
+            for (int di = -1; di <= 1; ++di) {
+                int xi = bi + di;
+                if (V.P.x_solid) {
+                    if (xi < 0 || xi >= V.cbx) continue;
+                } else {
+                    xi = (xi + V.cbx) % V.cbx;
+                }
+                V.near[((size_t)zk * V.cby + yj) * V.cbx + xi] = 1;
+            }
+        }
+    }
+}
+LBM_DEV bool vof_near(const VofArgs &V, int k, int j, int i) {
+    return !V.near_ok || V.near[((size_t)(k / VOF_CB) * V.cby + j / VOF_CB) * V.cbx + i / VOF_CB] != 0;
+}
+
 __global__ void k_vof_open(VofArgs V, BedView B) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= (int)V.D.n) return;
     int k, j, i;
     vkji(V.D, c, k, j, i);
+    // far from the bed and every other geometry (solid x walls close links,
+    // not cells): open, full open fraction
+    if (geo_far_except_x(V.P, V.D, B, k, j, i)) {
+        V.open[c] = 1;
+        V.lf0[c] = 1.0f;
+        return;
+    }
     GeoLinks L;
     Geo g = geo_cell(V.P, V.slot, V.D, B, k, j, i, L, true);
     V.open[c] = (int8_t)(g.lo & 1u);
@@ -209,6 +248,7 @@ __global__ void k_vof_redist_donor(VofArgs V) {
         }
     }
     donor[c] = 1;
+    vof_mark_near(V, k, j, i);
     dir[c] = (int8_t)d;
     nxv[c] = nx_;
     nyv[c] = ny_;
@@ -227,7 +267,7 @@ __global__ void k_vof_redist_recv(VofArgs V) {
     int k, j, i;
     vkji(D, r, k, j, i);
     float acc = V.m0[r];
-    if (V.open[r] == 1) {
+    if (V.open[r] == 1 && vof_near(V, k, j, i)) {
 #pragma unroll
         for (int q = 1; q < 19; ++q) {
             int d;
@@ -367,6 +407,7 @@ __global__ void k_vof_orphan_donor(VofArgs V, int *cnt) {
                     }
                 if (m > VOF_E12 && (cw > VOF_E12 || tw > VOF_E12)) {
                     orphan[c] = 1;
+                    vof_mark_near(V, k, j, i);
                     capw[c] = cw;
                     topw[c] = tw;
                     counted = true;
@@ -389,7 +430,8 @@ __global__ void k_vof_orphan_recv(VofArgs V) {
     int k, j, i;
     vkji(D, r, k, j, i);
     float acc = orphan[r] ? 0.0f : V.m0[r];
-    if (V.open[r] == 1 && V.t0[r] != LBM_FS_GAS && V.x0[r] >= othr) {
+    // orphans reach R cells: the flags cover VOF_CB
+    if (V.open[r] == 1 && V.t0[r] != LBM_FS_GAS && V.x0[r] >= othr && (R > VOF_CB || vof_near(V, k, j, i))) {
         float rr = V.rho[r];
         if (rr < VOF_E8) rr = V.P.rho0;
         const float room = rr - V.m0[r];

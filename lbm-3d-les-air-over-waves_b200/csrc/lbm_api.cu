@@ -462,18 +462,13 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
     // LBM_B200_TEST_TMA_TIMEOUT=1: the tile-copy kernel takes its wait-timeout
     // exit (status bit 2) at its first plane; used only by the error-path test
     const char *tt = getenv("LBM_B200_TEST_TMA_TIMEOUT");
-    // with the stash, the band cells away from the bed take the compact
-    // kernels (LBM_B200_NO_BAND_SPLIT=1: all in the general kernels)
-    const char *nb = getenv("LBM_B200_NO_BAND_SPLIT");
-    const bool band = stash && !(nb && nb[0] == '1');
-    const int tflag = (R.classic ? F_TILE_CLASSIC : 0) | (stash ? F_STASH : 0) | (band ? F_BAND_SPLIT : 0) |
+    const int tflag = (R.classic ? F_TILE_CLASSIC : 0) | (stash ? F_STASH : 0) |
                       ((tt && tt[0] == '1') ? F_TEST_WAIT_TIMEOUT : 0);
     A.flags = ((K == 1) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
     // fused interior steps with LES: the tile-copy kernel (32-bit population indices)
     const bool tma = R.tile && les && !R.classic && !R.no_tma && 19.0 * (double)ctx->D.n < 2147483647.0 &&
                      tile_maps_ready(ctx);
     if (les) {
-        if (band) launch_step_kernel(KER_BAND_PREPASS_CANON, A, st);
         launch_step_kernel(KER_PREPASS_CANON, A, st);
         CK_LAUNCH("prepass");
     }
@@ -481,7 +476,6 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
         launch_step_kernel(KER_TILE_CANON, A, st);
         CK_LAUNCH("tile");
     }
-    if (band) launch_step_kernel(KER_BAND_COLLIDE_CANON, A, st);
     launch_step_kernel(KER_COLLIDE_CANON, A, st);
     CK_LAUNCH("collide");
     src = 1 - src;
@@ -494,7 +488,6 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
         A.step = (uint64_t)(m + 1 - key0);
         A.flags = ((m + 1 == n + K) ? (F_WRITE_MACRO | F_WRITE_ALL_OMEGA) : 0) | tflag;
         if (les) {
-            if (band) launch_step_kernel(KER_BAND_PREPASS_FUSED, A, st);
             launch_step_kernel(KER_PREPASS_FUSED, A, st);
             CK_LAUNCH("prepass fused");
         }
@@ -510,7 +503,6 @@ static int step_air(lbm_ctx *ctx, int K, cudaStream_t st) {
                 ctx->timed_cells = (int64_t)(R.zi1 - R.zi0 + 1) * P_nx(ctx) * P_ny(ctx);
             }
         }
-        if (band) launch_step_kernel(KER_BAND_COLLIDE_FUSED, A, st);
         launch_step_kernel(KER_COLLIDE_FUSED, A, st);
         CK_LAUNCH("fused");
         src = 1 - src;
@@ -1453,9 +1445,7 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
     for (BatchGroupPlan &g : b->groups)
         if ((e = cudaStreamWaitEvent(g.stream, b->start, 0)) != cudaSuccess)
             return batch_fail(b, LBM_ERR_CUDA, cudaGetErrorString(e));
-    const char *nb = getenv("LBM_B200_NO_BAND_SPLIT");
-    const bool band = b->stash[0] && !(nb && nb[0] == '1');
-    const int tflag = (b->stash[0] ? F_STASH : 0) | (band ? F_BAND_SPLIT : 0);
+    const int tflag = b->stash[0] ? F_STASH : 0;
     const int K = nsteps;
     // step s of every group, then step s + 1: the groups' streams run side by side
     for (int s = 0; s < K; ++s) {
@@ -1466,13 +1456,10 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
         for (BatchGroupPlan &g : b->groups) {
             launch_batch_bed(g.L, m + 1, g.stream);
             if (s == 0) {
-                if (band) batch_issue(b, g, KER_BAND_PREPASS_CANON, 0, step, flags);
                 if (b->les) batch_issue(b, g, KER_PREPASS_CANON, 0, step, flags);
                 batch_issue(b, g, KER_TILE_CANON, 0, step, flags);
-                if (band) batch_issue(b, g, KER_BAND_COLLIDE_CANON, 0, step, flags);
                 batch_issue(b, g, KER_COLLIDE_CANON, 0, step, flags);
             } else {
-                if (band) batch_issue(b, g, KER_BAND_PREPASS_FUSED, q, step, flags);
                 if (b->les) batch_issue(b, g, KER_PREPASS_FUSED, q, step, flags);
                 if (g.ninner) {
                     batch_issue(b, g, KER_TILE_FUSED, q, step, flags, true);
@@ -1480,7 +1467,6 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
                 } else {
                     batch_issue(b, g, KER_TILE_FUSED, q, step, flags);
                 }
-                if (band) batch_issue(b, g, KER_BAND_COLLIDE_FUSED, q, step, flags);
                 batch_issue(b, g, KER_COLLIDE_FUSED, q, step, flags);
             }
         }

@@ -70,19 +70,15 @@ __global__ void kb_colgeo(BatchLaunch L, int par) {
     colgeo_column(B.P, B.D, V, j, i, B.cg);
 }
 
-// KIND 0: pre-pass, 1: collide, 2: stream (column-cache kernels); 3, 4:
-// pre-pass and collide of the band cells away from the bed (the group's
-// collision model COLL)
-template <int S, int IN, int KIND, int COLL = -1>
-__global__ void __launch_bounds__(256, (KIND == 0 || KIND == 3) ? LBM_CG_PRE_MINB : LBM_CG_MINB)
+// KIND 0: pre-pass, 1: collide, 2: stream (column-cache kernels)
+template <int S, int IN, int KIND>
+__global__ void __launch_bounds__(256, KIND == 0 ? LBM_CG_PRE_MINB : LBM_CG_MINB)
     kb_general(const __grid_constant__ BatchGroup G) {
     const int4 m = G.map[blockIdx.x];
     const StepArgs &A = G.a[m.x];
     const int gz = A.zcnt[0] + A.zcnt[1] + A.zcnt[2];
     if constexpr (KIND == 0) prepass_body<S, IN, true>(A, m.y, m.z, m.w, gz);
     else if constexpr (KIND == 1) collide_body<S, IN, true>(A, m.y, m.z, m.w, gz);
-    else if constexpr (KIND == 3) band_prepass_body<S, IN>(A, m.y, m.z, m.w, gz);
-    else if constexpr (KIND == 4) band_collide_body<S, IN, COLL>(A, m.y, m.z, m.w, gz);
     else stream_body<S, true>(A, m.y, m.z, m.w);
 }
 

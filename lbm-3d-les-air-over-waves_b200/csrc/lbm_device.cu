@@ -389,7 +389,6 @@ template <int S, int IN, bool CG>
 __device__ __forceinline__ void prepass_body(const StepArgs &A, int bx, int by, int bz, int gz) {
     int i, j, k, c;
     if (!cell_xyz(A, bx, by, bz, i, j, k, c)) return;
-    if (CG && (A.flags & F_BAND_SPLIT) && cell_fast(A, IN == 1, true, k, j, i)) return;   // band_prepass_body
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
@@ -424,8 +423,6 @@ __device__ __forceinline__ void collide_body(const StepArgs &A, int bx, int by, 
     int i, j, k, c;
     if (!cell_xyz(A, bx, by, bz, i, j, k, c)) return;
     if (!CG && IN == 0 && (A.flags & F_WATER_SPLIT) && water_collide_local(A, k, j, i)) return;   // k_collide_water
-    if (CG && (A.flags & F_BAND_SPLIT) && (A.flags & F_STASH) && cell_fast(A, IN == 1, true, k, j, i))
-        return;   // band_collide_body
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
@@ -478,74 +475,6 @@ __device__ __forceinline__ void collide_body(const StepArgs &A, int bx, int by, 
 template <int S, int IN, bool CG>
 __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collide(StepArgs A) {
     collide_body<S, IN, CG>(A, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.z);
-}
-
-// ---------------------------------------- compact kernels of the air bed band
-// Cells of the general planes (bed band, top row) of the column-cache path
-// that are away from the bed in both geometries of the step (cell_fast): the
-// pre-pass and the collide of the general kernels take their fast paths
-// there (plain gather or stored populations, no link geometry), so the same
-// stage calls run here in kernels without the near-bed code.  The general
-// kernels, launched with F_BAND_SPLIT, skip these cells.  With the stash
-// (LES) only.
-template <int S, int IN>
-__device__ __forceinline__ void band_prepass_body(const StepArgs &A, int bx, int by, int bz, int gz) {
-    int i, j, k, c;
-    if (!cell_xyz(A, bx, by, bz, i, j, k, c)) return;
-    if (!cell_fast(A, IN == 1, true, k, j, i)) return;
-    float f[19], r, vx, vy, vz;
-    if (IN == 0) load_cell<S>(A, c, f);
-    else stream_fast<S>(A, (const typename Store<S>::T *)A.fsrc, k, j, i, c, f);
-    macro(A.P, A.D, f, k, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
-    A.u_out[c] = vx;
-    A.u_out[A.D.n + c] = vy;
-    A.u_out[2 * A.D.n + c] = vz;
-    if (S == LBM_STORE_F32) {
-        store_cell<S>(A, c, f);
-    } else {
-        const size_t ng = (size_t)gz * A.D.nx * A.D.ny;
-        const size_t g = ((size_t)bz * A.D.ny + j) * A.D.nx + i;
-#pragma unroll
-        for (int q = 0; q < 19; ++q) A.stash[q * ng + g] = f[q];
-    }
-}
-template <int S, int IN, int COLL>
-__device__ __forceinline__ void band_collide_body(const StepArgs &A, int bx, int by, int bz, int gz) {
-    int i, j, k, c;
-    if (!cell_xyz(A, bx, by, bz, i, j, k, c)) return;
-    if (!cell_fast(A, IN == 1, true, k, j, i)) return;
-    const lbm_params &P = A.P;
-    float f[19], r, vx, vy, vz;
-    if (S == LBM_STORE_F32) {
-        const float *fd = (const float *)A.fdst;
-#pragma unroll
-        for (int q = 0; q < 19; ++q) f[q] = fd[(size_t)q * A.D.n + c];
-    } else {
-        const size_t ng = (size_t)gz * A.D.nx * A.D.ny;
-        const size_t g = ((size_t)bz * A.D.ny + j) * A.D.nx + i;
-#pragma unroll
-        for (int q = 0; q < 19; ++q) f[q] = A.stash[q * ng + g];
-    }
-    macro(P, A.D, f, k, false, LBM_FS_LIQUID, 0.0f, r, vx, vy, vz);
-    if (A.flags & F_WRITE_MACRO) {
-        A.rho[c] = r; A.ux[c] = vx; A.uy[c] = vy; A.uz[c] = vz;
-    }
-    if (!(r == r) || fabsf(r) > 3.0e38f) atomicOr(A.status, 1u);
-    float om = P.omega0;
-    if (P.use_les) {
-        om = les_omega(A, k, j, i, c, vx, vy, vz);
-        if (A.flags & F_WRITE_ALL_OMEGA) A.omega[c] = om;   // fast geometry: the band's omega only on request
-    }
-    collide<COLL>(A, c, k, false, false, false, 0.0f, r, vx, vy, vz, om, f);
-    store_cell<S>(A, c, f);
-}
-template <int S, int IN>
-__global__ void __launch_bounds__(256, 3) k_band_prepass(StepArgs A) {
-    band_prepass_body<S, IN>(A, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.z);
-}
-template <int S, int IN, int COLL>
-__global__ void __launch_bounds__(256, 2) k_band_collide(StepArgs A) {
-    band_collide_body<S, IN, COLL>(A, blockIdx.x, blockIdx.y, blockIdx.z, gridDim.z);
 }
 
 template <int S, bool CG>
@@ -1506,18 +1435,6 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
             else k_stream<S, false><<<g, kBlock3, 0, st>>>(A);
             LAUNCHED(1);
             break;
-        case KER_BAND_PREPASS_CANON: k_band_prepass<S, 0><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); break;
-        case KER_BAND_PREPASS_FUSED: k_band_prepass<S, 1><<<g, kBlock3, 0, st>>>(A); LAUNCHED(1); break;
-        case KER_BAND_COLLIDE_CANON:
-            if (A.P.collision == LBM_COLLIDE_KBC) k_band_collide<S, 0, LBM_COLLIDE_KBC><<<g, kBlock3, 0, st>>>(A);
-            else k_band_collide<S, 0, LBM_COLLIDE_REGULARIZED><<<g, kBlock3, 0, st>>>(A);
-            LAUNCHED(1);
-            break;
-        case KER_BAND_COLLIDE_FUSED:
-            if (A.P.collision == LBM_COLLIDE_KBC) k_band_collide<S, 1, LBM_COLLIDE_KBC><<<g, kBlock3, 0, st>>>(A);
-            else k_band_collide<S, 1, LBM_COLLIDE_REGULARIZED><<<g, kBlock3, 0, st>>>(A);
-            LAUNCHED(1);
-            break;
         case KER_WATER_COLLIDE:
             if (A.P.collision == LBM_COLLIDE_KBC) k_collide_water<S, LBM_COLLIDE_KBC><<<g, kBlock3, 0, st>>>(A);
             else k_collide_water<S, LBM_COLLIDE_REGULARIZED><<<g, kBlock3, 0, st>>>(A);
@@ -1820,7 +1737,7 @@ int batch_tile_blocks(int storage, bool les, int collision, int arith, bool tma)
 }
 
 template <int S>
-static void launch_batch_group_s(int which, const BatchGroup &G, int collision, cudaStream_t st) {
+static void launch_batch_group_s(int which, const BatchGroup &G, cudaStream_t st) {
     if (!G.nmap) return;
     const dim3 b3(32, 8, 1);
     switch (which) {
@@ -1830,16 +1747,6 @@ static void launch_batch_group_s(int which, const BatchGroup &G, int collision, 
         case KER_COLLIDE_FUSED: kb_general<S, 1, 1><<<G.nmap, b3, 0, st>>>(G); break;
         case KER_STREAM: kb_general<S, 0, 2><<<G.nmap, b3, 0, st>>>(G); break;
         case KER_STREAM_INTERIOR: kb_stream_interior<S><<<G.nmap, 256, 0, st>>>(G); break;
-        case KER_BAND_PREPASS_CANON: kb_general<S, 0, 3><<<G.nmap, b3, 0, st>>>(G); break;
-        case KER_BAND_PREPASS_FUSED: kb_general<S, 1, 3><<<G.nmap, b3, 0, st>>>(G); break;
-        case KER_BAND_COLLIDE_CANON:
-            if (collision == LBM_COLLIDE_KBC) kb_general<S, 0, 4, LBM_COLLIDE_KBC><<<G.nmap, b3, 0, st>>>(G);
-            else kb_general<S, 0, 4, LBM_COLLIDE_REGULARIZED><<<G.nmap, b3, 0, st>>>(G);
-            break;
-        case KER_BAND_COLLIDE_FUSED:
-            if (collision == LBM_COLLIDE_KBC) kb_general<S, 1, 4, LBM_COLLIDE_KBC><<<G.nmap, b3, 0, st>>>(G);
-            else kb_general<S, 1, 4, LBM_COLLIDE_REGULARIZED><<<G.nmap, b3, 0, st>>>(G);
-            break;
         default: return;
     }
     LAUNCHED(1);
@@ -1852,9 +1759,9 @@ void launch_batch_group(int which, int storage, const BatchGroup &G, bool les, i
         return;
     }
     switch (storage) {
-        case LBM_STORE_F16S: launch_batch_group_s<LBM_STORE_F16S>(which, G, collision, st); break;
-        case LBM_STORE_BF16S: launch_batch_group_s<LBM_STORE_BF16S>(which, G, collision, st); break;
-        default: launch_batch_group_s<LBM_STORE_F32>(which, G, collision, st); break;
+        case LBM_STORE_F16S: launch_batch_group_s<LBM_STORE_F16S>(which, G, st); break;
+        case LBM_STORE_BF16S: launch_batch_group_s<LBM_STORE_BF16S>(which, G, st); break;
+        default: launch_batch_group_s<LBM_STORE_F32>(which, G, st); break;
     }
 }
 

@@ -18,16 +18,13 @@ enum : int {
     F_TILE_CLASSIC = 16,    // interior planes: the unpipelined tile kernel even for FP32
     F_STASH = 32,           // general planes: the pre-pass leaves its populations in the destination for the collide
     F_TEST_WAIT_TIMEOUT = 64,  // tile-copy kernel: treat the first wait as timed out (tests of the error path)
-    F_WATER_SPLIT = 128,    // water: the general collide leaves the cells of the compact kernel
-    F_BAND_SPLIT = 256,     // air, column cache, stash: the general pre-pass / collide leave the cells away from the bed
+    F_WATER_SPLIT = 128,    // height-path water: the general collide / stream leave the cells of the compact kernels
 };
 
 enum {
     KER_PREPASS_CANON = 0, KER_PREPASS_FUSED = 1, KER_COLLIDE_CANON = 2, KER_COLLIDE_FUSED = 3, KER_STREAM = 4,
     KER_TILE_CANON = 5, KER_TILE_FUSED = 6, KER_STREAM_INTERIOR = 7, KER_WATER_COLLIDE = 8,
-    KER_TILE_TMA = 10,  // ensembles: the fused interior step with LES on the tiles off the domain edge, tile copies
-    // air bed band (column cache, stash): the cells away from the bed in compact kernels
-    KER_BAND_PREPASS_CANON = 11, KER_BAND_PREPASS_FUSED = 12, KER_BAND_COLLIDE_CANON = 13, KER_BAND_COLLIDE_FUSED = 14
+    KER_TILE_TMA = 10   // ensembles: the fused interior step with LES on the tiles off the domain edge, tile copies
 };
 // device counters of a context (int slots)
 enum { CNT_CUT = 0, CNT_FSCUT = 1, CNT_BRIDGE = 2, CNT_FS_REFILL = 3, CNT_COALESCE = 4, CNT_VOF_EXCESS = 5,

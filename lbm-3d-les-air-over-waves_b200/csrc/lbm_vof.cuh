@@ -355,7 +355,10 @@ __global__ void k_vof_interface_layer(VofArgs V) {
     for (int q = 1; q < 19; ++q) {
         int n;
         if (!vnbr(D, V.P.x_solid, k, j, i, cxq(q), cyq(q), czq(q), n)) continue;
-        if (V.open[n] == 1 && V.t0[n] == LBM_FS_GAS) touches = true;
+        if (V.open[n] == 1 && V.t0[n] == LBM_FS_GAS) {
+            touches = true;
+            break;
+        }
     }
     if (touches) {
         V.type[c] = LBM_FS_INTERFACE;
@@ -386,7 +389,10 @@ __global__ void k_vof_orphan_donor(VofArgs V, int *cnt) {
                 if (!vnbr(D, V.P.x_solid, k, j, i, cxq(q), cyq(q), czq(q), n) || V.open[n] != 1) continue;
                 if (V.t0[n] != LBM_FS_GAS) {
                     wet++;
-                    if (V.x0[n] >= othr) res++;
+                    if (V.x0[n] >= othr) {
+                        res++;
+                        break;   // a resolved neighbour: not an orphan (res == 0 below fails)
+                    }
                 }
             }
             if (res == 0 && (V.x0[c] < othr || wet <= V.P.vof_orphan_max_weak_neighbors)) {
@@ -468,6 +474,7 @@ LBM_DEV bool detached_cell(const VofArgs &V, int c, int k, int j, int i) {
     if (!(V.open[c] == 1 && V.type[c] != LBM_FS_GAS && V.fill[c] > FILL_LO)) return false;
     int wet = 0, res = 0;
     const float othr = V.P.vof_orphan_empty_threshold;
+    const int maxw = V.P.vof_detached_max_wet_neighbors, maxr = V.P.vof_detached_max_resolved_neighbors;
 #pragma unroll
     for (int q = 1; q < 19; ++q) {
         int n;
@@ -475,9 +482,10 @@ LBM_DEV bool detached_cell(const VofArgs &V, int c, int k, int j, int i) {
         if (V.type[n] != LBM_FS_GAS) {
             wet++;
             if (V.fill[n] >= othr) res++;
+            if (wet > maxw || res > maxr) return false;   // the counts only grow
         }
     }
-    return wet <= V.P.vof_detached_max_wet_neighbors && res <= V.P.vof_detached_max_resolved_neighbors;
+    return true;
 }
 // vof_gas_neighbor_rate, CODEX.py:1813-1832
 LBM_DEV float gas_rate(const VofArgs &V, int k, int j, int i, int di, int dj, int dk, float rate) {
@@ -499,13 +507,14 @@ __global__ void k_vof_detached_donor(VofArgs V, int compress, int *cnt) {
         float *mv = V.fa + 6 * (size_t)c;
         int8_t *isd = V.ba;
         double moved_total = 0.0;
-#pragma unroll
-        for (int e = 0; e < 6; ++e) mv[e] = 0.0f;
         int k, j, i;
         vkji(D, c, k, j, i);
         const bool det = detached_cell(V, c, k, j, i);
         isd[c] = det ? 1 : 0;
         if (det) {
+            // the apply pass reads the moved masses of detached cells only
+#pragma unroll
+            for (int e = 0; e < 6; ++e) mv[e] = 0.0f;
             const float m = V.mass[c];
             const float vx = V.ux[c], vy = V.uy[c], vz = V.uz[c];
             float r[6];

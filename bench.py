@@ -58,9 +58,9 @@ CPU_SAMPLES = [(128, 64, 256), (64, 64, 256), (64, 32, 256), (64, 16, 256)]
 # interior grid, divided by the cells of the launch).  A profile figure, not
 # a live one: the source says which grid, kernels and commit it was taken on.
 PROFILE_TRAFFIC = {
-    "bytes_per_cell": 163.9,
-    "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, k_tile_edges + k_tile_tma, 256x256x96 air "
-              "(scaled per cell to the launch), commit 6a8f1aa; profiles/k_tile_air_interior.md",
+    "bytes_per_cell": 170.7,
+    "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_tile_edges + k_tile_tma pair at 512x256x256 "
+              "(this workload; one pass, --clock-control none), commit fa6d57e; profiles/k_tile_air_interior.md",
 }
 
 

@@ -619,7 +619,7 @@ static int step_vof(lbm_ctx *ctx, int K, cudaStream_t st) {
         CK(vof_sequence(V, due, ctx->v_tree, st), "vof sequence");
         A.flags = F_VOF_STATE;
         A.fdst = ctx->b.f[ctx->cur];
-        launch_refill(A, ctx->b.fs_type_prev, ctx->dcount + CNT_FS_REFILL, st);
+        launch_refill_vof(A, V, ctx->b.fs_type_prev, ctx->wlist, ctx->dcount + CNT_FS_REFILL, st);
         CK_LAUNCH("refill");
         CK(cudaMemsetAsync(ctx->dcount + CNT_COALESCE, 0, sizeof(int), st), "counter reset");
         launch_vof_coalesce(V, st);

@@ -963,6 +963,46 @@ __global__ void __launch_bounds__(256) k_refill(StepArgs A, const int8_t *type_p
     if ((threadIdx.x & 31) == 0 && s) atomicAdd(count, s);
 }
 
+// VOF path in two passes: the cells that turned wet (type_prev gas, type
+// not gas) are listed (one warp-aggregated atomic per warp) and their coarse
+// blocks marked for the coalescence repair (vof_mark_near), then the refill
+// runs over the list only.
+__global__ void __launch_bounds__(256) k_refill_vof_mark(StepArgs A, VofArgs V, const int8_t *type_prev, int *list,
+                                                           int *lcount) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    bool cand = false;
+    if (c < (int)A.D.n) {
+        cand = type_prev[c] == LBM_FS_GAS && A.fs_type[c] != LBM_FS_GAS;
+        if (cand) {
+            int k, j, i;
+            cell_of(A.D, c, k, j, i);
+            vof_mark_near(V, k, j, i);
+        }
+    }
+    const unsigned lanes = __ballot_sync(0xffffffffu, cand);
+    if (lanes) {
+        const int lane = threadIdx.x & 31, lead = __ffs(lanes) - 1;
+        int base = 0;
+        if (lane == lead) base = atomicAdd(lcount, __popc(lanes));
+        base = __shfl_sync(0xffffffffu, base, lead);
+        if (cand) list[base + __popc(lanes & ((1u << lane) - 1u))] = c;
+    }
+}
+template <int S>
+__global__ void __launch_bounds__(256) k_refill_vof_list(StepArgs A, const int8_t *type_prev, const int *list,
+                                                          const int *lcount, int *count) {
+    const int nl = *lcount;
+    int did = 0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nl; e += gridDim.x * blockDim.x) {
+        const int c = list[e];
+        int k, j, i;
+        cell_of(A.D, c, k, j, i);
+        did += refill_cell<S>(A, type_prev, c, k, j, i, type_prev[c], A.fs_type[c]);
+    }
+    const int s = __reduce_add_sync(0xffffffffu, did);
+    if ((threadIdx.x & 31) == 0 && s) atomicAdd(count, s);
+}
+
 // Height path: one thread per column.  A cell is refilled only if it was gas
 // under the height before advection and is not gas under the new one, which
 // needs k dx within a cell of the two heights: the planes from two below the
@@ -1530,6 +1570,26 @@ void launch_refill(const StepArgs &A, const int8_t *type_prev, int *count, cudaS
         case LBM_STORE_F16S: { k_refill<LBM_STORE_F16S><<<g, 256, 0, st>>>(A, type_prev, count); LAUNCHED(1); } break;
         case LBM_STORE_BF16S: { k_refill<LBM_STORE_BF16S><<<g, 256, 0, st>>>(A, type_prev, count); LAUNCHED(1); } break;
         default: k_refill<LBM_STORE_F32><<<g, 256, 0, st>>>(A, type_prev, count); LAUNCHED(1); break;
+    }
+}
+template <int S>
+static void launch_refill_vof_s(const StepArgs &A, const VofArgs &V, const int8_t *type_prev, int *list, int *count,
+                                cudaStream_t st) {
+    int *lcount = list + A.D.n;
+    cudaMemsetAsync(lcount, 0, sizeof(int), st);
+    cudaMemsetAsync(V.near, 0, vof_near_bytes(V.D), st);
+    k_refill_vof_mark<<<blocks_for(A.D.n, 256), 256, 0, st>>>(A, V, type_prev, list, lcount);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_refill_vof_list<S><<<(unsigned)sms, 256, 0, st>>>(A, type_prev, list, lcount, count);
+    LAUNCHED(2);
+}
+void launch_refill_vof(const StepArgs &A, const VofArgs &V, const int8_t *type_prev, int *list, int *count,
+                       cudaStream_t st) {
+    switch (A.P.pop_storage) {
+        case LBM_STORE_F16S: launch_refill_vof_s<LBM_STORE_F16S>(A, V, type_prev, list, count, st); break;
+        case LBM_STORE_BF16S: launch_refill_vof_s<LBM_STORE_BF16S>(A, V, type_prev, list, count, st); break;
+        default: launch_refill_vof_s<LBM_STORE_F32>(A, V, type_prev, list, count, st); break;
     }
 }
 void launch_height_types(const StepArgs &A, float *fill, int8_t *type, int8_t *type_prev, cudaStream_t st) {

@@ -143,6 +143,10 @@ void launch_water_stream(const StepArgs &A, int *list, int *count, cudaStream_t 
 void launch_advect(const lbm_params &P, const Dom &D, const float *bed_h, const float *qx, const float *qy,
                    const float *h_in, float *h_out, float *h_last, float t, cudaStream_t st);
 void launch_refill(const StepArgs &A, const int8_t *type_prev, int *count, cudaStream_t st);
+// VOF path: list the cells that turned wet (list: one int per cell and a count), mark their coarse blocks in
+// V.near for the coalescence repair, refill the listed cells
+void launch_refill_vof(const StepArgs &A, const VofArgs &V, const int8_t *type_prev, int *list, int *count,
+                       cudaStream_t st);
 void launch_height_types(const StepArgs &A, float *fill, int8_t *type, int8_t *type_prev, cudaStream_t st);
 
 void launch_init_constants(const InitArgs &I, cudaStream_t st);

@@ -772,10 +772,12 @@ __global__ void k_vof_coalesce(VofArgs V, int *cnt) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const Dom &D = V.D;
     int reps = 0;
-    if (c < (int)D.n && V.open[c] == 1 && V.type[c] != LBM_FS_GAS && V.type_prev[c] != LBM_FS_GAS) {
+    int k = 0, j = 0, i = 0;
+    if (c < (int)D.n) vkji(D, c, k, j, i);
+    // vof_near: a cell that turned wet lies within one cell (marked by k_refill_vof_mark)
+    if (c < (int)D.n && V.open[c] == 1 && V.type[c] != LBM_FS_GAS && V.type_prev[c] != LBM_FS_GAS &&
+        vof_near(V, k, j, i)) {
         typename Store<S>::T *f = (typename Store<S>::T *)V.f;
-        int k, j, i;
-        vkji(D, c, k, j, i);
 #pragma unroll
         for (int q = 1; q < 19; ++q) {
             int sir = i - cxq(q);

@@ -126,3 +126,34 @@ def test_water_height_storage_error_vs_fp64(storage):
     _record("water height 256x128x96, 60 steps", storage, errs)
     assert errs["velocity"] <= WATER_VEL_MAX[storage], errs
     assert errs["elevation"] <= 1e-3, errs
+
+
+@pytest.mark.parametrize("storage", ["f16s", "bf16s"])
+def test_water_height_16bit_storage_vs_fp32(storage):
+    """The storage's own error at the water configuration's shape: the 16-bit
+    form against the FP32 form of the same run (60 steps), which separates it
+    from the FP32 arithmetic's distance to FP64 that the test above measures.
+    Velocity relative to the FP32 run's maximum over liquid and interface
+    cells; the north star's 1e-3 bound for shifted FP16, 2e-2 for BF16."""
+    from lbm_b200.domain import Domain
+
+    env = water_gaussian_env(256, 128, 96, depth=48.0, amp=8.0, sigma=16.0, g_lb=1e-5, tau0=0.51)
+    runs = {}
+    for st in ("f32", storage):
+        e = dict(env)
+        e["LBM_B200_POP_STORAGE"] = st
+        dom = Domain(e, device="cuda:0", with_diag=False)
+        dom.step(60)
+        dom.synchronize()
+        wet = dom.field("fs_type").cpu().numpy() != 0
+        u = np.stack([dom.field(k).cpu().numpy() for k in ("ux", "uy", "uz")]).astype(np.float64)
+        runs[st] = (u, wet)
+        dom.close()
+    u32, wet = runs["f32"]
+    u16, _ = runs[storage]
+    speed = np.sqrt((u32 ** 2).sum(0))[wet].max()
+    err = float(np.abs(u16 - u32).max(0)[wet].max() / speed)
+    rms = float(np.sqrt(((u16 - u32) ** 2).sum(0)[wet].mean()) / np.sqrt((speed ** 2)))
+    print(json.dumps({"case": "water height 256x128x96, 60 steps, 16-bit vs FP32 storage", "storage": storage,
+                      "velocity": err, "velocity_rms_over_max": rms}), flush=True)
+    assert err <= {"f16s": 1e-3, "bf16s": 2e-2}[storage], err

@@ -689,7 +689,7 @@ __global__ void __launch_bounds__(256, 2) k_stream_water(StepArgs A, int *list, 
 
 // the general stream over the cells k_stream_water left (grid-stride over the list)
 template <int S>
-__global__ void __launch_bounds__(256, LBM_GEN_MINB) k_stream_list(StepArgs A, const int *list, const int *count) {
+__global__ void __launch_bounds__(256, 2) k_stream_list(StepArgs A, const int *list, const int *count) {
     const int nl = *count;
     int cut = 0, fscut = 0, bridge = 0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nl; e += gridDim.x * blockDim.x) {
@@ -1536,7 +1536,7 @@ static void launch_water_stream_s(const StepArgs &A, int *list, int *count, cuda
     k_stream_water<S><<<g, kBlock3, 0, st>>>(A, list, count);
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    k_stream_list<S><<<(unsigned)(sms * LBM_GEN_MINB), 256, 0, st>>>(A, list, count);
+    k_stream_list<S><<<(unsigned)(sms * 2), 256, 0, st>>>(A, list, count);
     LAUNCHED(2);
 }
 void launch_water_stream(const StepArgs &A, int *list, int *count, cudaStream_t st) {

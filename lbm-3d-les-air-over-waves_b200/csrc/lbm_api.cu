@@ -1117,6 +1117,7 @@ struct lbm_batch {
     std::vector<Plan> plan;
     std::vector<bool> stash;
     std::vector<bool> tma;              // domains whose inner tiles take the tile-copy grid
+    bool pdl = true;                    // tile-copy grid behind the edge grid as a programmatic dependent launch
     std::vector<BatchGroupPlan> groups;
     int storage = 0;
     int arith = LBM_ARITH_EXACT;        // of the interior planes, uniform over the ensemble
@@ -1176,6 +1177,7 @@ static void batch_issue(lbm_batch *b, const BatchGroupPlan &g, int which, int q,
         G.a[d].flags = flags;
     }
     G.queue = g.d_queue;
+    G.pdl = 0;
     int blocks = g.tile_blocks;
     if (which == KER_TILE_TMA) {
         for (int d = 0; d < g.nd; ++d) {
@@ -1187,11 +1189,13 @@ static void batch_issue(lbm_batch *b, const BatchGroupPlan &g, int which, int q,
         G.map = g.d_inner;
         G.nmap = g.ninner;
         G.queue = g.d_queue + 2;
+        G.pdl = b->pdl && g.nedge ? 1 : 0;
         blocks = g.tma_blocks;
     } else if (edge) {
         G.map = g.d_edge;
         G.nmap = g.nedge;
         G.queue = g.d_queue + 1;
+        G.pdl = b->pdl ? 1 : 0;   // the edge launch zeroes the tile-copy grid's counter (d_queue + 2) too
     } else if (which == KER_TILE_CANON || which == KER_TILE_FUSED) {
         G.map = g.d_items;
         G.nmap = g.nitems;
@@ -1274,6 +1278,9 @@ int lbm_batch_create(lbm_ctx *const *ctxs, int32_t n, lbm_batch **out) {
     const char *tv = getenv("LBM_B200_BATCH_TMA");
     const bool tma_on = !(tv && tv[0] == '0');
     b->tma.assign(n, false);
+    // LBM_B200_BATCH_PDL=0: the tile-copy grid in plain stream order after the edge grid
+    const char *pv = getenv("LBM_B200_BATCH_PDL");
+    b->pdl = !(pv && pv[0] == '0');
     for (BatchGroupPlan &g : b->groups) {
         std::vector<long long> col0(1, 0);
         std::vector<int4> gmap, smap, items, edge, inner;

@@ -22,6 +22,9 @@ template <int S, int IN, bool LES, class Ar>
 __global__ void __launch_bounds__(256, 2) kb_tile(const __grid_constant__ BatchGroup G) {
     extern __shared__ __align__(16) float smem[];
     __shared__ int s_item;
+    // a tile-copy grid launched behind this one may start once every block
+    // runs (the two take disjoint tiles)
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
     for (;;) {
         __syncthreads();   // every thread is done with the last item's shared memory
         if (threadIdx.x == 0) s_item = atomicAdd(G.queue, 1);
@@ -54,6 +57,9 @@ __global__ void __launch_bounds__(256, 2) kb_tile_tma(const __grid_constant__ Ba
                                   it.z * LBM_TILE, it.w))
             break;   // a wait gave up (status bit 2 of the domain)
     }
+    // complete only after the edge grid this one may have been launched
+    // behind, so that the work after it sees both grids' results
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
 }
 
 template <int S, class Ar>
@@ -84,9 +90,22 @@ static int batch_tma_blocks_t() {
 template <int S, class Ar>
 static void launch_batch_tma_t(const BatchGroup &G, int tile_blocks, cudaStream_t st) {
     if (!G.nmap || tile_blocks <= 0 || !batch_tma_ready_t<S, Ar>()) return;
-    cudaMemsetAsync(G.queue, 0, sizeof(int), st);
+    if (!G.pdl) cudaMemsetAsync(G.queue, 0, sizeof(int), st);
     const unsigned g = (unsigned)(tile_blocks < G.nmap ? tile_blocks : G.nmap);
-    kb_tile_tma<S, Ar><<<g, 256, tma_smem_bytes<S>(), st>>>(G);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(g, 1, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = tma_smem_bytes<S>();
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = G.pdl ? 1 : 0;
+    if (cudaLaunchKernelEx(&cfg, kb_tile_tma<S, Ar>, G) != cudaSuccess) {
+        cudaGetLastError();
+        kb_tile_tma<S, Ar><<<g, 256, tma_smem_bytes<S>(), st>>>(G);
+    }
     launch_count_add(1);
 }
 
@@ -121,7 +140,7 @@ static int batch_tile_blocks_t() {
 template <int S, bool LES, class Ar>
 static void launch_batch_tile_t(int which, const BatchGroup &G, int tile_blocks, cudaStream_t st) {
     if (!G.nmap || tile_blocks <= 0 || !batch_tile_ready_t<S, LES, Ar>()) return;
-    cudaMemsetAsync(G.queue, 0, sizeof(int), st);
+    cudaMemsetAsync(G.queue, 0, (G.pdl ? 2 : 1) * sizeof(int), st);   // with pdl: the tile-copy grid's counter too
     const unsigned g = (unsigned)(tile_blocks < G.nmap ? tile_blocks : G.nmap);
     if (which == KER_TILE_CANON) kb_tile<S, 0, LES, Ar><<<g, 256, batch_tile_smem<S>(), st>>>(G);
     else kb_tile<S, 1, LES, Ar><<<g, 256, batch_tile_smem<S>(), st>>>(G);

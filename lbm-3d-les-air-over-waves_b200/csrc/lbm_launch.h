@@ -238,6 +238,8 @@ struct BatchGroup {
     int nmap;
     int ndom;
     int *queue;                      // interior grids: next work item
+    int pdl;                         // interior grids: the tile-copy grid follows the edge grid as a programmatic
+                                     // dependent launch (the edge launch zeroes both counters)
     StepArgs a[BATCH_GROUP];         // step arguments of the launch (step number and flags included)
 };
 static_assert(sizeof(BatchGroup) <= 32764, "kernel parameter space");

@@ -551,10 +551,8 @@ static int step_height(lbm_ctx *ctx, int K, cudaStream_t st) {
             CK_LAUNCH("prepass");
         }
         // the compact kernels take the cells with local collide / plain-gather
-        // stream, the general ones the rest (disjoint cells, either order)
-        A.flags |= F_WATER_SPLIT;
-        launch_step_kernel(KER_WATER_COLLIDE, A, st);
-        launch_step_kernel(KER_COLLIDE_CANON, A, st);
+        // stream, the general ones the rest, from a list
+        launch_water_collide(A, ctx->wlist, ctx->wlist + ctx->D.n, st);
         CK_LAUNCH("collide");
         CK(cudaMemsetAsync(ctx->dcount, 0, 4 * sizeof(int), st), "counter reset");
         A.fsrc = ctx->b.f[1 - ctx->cur];
@@ -605,9 +603,8 @@ static int step_vof(lbm_ctx *ctx, int K, cudaStream_t st) {
             launch_step_kernel(KER_PREPASS_CANON, A, st);
             CK_LAUNCH("prepass");
         }
-        A.flags |= F_WATER_SPLIT;   // compact kernels for the cells with local collide / plain-gather stream
-        launch_step_kernel(KER_WATER_COLLIDE, A, st);
-        launch_step_kernel(KER_COLLIDE_CANON, A, st);
+        // compact kernels for the cells with local collide / plain-gather stream, the general ones over a list
+        launch_water_collide(A, ctx->wlist, ctx->wlist + ctx->D.n, st);
         CK_LAUNCH("collide");
         CK(cudaMemsetAsync(ctx->dcount, 0, 4 * sizeof(int), st), "counter reset");
         A.fsrc = ctx->b.f[1 - ctx->cur];

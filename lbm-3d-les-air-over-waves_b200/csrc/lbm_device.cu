@@ -419,10 +419,7 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_PRE_MINB : LBM_GEN_MINB) k_pr
 }
 
 template <int S, int IN, bool CG>
-__device__ __forceinline__ void collide_body(const StepArgs &A, int bx, int by, int bz, int gz) {
-    int i, j, k, c;
-    if (!cell_xyz(A, bx, by, bz, i, j, k, c)) return;
-    if (!CG && IN == 0 && (A.flags & F_WATER_SPLIT) && water_collide_local(A, k, j, i)) return;   // k_collide_water
+__device__ __forceinline__ void collide_cell(const StepArgs &A, int k, int j, int i, int c, int bz, int gz) {
     float f[19], r, vx, vy, vz, gbf;
     int type;
     bool fast_c, open;
@@ -471,6 +468,12 @@ __device__ __forceinline__ void collide_body(const StepArgs &A, int bx, int by, 
     }
     collide(A, c, k, !open, water, gas, gbf, r, vx, vy, vz, om, f);
     store_cell<S>(A, c, f);
+}
+template <int S, int IN, bool CG>
+__device__ __forceinline__ void collide_body(const StepArgs &A, int bx, int by, int bz, int gz) {
+    int i, j, k, c;
+    if (!cell_xyz(A, bx, by, bz, i, j, k, c)) return;
+    collide_cell<S, IN, CG>(A, k, j, i, c, bz, gz);
 }
 template <int S, int IN, bool CG>
 __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_collide(StepArgs A) {
@@ -564,8 +567,7 @@ __device__ __forceinline__ void stream_body(const StepArgs &A, int bx, int by, i
     int cut = 0, fscut = 0, bridge = 0;
     if (cell_xyz(A, bx, by, bz, i, j, k, c)) {
         const int wcls = CG ? 0 : water_stream_class(A, k, j, i);
-        if (CG || wcls == 0 || !(A.flags & F_WATER_SPLIT))   // else: k_stream_water
-            stream_cell<S, CG>(A, k, j, i, c, wcls, cut, fscut, bridge);
+        stream_cell<S, CG>(A, k, j, i, c, wcls, cut, fscut, bridge);
     }
     stream_counts(A, cut, fscut, bridge);
 }
@@ -574,17 +576,47 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream
     stream_body<S, CG>(A, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-// ------------------------------------------ compact kernels of height-path water
+// ------------------------------------------------ compact kernels of water
 // The cells that water_collide_local (collide) or water_stream_class (stream)
 // admit take the same stage functions as in the general kernels, in kernels
 // that carry none of the near-wall, free-surface-cut or VOF code, so they are
 // small enough to run without register spills or instruction-cache misses.
-// The general kernels, launched with F_WATER_SPLIT, skip these cells.
+// They list the other cells, and the general collide / stream run over the
+// list only (k_collide_list, k_stream_list).
+// list / count: the cells left to the general collide are appended, for k_collide_list
 template <int S, int COLL>
-__global__ void __launch_bounds__(256, 2) k_collide_water(StepArgs A) {
+__device__ __forceinline__ void collide_water_cell(const StepArgs &A, int k, int j, int i, int c);
+template <int S, int COLL>
+__global__ void __launch_bounds__(256, 2) k_collide_water(StepArgs A, int *list, int *count) {
     int i, j, k, c;
-    if (!cell_xyz(A, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k, c)) return;
-    if (!water_collide_local(A, k, j, i)) return;
+    bool local = false, general = false;
+    if (cell_xyz(A, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k, c)) {
+        local = water_collide_local(A, k, j, i);
+        general = !local;
+    }
+    const unsigned lanes = __ballot_sync(0xffffffffu, general);
+    if (lanes) {
+        const int lane = threadIdx.x & 31, lead = __ffs(lanes) - 1;
+        int base = 0;
+        if (lane == lead) base = atomicAdd(count, __popc(lanes));
+        base = __shfl_sync(0xffffffffu, base, lead);
+        if (general) list[base + __popc(lanes & ((1u << lane) - 1u))] = c;
+    }
+    if (local) collide_water_cell<S, COLL>(A, k, j, i, c);
+}
+// the general collide over the cells k_collide_water left (grid-stride over the list)
+template <int S>
+__global__ void __launch_bounds__(256, 2) k_collide_list(StepArgs A, const int *list, const int *count) {
+    const int nl = *count;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nl; e += gridDim.x * blockDim.x) {
+        const int c = list[e];
+        int k, j, i;
+        cell_of(A.D, c, k, j, i);
+        collide_cell<S, 0, false>(A, k, j, i, c, 0, 1);
+    }
+}
+template <int S, int COLL>
+__device__ __forceinline__ void collide_water_cell(const StepArgs &A, int k, int j, int i, int c) {
     const lbm_params &P = A.P;
     // front() for such a cell: open, no closed link to condition
     const bool fast_c = !(P.x_solid && (i == 0 || i == A.D.nx - 1));
@@ -1475,11 +1507,7 @@ static void launch_step_kernel_s(int which, const StepArgs &A, cudaStream_t st) 
             else k_stream<S, false><<<g, kBlock3, 0, st>>>(A);
             LAUNCHED(1);
             break;
-        case KER_WATER_COLLIDE:
-            if (A.P.collision == LBM_COLLIDE_KBC) k_collide_water<S, LBM_COLLIDE_KBC><<<g, kBlock3, 0, st>>>(A);
-            else k_collide_water<S, LBM_COLLIDE_REGULARIZED><<<g, kBlock3, 0, st>>>(A);
-            LAUNCHED(1);
-            break;
+
 
         case KER_TILE_CANON:
             if constexpr (S != LBM_STORE_F32) {
@@ -1526,6 +1554,25 @@ void launch_step_kernel(int which, const StepArgs &A, cudaStream_t st) {
         case LBM_STORE_F16S: launch_step_kernel_s<LBM_STORE_F16S>(which, A, st); break;
         case LBM_STORE_BF16S: launch_step_kernel_s<LBM_STORE_BF16S>(which, A, st); break;
         default: launch_step_kernel_s<LBM_STORE_F32>(which, A, st); break;
+    }
+}
+template <int S>
+static void launch_water_collide_s(const StepArgs &A, int *list, int *count, cudaStream_t st) {
+    const dim3 g = grid3(A);
+    if (g.z == 0) return;
+    cudaMemsetAsync(count, 0, sizeof(int), st);
+    if (A.P.collision == LBM_COLLIDE_KBC) k_collide_water<S, LBM_COLLIDE_KBC><<<g, kBlock3, 0, st>>>(A, list, count);
+    else k_collide_water<S, LBM_COLLIDE_REGULARIZED><<<g, kBlock3, 0, st>>>(A, list, count);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_collide_list<S><<<(unsigned)(sms * 2), 256, 0, st>>>(A, list, count);
+    LAUNCHED(2);
+}
+void launch_water_collide(const StepArgs &A, int *list, int *count, cudaStream_t st) {
+    switch (A.P.pop_storage) {
+        case LBM_STORE_F16S: launch_water_collide_s<LBM_STORE_F16S>(A, list, count, st); break;
+        case LBM_STORE_BF16S: launch_water_collide_s<LBM_STORE_BF16S>(A, list, count, st); break;
+        default: launch_water_collide_s<LBM_STORE_F32>(A, list, count, st); break;
     }
 }
 template <int S>

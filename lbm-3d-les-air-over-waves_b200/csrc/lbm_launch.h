@@ -18,12 +18,11 @@ enum : int {
     F_TILE_CLASSIC = 16,    // interior planes: the unpipelined tile kernel even for FP32
     F_STASH = 32,           // general planes: the pre-pass leaves its populations in the destination for the collide
     F_TEST_WAIT_TIMEOUT = 64,  // tile-copy kernel: treat the first wait as timed out (tests of the error path)
-    F_WATER_SPLIT = 128,    // height-path water: the general collide / stream leave the cells of the compact kernels
 };
 
 enum {
     KER_PREPASS_CANON = 0, KER_PREPASS_FUSED = 1, KER_COLLIDE_CANON = 2, KER_COLLIDE_FUSED = 3, KER_STREAM = 4,
-    KER_TILE_CANON = 5, KER_TILE_FUSED = 6, KER_STREAM_INTERIOR = 7, KER_WATER_COLLIDE = 8,
+    KER_TILE_CANON = 5, KER_TILE_FUSED = 6, KER_STREAM_INTERIOR = 7,
     KER_TILE_TMA = 10   // ensembles: the fused interior step with LES on the tiles off the domain edge, tile copies
 };
 // device counters of a context (int slots)
@@ -140,6 +139,9 @@ void launch_column_flux(const StepArgs &A, float *qx, float *qy, cudaStream_t st
 // water_stream_class, then the general stream on the cells it left, listed in
 // list[*count] (list: one int per cell)
 void launch_water_stream(const StepArgs &A, int *list, int *count, cudaStream_t st);
+// the water collide: the compact kernel on the cells of water_collide_local, then the general collide on the
+// cells it left, listed in list[*count]
+void launch_water_collide(const StepArgs &A, int *list, int *count, cudaStream_t st);
 void launch_advect(const lbm_params &P, const Dom &D, const float *bed_h, const float *qx, const float *qy,
                    const float *h_in, float *h_out, float *h_last, float t, cudaStream_t st);
 void launch_refill(const StepArgs &A, const int8_t *type_prev, int *count, cudaStream_t st);

@@ -1,7 +1,7 @@
 """Replicas across GPUs: one independent domain per rank, no data-path
 collective.
 
-The step does not shard here (the north star fixes one GPU per solve), so a
+The step does not shard here (each solve runs on one GPU), so a
 multi-GPU run is N independent replicas: each rank advances its own domain
 (seed offset by the rank), and the only collectives are a barrier around the
 timed region and a max of the ranks' timings.  Launched one process per GPU

@@ -4,7 +4,7 @@ LBM_ARITH_FAST evaluates the interior cells' moments, LES rate and
 collision in pair form with multiply-add contraction (lbm_fast.cuh); every
 near-wall cell, the geometry and the flags stay exact.  Its results differ
 from the reference arithmetic by rounding only, and the bound on that
-difference is the north star's for the FP32 form: 1e-5 relative error
+difference is the one stated for the FP32 form: 1e-5 relative error
 against the reference after the configuration's full run.
 
 Error measures after N steps, over open cells:

@@ -19,7 +19,7 @@ link endpoint and the bed (CODEX.py:2604-2640), a discontinuous test, and a
 bed whose extremes fall exactly on link-endpoint heights (level 6, amplitude
 3 with dx = 1) gets hundreds of flags that FP32 and FP64 round to opposite
 sides (test_oracle_precision.py).  The air case here therefore uses level 6.3.
-Bounds: FP32 max 1e-4; shifted FP16 max 1e-3 (the north star's bound for the
+Bounds: FP32 max 1e-4; shifted FP16 max 1e-3 (the stated bound for the
 16-bit form); BF16 (8 mantissa bits) max 2e-2, rms 5e-3.  The water case runs
 at the water configuration's own shape (256x128x96, depth 48, Gaussian ridge
 amplitude 8, sigma 16, g = 1e-5, tau = 0.51) for 60 of its 10,000 steps.
@@ -139,7 +139,7 @@ def test_water_height_16bit_storage_vs_fp32(storage):
     g t = 6e-4), while the stored shifted populations carry the hydrostatic
     head (f - w rho0 of order w rho0 g z / cs^2), so FP16's relative step of
     2^-11 on that head is not small against the velocity signal: above the
-    north star's 1e-3 for the 16-bit form, which the air case meets (6.4e-4).
+    stated 1e-3 for the 16-bit form, which the air case meets (6.4e-4).
     The bounds hold the measured errors with margin."""
     from lbm_b200.domain import Domain
 

@@ -707,7 +707,7 @@ int lbm_bind(lbm_ctx *ctx, const lbm_buffers *bufs) {
                 (s = alloc(ctx, (void **)&ctx->v_m0, 4 * n)) || (s = alloc(ctx, (void **)&ctx->v_x0, 4 * n)) ||
                 (s = alloc(ctx, (void **)&ctx->v_fa, 24 * n)) || (s = alloc(ctx, (void **)&ctx->v_dd, 8 * n)) ||
                 (s = alloc(ctx, (void **)&ctx->v_tree, 8 * nt)) || (s = alloc(ctx, (void **)&ctx->v_dist, 4 * n)) ||
-                (s = alloc(ctx, (void **)&ctx->v_near, vof_near_bytes(ctx->D))))
+                (s = alloc(ctx, (void **)&ctx->v_near, 2 * vof_near_bytes(ctx->D))))
                 return s;
             CK(cudaMemset(ctx->v_dist, 0xff, 4 * n), "memset");
         }

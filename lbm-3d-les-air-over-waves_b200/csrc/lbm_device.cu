@@ -1729,8 +1729,13 @@ static void vof_finalize(const VofArgs &V, int *cnt, cudaStream_t st) {
     k_vof_finalize<<<vblocks(V), 256, 0, st>>>(V, cnt); LAUNCHED(1);
 }
 cudaError_t vof_interface_layer(const VofArgs &V, cudaStream_t st) {
-    cudaError_t e = vof_snapshot(V, nullptr, nullptr, nullptr, nullptr, true, st);
+    // type snapshot with the coarse marks of open gas cells, dilated by one
+    // block into V.near, which the layer kernel tests before its 18 neighbours
+    const size_t nb = vof_near_bytes(V.D);
+    cudaError_t e = cudaMemsetAsync(V.near + nb, 0, nb, st);
     if (e != cudaSuccess) return e;
+    k_vof_types_gas_mark<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
+    k_vof_gas_dilate<<<blocks_for(nb, 256), 256, 0, st>>>(V); LAUNCHED(1);
     k_vof_interface_layer<<<vblocks(V), 256, 0, st>>>(V); LAUNCHED(1);
     return cudaGetLastError();
 }

@@ -98,7 +98,8 @@ struct VofArgs {
     int8_t *ba;                       // 2 n bytes
     double *dd;                       // n doubles
     int *dist;                        // flood-fill distance of the last collapse pass (-1: not reached)
-    uint8_t *near;                    // [cbz][cby][cbx] blocks of VOF_CB^3 cells with a donor within reach (vof_near_*)
+    uint8_t *near;                    // [2][cbz][cby][cbx] blocks of VOF_CB^3 cells with a donor within reach
+                                      // (vof_near_*); the second half: scratch of the interface layer's marks
     int cbx, cby, cbz;
     int near_ok;                      // the periodic extents are multiples of VOF_CB (else the flags are not used)
     int *count;                       // integer counters (CNT_*)

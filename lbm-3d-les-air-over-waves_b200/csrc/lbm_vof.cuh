@@ -343,6 +343,47 @@ __global__ void k_vof_finalize(VofArgs V, int *cnt) {
 }
 
 // enforce_vof_interface_layer, CODEX.py:1627-1656 (reads the type snapshot t0)
+// Snapshot of the types for the interface layer (t0 = type) that also marks
+// the coarse blocks holding an open gas cell (second half of V.near)
+__global__ void k_vof_types_gas_mark(VofArgs V) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (int)V.D.n) return;
+    const int8_t t = V.type[c];
+    V.t0[c] = t;
+    if (V.near_ok && t == LBM_FS_GAS && V.open[c] == 1) {
+        int k, j, i;
+        vkji(V.D, c, k, j, i);
+        const size_t nb = (size_t)V.cbx * V.cby * V.cbz;
+        V.near[nb + ((size_t)(k / VOF_CB) * V.cby + j / VOF_CB) * V.cbx + i / VOF_CB] = 1;
+    }
+}
+// one thread per coarse block: marked (first half of V.near) when a block
+// within one block (wrapping as the neighbour lookup does) holds an open gas cell
+__global__ void k_vof_gas_dilate(VofArgs V) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nb = V.cbx * V.cby * V.cbz;
+    if (b >= nb) return;
+    const int bi = b % V.cbx, bj = (b / V.cbx) % V.cby, bk = b / (V.cbx * V.cby);
+    uint8_t any = 0;
+    for (int dk = -1; dk <= 1 && !any; ++dk) {
+        const int zk = bk + dk;
+        if (zk < 0 || zk >= V.cbz) continue;
+        for (int dj = -1; dj <= 1 && !any; ++dj) {
+            const int yj = (bj + dj + V.cby) % V.cby;
+            for (int di = -1; di <= 1 && !any; ++di) {
+                int xi = bi + di;
+                if (V.P.x_solid) {
+                    if (xi < 0 || xi >= V.cbx) continue;
+                } else {
+                    xi = (xi + V.cbx) % V.cbx;
+                }
+                any = V.near[nb + ((size_t)zk * V.cby + yj) * V.cbx + xi];
+            }
+        }
+    }
+    V.near[b] = any;
+}
+
 __global__ void k_vof_interface_layer(VofArgs V) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const Dom &D = V.D;
@@ -350,6 +391,7 @@ __global__ void k_vof_interface_layer(VofArgs V) {
     if (!(V.open[c] == 1 && V.t0[c] == LBM_FS_LIQUID)) return;
     int k, j, i;
     vkji(D, c, k, j, i);
+    if (!vof_near(V, k, j, i)) return;   // no open gas cell within one cell
     bool touches = false;
 #pragma unroll
     for (int q = 1; q < 19; ++q) {

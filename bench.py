@@ -563,8 +563,11 @@ def _config_env(name: str, storage: str) -> dict:
 
 
 def configs(args):
-    """Device time per step of the stated-size configurations (eager calls,
-    CUDA events on the domain's stream, after warm-up), one JSON line."""
+    """Device time per step of the stated-size configurations (CUDA events on
+    the domain's stream, after warm-up), one JSON line.  Step calls replay
+    captured step graphs where the mode allows them (air and the kinematic
+    height path; --no-graphs: eager calls); the warm-up captures the timed
+    call shape."""
     import torch
 
     from lbm_b200.domain import Domain
@@ -577,6 +580,17 @@ def configs(args):
         d.step(max(3, args.warmup))
         d.synchronize()
         K = args.steps
+        graphs = False
+        if not args.no_graphs:
+            try:
+                d.set_step_graphs(True)
+                graphs = True
+            except RuntimeError:
+                graphs = False   # the VOF path runs eager calls
+        if graphs:
+            for _ in range(3):
+                d.step(K)
+            d.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(d.stream)
         d.step(K)
@@ -585,7 +599,8 @@ def configs(args):
         ms = e0.elapsed_time(e1) / K
         cells = d.cfg.Nx * d.cfg.Ny * d.cfg.Nz
         out[name] = {"workload": what, "storage": storage, "cells": cells, "steps": K, "ms_per_step": ms,
-                     "value": cells / ms / 1e3, "unit": UNIT, "status_flags": d.counters()["status_flags"]}
+                     "value": cells / ms / 1e3, "unit": UNIT, "step_graphs": graphs,
+                     "status_flags": d.counters()["status_flags"]}
         d.close()
         del d
         torch.cuda.empty_cache()

@@ -376,7 +376,8 @@ int lbm_set_arithmetic(lbm_ctx *ctx, int32_t mode);
 int lbm_get_arithmetic(lbm_ctx *ctx, int32_t *mode);
 /* Step graphs (no counterpart in the reference; the reference launches
    every kernel from its Python step loop): when enabled, each lbm_step call
-   of the air path runs as one CUDA graph launch.  The first call of a given
+   of the air path or of the kinematic height path runs as one CUDA graph
+   launch.  The first call of a given
    step count, step parity and current population buffer is captured on the
    caller's stream (nothing runs during the capture) and kept; every later
    call of that shape replays it after one launch that writes the step
@@ -386,8 +387,10 @@ int lbm_get_arithmetic(lbm_ctx *ctx, int32_t *mode);
    stream) and start after one eager call; they are dropped by lbm_bind,
    lbm_set_tile_chunk with a new value and lbm_destroy, and not used while
    kernel timing is on.  A refused capture turns the context back to eager
-   calls.  Water modes return LBM_ERR_UNSUPPORTED (their steps synchronise
-   with the host).  The CPU oracle accepts and ignores it. */
+   calls.  The VOF path, the static height and the prescribed solitary
+   height return LBM_ERR_UNSUPPORTED (the VOF step decides on the host; the
+   prescribed height reads the host's step time).  The CPU oracle accepts
+   and ignores it. */
 int lbm_set_step_graphs(lbm_ctx *ctx, int32_t enable);
 
 /* Measurement hook (no counterpart in the reference): number of kernels the

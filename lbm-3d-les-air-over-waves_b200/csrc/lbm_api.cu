@@ -542,7 +542,9 @@ static int step_height(lbm_ctx *ctx, int K, cudaStream_t st) {
         A.zcnt[0] = ctx->P.nz;
         A.bed_s = slot_view(ctx, (int)(m & 1));
         A.bed_c = A.bed_s;
-        A.step = (uint64_t)m;
+        // under capture the step number is an offset from the device clock
+        if (ctx->capturing) A.clock = ctx->dclock;
+        A.step = (uint64_t)(m - (ctx->capturing ? ctx->cap_n0 : 0));
         A.fsrc = ctx->b.f[ctx->cur];
         A.fdst = ctx->b.f[1 - ctx->cur];
         A.flags = F_WRITE_MACRO | F_WRITE_ALL_OMEGA;
@@ -805,6 +807,14 @@ int lbm_init_fields(lbm_ctx *ctx, void *stream) {
 
 }  // extern "C"
 
+// Modes whose step calls can be captured as graphs: air, and the height
+// path with the kinematic height update (its advection does not read the
+// step time; the prescribed solitary height does).  The VOF path decides on
+// the host per step (trapped-gas collapse steps, the flood fill's stop).
+static bool graph_mode(const lbm_params &P) {
+    return P.fs_mode == LBM_FS_NONE || (P.fs_mode == LBM_FS_HEIGHT_KINEMATIC && P.fs_tracking != LBM_TRACK_VOF);
+}
+
 static int step_call(lbm_ctx *ctx, int32_t nsteps, cudaStream_t st) {
     int s;
     int64_t n0 = ctx->nstep;
@@ -879,7 +889,7 @@ int lbm_step(lbm_ctx *ctx, int32_t nsteps, void *stream) {
     ctx->last_stream = st;
     // step graphs: air mode, a stream of the caller's, no per-launch timing,
     // after one eager call (which sets the kernels' shared-memory limits)
-    if (ctx->graphs && st != 0 && ctx->P.fs_mode == LBM_FS_NONE && !ctx->timing && ctx->warm) {
+    if (ctx->graphs && st != 0 && graph_mode(ctx->P) && !ctx->timing && ctx->warm) {
         const int s = step_graph(ctx, nsteps, st);
         if (s != LBM_ERR_UNSUPPORTED) return s;
         ctx->graphs = false;   // capture refused: eager from now on
@@ -1055,7 +1065,8 @@ int lbm_get_arithmetic(lbm_ctx *ctx, int32_t *mode) {
 
 int lbm_set_step_graphs(lbm_ctx *ctx, int32_t enable) {
     if (!ctx) return LBM_ERR_BAD_ARG;
-    if (enable && ctx->P.fs_mode != LBM_FS_NONE) return fail(ctx, LBM_ERR_UNSUPPORTED, "lbm_set_step_graphs: air mode only");
+    if (enable && !graph_mode(ctx->P))
+        return fail(ctx, LBM_ERR_UNSUPPORTED, "lbm_set_step_graphs: air mode or the kinematic height path only");
     if (!enable) drop_graphs(ctx);
     ctx->graphs = enable != 0;
     return LBM_OK;

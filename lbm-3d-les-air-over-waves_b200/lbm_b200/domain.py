@@ -125,8 +125,9 @@ class Domain:
         self._check(self.lib.lbm_set_tile_chunk(self.ctx, int(planes)), "lbm_set_tile_chunk")
 
     def set_step_graphs(self, enable: bool = True):
-        """Run each step call as one CUDA graph launch (air mode; captured on
-        first use per call shape, bit-identical to eager calls)."""
+        """Run each step call as one CUDA graph launch (air mode and the
+        kinematic height path; captured on first use per call shape,
+        bit-identical to eager calls)."""
         self._check(self.lib.lbm_set_step_graphs(self.ctx, 1 if enable else 0), "lbm_set_step_graphs")
 
     def set_arithmetic(self, mode: str):

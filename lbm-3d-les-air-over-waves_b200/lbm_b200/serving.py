@@ -103,9 +103,10 @@ class Server:
         from .domain import Domain
 
         dom = Domain(env, device=self.device, stream=torch.cuda.Stream(torch.device(self.device)), with_diag=False)
-        if dom.cfg.physics_mode == "air":
-            if self.arith is not None:
-                dom.set_arithmetic(self.arith)
+        if dom.cfg.physics_mode == "air" and self.arith is not None:
+            dom.set_arithmetic(self.arith)
+        if dom.cfg.physics_mode == "air" or (dom.cfg.free_surface_mode == "height_kinematic"
+                                             and dom.cfg.free_surface_tracking_mode != "vof"):
             dom.set_step_graphs(True)   # calls of `chunk` steps replay one captured graph per call shape
         return dom
 

@@ -267,12 +267,13 @@ def test_gpu_tile_copy_kernel_equals_cp_async_kernel(storage, monkeypatch):
         assert np.array_equal(out["tile_copies"][k].view(np.uint8), out["pipe"][k].view(np.uint8)), k
 
 
-@pytest.mark.parametrize("variant", ["tiles", "small", "backscatter"])
+@pytest.mark.parametrize("variant", ["tiles", "small", "backscatter", "water", "water_kbc_backscatter"])
 def test_gpu_step_graphs_equal_eager_calls(variant):
     """Calls replayed from captured step graphs equal eager calls bit for
     bit.  The call lengths cover both step parities and both population
-    buffers, first captures and later replays; the backscatter variant
-    takes its random-kick key from the device step clock."""
+    buffers, first captures and later replays; the backscatter variants
+    take their random-kick key from the device step clock.  The water
+    variants run the kinematic height path (solid x walls)."""
     import numpy as np
     import torch
 
@@ -280,6 +281,11 @@ def test_gpu_step_graphs_equal_eager_calls(variant):
 
     if variant == "small":
         env = air_wave_env(32, 16, 24, amp=2.0, level=5.0, wavelength=16.0)
+    elif variant.startswith("water"):
+        env = water_gaussian_env(64, 16, 32, depth=16.0, amp=2.0, sigma=6.0, g_lb=1e-3)
+        if variant == "water_kbc_backscatter":
+            env["LBM_COLLISION"] = "kbc"
+            env["LBM_BACKSCATTER"] = "0.02"
     else:
         env = air_wave_env(64, 64, 40, amp=3.0, level=6.0, wavelength=32.0)
     if variant == "backscatter":
@@ -295,7 +301,10 @@ def test_gpu_step_graphs_equal_eager_calls(variant):
         assert ce["step"] == cg["step"] and ce["current_f"] == cg["current_f"], n
         assert cg["status_flags"] == 0
         assert torch.equal(eager.f(), graphed.f()), (n, ce["step"])
-        for k in ("rho", "ux", "uy", "uz", "omega", "water_h"):
+        names = ("rho", "ux", "uy", "uz", "omega", "water_h")
+        if variant.startswith("water"):
+            names += ("fs_h", "fs_fill")
+        for k in names:
             a, b = eager.field(k).cpu().numpy(), graphed.field(k).cpu().numpy()
             assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (n, k)
     eager.close()

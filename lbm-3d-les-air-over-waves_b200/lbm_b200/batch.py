@@ -104,12 +104,14 @@ def domain_bytes(cfg, with_diag: bool = False) -> int:
 class Batch:
     """Domains stepped together.
 
-    queue=True (air ensembles): one launch per phase of the step for all
-    domains (lbm_batch_*): the interior planes of every domain form one work
-    queue of (domain, tile, z chunk) items taken by a grid of resident
-    blocks; the planes next to the bed and the top, the bed and the final
-    stream are single grids over all domains.  Steps run on the batch's own
-    stream; results equal stepping each domain alone, bit for bit.
+    queue=True (air ensembles): one launch per phase of the step for each
+    group of up to 28 domains of one collision model (lbm_batch_*), each
+    group on a stream of the library's, joined to the batch's own stream at
+    the end of a call: the interior planes of a group's domains form work
+    queues of (domain, tile, z chunk) items taken by grids of resident blocks
+    (tile copies for the tiles off each domain's edge); the planes next to
+    the bed and the top, the bed and the final stream are single grids over
+    the group.  Results equal stepping each domain alone, bit for bit.
 
     arith: "exact" or "fast" interior arithmetic for every domain (default:
     each context's own, from LBM_B200_ARITH).
@@ -156,7 +158,7 @@ class Batch:
     @property
     def mode(self) -> str:
         if self.handle is not None:
-            return "one launch per phase over all domains (interior planes as one work queue)"
+            return "one launch per phase over each group of up to 28 domains (interior planes as work queues)"
         return "one stream and one step graph per domain" if self.graphs else "one stream per domain"
 
     @property

@@ -747,7 +747,7 @@ namespace lbm {
 // plane order, so each column's sum is the reference's sequential one.  A
 // gas or closed cell adds +0, which leaves a sum that starts at +0 unchanged.
 constexpr int FLUX_KC = 64;
-__global__ void __launch_bounds__(256) k_column_flux(StepArgs A, float *qx_out, float *qy_out) {
+__global__ void __launch_bounds__(256, 4) k_column_flux(StepArgs A, float *qx_out, float *qy_out) {
     __shared__ float sq[2][FLUX_KC][33];
     const Dom &D = A.D;
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -777,6 +777,7 @@ __global__ void __launch_bounds__(256) k_column_flux(StepArgs A, float *qx_out, 
         __syncthreads();
         if (ty < 2) {
             const int kn = min(FLUX_KC, D.nz - k0);
+#pragma unroll 8
             for (int kk = 0; kk < kn; ++kk) q += sq[ty][kk][tx];
         }
         __syncthreads();

@@ -586,8 +586,11 @@ __global__ void __launch_bounds__(256, CG ? LBM_CG_MINB : LBM_GEN_MINB) k_stream
 // list / count: the cells left to the general collide are appended, for k_collide_list
 template <int S, int COLL>
 __device__ __forceinline__ void collide_water_cell(const StepArgs &A, int k, int j, int i, int c);
+#ifndef LBM_WATER_MINB
+#define LBM_WATER_MINB 3   // resident blocks per SM of the compact water collide (80 registers, a few spilled)
+#endif
 template <int S, int COLL>
-__global__ void __launch_bounds__(256, 2) k_collide_water(StepArgs A, int *list, int *count) {
+__global__ void __launch_bounds__(256, LBM_WATER_MINB) k_collide_water(StepArgs A, int *list, int *count) {
     int i, j, k, c;
     bool local = false, general = false;
     if (cell_xyz(A, blockIdx.x, blockIdx.y, blockIdx.z, i, j, k, c)) {

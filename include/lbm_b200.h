@@ -437,14 +437,19 @@ const char *lbm_last_error(lbm_ctx *ctx);
 
 /* Ensembles (no counterpart in the reference, which runs one domain per
    process; replaces running run_ab_case.py once per ensemble member):
-   independent air contexts stepped together with one launch per phase of
-   the step for all of them.  The interior planes of every domain form one
-   work queue of (domain, tile, z chunk) items taken by a grid of resident
-   blocks, so domains of uneven size share the SMs; the planes next to the
-   bed and the top, the bed and the final stream run as single grids over
-   block maps of all domains.  Results equal those of stepping each context
-   with lbm_step, bit for bit (with fast arithmetic, those of its
-   cp.async-staged tiles).  Requirements: every context bound and
+   independent air contexts stepped together.  The contexts are ordered by
+   collision model and split into groups of at most 28; each group runs one
+   launch per phase of the step on a stream of the library's, joined to
+   `stream` at the end of the call.  The interior planes of a group's
+   domains form work queues of (domain, tile, z chunk) items taken by grids
+   of resident blocks (tile copies for the tiles off each domain's edge,
+   cp.async staging for the others), so domains of uneven size share the
+   SMs; the planes next to the bed and the top, the bed and the final
+   stream run as single grids over block maps of the group's domains.
+   Results equal those of stepping each context with lbm_step, bit for bit,
+   with the exact arithmetic (with the fast one, a domain of fewer than 3 x 3
+   tiles differs by rounding: its own calls take the exact cp.async kernel
+   for the interior).  Requirements: every context bound and
    initialised, air mode with bed-only geometry and periodic x, nx and ny
    multiples of 16, one population storage, one arithmetic
    (lbm_set_arithmetic), LES on for all or none, all at the same step; else LBM_ERR_UNSUPPORTED (message in lbm_last_error of the

@@ -166,6 +166,7 @@ def load_config(environ: Mapping[str, str] | None = None) -> SolverConfig:
     default_pf = "hydrostatic_balanced" if physics_mode == "water" else "total_pressure"
     if physics_mode == "water" and vis != "none":
         default_pf = "vof_component_balanced"
+    c.default_pressure_formulation = default_pf
     c.pressure_formulation = env.choice(
         "LBM_PRESSURE_FORMULATION", default_pf,
         ("total_pressure", "hydrostatic_balanced", "vof_component_balanced"),
@@ -252,7 +253,7 @@ def load_config(environ: Mapping[str, str] | None = None) -> SolverConfig:
     c.boundary_geometry_mode = bgm
     c.use_phi_open_fraction = 1 if bgm in ("phi_fraction", "phi") else 0
     c.use_phi_open_flags = 1 if bgm == "phi" else 0
-    default_xb = "solid" if (physics_mode == "water" and fsi == "gaussian") else "periodic"
+    default_xb = c.default_x_boundary_mode = "solid" if (physics_mode == "water" and fsi == "gaussian") else "periodic"
     c.x_boundary_mode = env.choice("LBM_X_BOUNDARY", default_xb, ("periodic", "solid"))
     c.wall_velocity_sampling = env.choice("LBM_WALL_VELOCITY_SAMPLING", "link", ("cell", "link"))
     c.use_link_wall_velocity = 1 if c.wall_velocity_sampling == "link" else 0
@@ -286,7 +287,7 @@ def load_config(environ: Mapping[str, str] | None = None) -> SolverConfig:
     c.free_surface_base_m = env.float("LBM_FREE_SURFACE_LEVEL_M", c.offset_m + c.free_surface_depth_m)
     if c.free_surface_depth_m <= 0.0:
         raise ValueError("LBM_FREE_SURFACE_DEPTH_M must be positive")
-    ratio_env = env.get("LBM_SOLITARY_HEIGHT_DEPTH_RATIO", None)
+    ratio_env = c.solitary_height_depth_ratio_env = env.get("LBM_SOLITARY_HEIGHT_DEPTH_RATIO", None)
     if ratio_env is not None:
         c.solitary_height_depth_ratio = float(ratio_env)
         if c.solitary_height_depth_ratio <= 0.0:
@@ -323,7 +324,8 @@ def load_config(environ: Mapping[str, str] | None = None) -> SolverConfig:
     c.vof_block_size_z_m = env.float("LBM_VOF_BLOCK_SIZE_Z_M", c.vof_block_size_m)
     c.vof_block_center_x_m = env.float("LBM_VOF_BLOCK_CENTER_X_M", 0.5 * c.Lx_m)
     c.vof_block_center_y_m = env.float("LBM_VOF_BLOCK_CENTER_Y_M", 0.5 * c.Ly_m)
-    bottom_default = min(c.Lz_m - c.vof_block_size_z_m - dx, c.free_surface_base_m + 2.0 * dx)
+    bottom_default = c.vof_block_bottom_default_m = min(c.Lz_m - c.vof_block_size_z_m - dx,
+                                                        c.free_surface_base_m + 2.0 * dx)
     c.vof_block_bottom_m = env.float("LBM_VOF_BLOCK_BOTTOM_M", bottom_default)
     c.vof_block_center_z_m = env.float("LBM_VOF_BLOCK_CENTER_Z_M", c.vof_block_bottom_m + 0.5 * c.vof_block_size_z_m)
     if vis != "none" and fst != "vof":
@@ -366,13 +368,13 @@ def load_config(environ: Mapping[str, str] | None = None) -> SolverConfig:
     c.cube_center_x_m = env.float("LBM_CUBE_CENTER_X_M", 0.5 * c.Lx_m)
     c.cube_center_y_m = env.float("LBM_CUBE_CENTER_Y_M", 0.5 * c.Ly_m)
     c.cube_yaw_deg = env.float("LBM_CUBE_YAW_DEG", 0.0)
-    yaw = float(np.deg2rad(c.cube_yaw_deg))
+    yaw = c.cube_yaw_rad = float(np.deg2rad(c.cube_yaw_deg))
     c.cube_yaw_cos, c.cube_yaw_sin = float(np.cos(yaw)), float(np.sin(yaw))
     c.cube_pitch_deg = env.float("LBM_CUBE_PITCH_DEG", 0.0)
-    pitch = float(np.deg2rad(c.cube_pitch_deg))
+    pitch = c.cube_pitch_rad = float(np.deg2rad(c.cube_pitch_deg))
     c.cube_pitch_cos, c.cube_pitch_sin = float(np.cos(pitch)), float(np.sin(pitch))
     c.cube_vertical_half_extent_m = c.cube_half_z_m * abs(c.cube_pitch_cos) + c.cube_half_x_m * abs(c.cube_pitch_sin)
-    cz_default = min(
+    cz_default = c.cube_center_z_default = min(
         c.Lz_m - c.cube_vertical_half_extent_m - dx,
         max(0.5 * c.Lz_m, c.offset_m + 2.0 * c.bed_amp_m + c.cube_vertical_half_extent_m + dx),
     )

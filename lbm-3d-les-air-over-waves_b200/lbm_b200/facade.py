@@ -231,7 +231,7 @@ def write_render_snapshot(ns, *, label: str, step: int, time_phys: float, output
         "y_phys": np.asarray(ns["y_phys"]).astype(np.float32),
         "z_phys": np.asarray(ns["z_phys"]).astype(np.float32),
         "water_h": water_h.astype(np.float32),
-        "obstacle": obstacle.astype(np.uint8),
+        "obstacle": obstacle.astype(bool).astype(np.uint8),
         "free_surface_enabled": np.array(int(fs_enabled), dtype=np.int8),
         "tracking_mode": np.array(tracking),
         "include_cube_geometry": np.array(int(ns.get("include_cube_geometry", 0)), dtype=np.int8),
@@ -242,11 +242,9 @@ def write_render_snapshot(ns, *, label: str, step: int, time_phys: float, output
         "cube_yaw_pitch_deg": np.array([float(ns.get("cube_yaw_deg", 0.0)), float(ns.get("cube_pitch_deg", 0.0))],
                                        dtype=np.float32),
     }
-    if fs_enabled:
+    if fs_enabled:   # without a free surface the reference's caller passes neither array
         data["free_surface_h"] = ns["free_surface_h"].to_numpy().astype(np.float32)
         data["free_surface_fill"] = ns["free_surface_fill"].to_numpy().astype(np.float32)
-    else:
-        data["free_surface_h"] = water_h.astype(np.float32)
     path = out / f"{label}_render_{int(step):05d}.npz"
     np.savez_compressed(path, **data)
     return str(path)

@@ -1,0 +1,69 @@
+"""The metric-row restatement against the reference's own make_visualize.
+
+tests/golden/metrics_rows.json holds the rows that run_ab_case.py's
+visualize callback (run_ab_case.py:283-596) computed from the seeded fields
+of metrics_inputs() (gen_metrics_golden.py beside it).  The restatement in
+metrics_restatement.py, which the device diagnostics are checked against,
+must give the same values from the same fields: locations, types and counts
+exactly, the maximum speed to float32 rounding (the restatement takes it in
+float32 as Taichi's fields give it; the golden ran on float64 copies), and
+sums and band statistics to 1e-9 relative.  A metric the restatement does not
+produce for a mode must be the reference's not-applicable value there (NaN
+or -1)."""
+import json
+import math
+import os
+import sys
+import types
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+from gen_metrics_golden import CASES, metrics_inputs  # noqa: E402
+from metrics_restatement import metrics_from_fields  # noqa: E402
+
+with open(os.path.join(HERE, "golden", "metrics_rows.json"), encoding="utf-8") as _fh:
+    ROWS = json.load(_fh)
+
+RESTATED = ("max_speed_phys", "max_speed_x", "max_speed_y", "max_speed_z", "max_speed_fs_type",
+            "max_speed_wet_neighbors", "max_speed_full_neighbors", "max_speed_gas_neighbors", "water_volume",
+            "vof_mass_total", "vof_min_interface_fill", "vof_tiny_interface_count", "vof_pending_excess_mass",
+            "vof_pending_excess_count", "surface_min", "surface_max", "surface_symmetry_l2", "surface_eta_hp_rms",
+            "surface_left_max", "surface_right_max", "p_rms", "p_hp_rms", "p_total_rms", "p_total_hp_rms",
+            "vort_rms", "vort_hp_rms", "fs_p_rms", "fs_p_hp_rms", "fs_p_total_rms", "fs_p_total_hp_rms",
+            "fs_vort_rms", "fs_vort_hp_rms")
+INTEGER = {"max_speed_fs_type", "max_speed_wet_neighbors", "max_speed_full_neighbors", "max_speed_gas_neighbors",
+           "vof_tiny_interface_count", "vof_pending_excess_count"}
+
+
+def test_golden_rows_cover_every_case():
+    assert sorted(ROWS) == sorted(CASES)
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_restatement_matches_the_reference_row(case):
+    g, opts = metrics_inputs(case)
+    ours = metrics_from_fields(g, types.SimpleNamespace(**opts))
+    dx = opts["dx"]
+    for axis, index in (("x", "max_i"), ("y", "max_j"), ("z", "max_k")):
+        ours[f"max_speed_{axis}"] = (ours[index] + 0.5) * dx
+    row = ROWS[case]
+    compared = 0
+    for key in RESTATED:
+        ref = row[key]
+        if key not in ours:
+            assert ref is None or ref == -1, (key, ref)
+            continue
+        v = ours[key]
+        if ref is None:
+            assert isinstance(v, float) and math.isnan(v), (key, v)
+        elif key in INTEGER:
+            assert v == ref, (key, v, ref)
+        elif key == "max_speed_phys":
+            assert abs(v - ref) <= 2e-7 * abs(ref), (key, v, ref)
+        else:
+            assert abs(v - ref) <= 1e-9 * max(1.0, abs(ref)), (key, v, ref)
+        compared += 1
+    # every metric of the mode is compared: air has no free-surface metrics, the height path no VOF ones
+    assert compared == {"air_periodic": 10, "vof_component_balanced": 32}.get(case, 27), compared

@@ -10,7 +10,7 @@ variable).  For each case, render_inputs() builds a seeded stand-in for the
 solver module (scalars and fields with .to_numpy()).  The reference's
 save_render_snapshot (run_ab_case.py:140-202) writes it with the arguments
 that its visualize callback passes (run_ab_case.py:291-301, 829-841).  The
-result is tests/golden/render_<case>.npz.  run_ab_case.py imports
+result is tests/golden/render/<case>.npz.  run_ab_case.py imports
 matplotlib at the top; it is absent here and the writer does not use it, so
 an empty stand-in module takes its place for the import.
 """
@@ -111,10 +111,11 @@ def main():
     reference = os.path.abspath(args.reference) if args.reference else ""
     if not reference or not os.path.exists(os.path.join(reference, HARNESS_FILE)):
         raise SystemExit(f"{HARNESS_FILE} not found: pass --reference PATH or set LBM_REFERENCE_DIR")
+    os.makedirs(os.path.join(HERE, "render"), exist_ok=True)
     with tempfile.TemporaryDirectory() as folder:
         for case in CASES:
             path = write_with_reference(reference, case, Path(folder))
-            out = os.path.join(HERE, f"render_{case}.npz")
+            out = os.path.join(HERE, "render", f"{case}.npz")
             shutil.copyfile(path, out)
             print(f"wrote {out} ({os.path.getsize(out)} B)")
 

@@ -1,6 +1,6 @@
 """The render-snapshot writer against the reference's own writer.
 
-tests/golden/render_<case>.npz were written by save_render_snapshot of
+tests/golden/render/<case>.npz were written by save_render_snapshot of
 run_ab_case.py:140-202 from the seeded inputs of render_inputs()
 (gen_render_golden.py beside them).  write_render_snapshot must write the
 same file name and the same arrays: names, dtypes, shapes and values."""
@@ -22,7 +22,7 @@ def test_snapshot_matches_the_reference_writer(case, tmp_path):
     path = write_render_snapshot(render_inputs(case), label=case, step=STEP, time_phys=TIME, output_dir=tmp_path)
     assert os.path.basename(path) == f"{case}_render_{STEP:05d}.npz"
     ours = np.load(path)
-    ref = np.load(os.path.join(HERE, "golden", f"render_{case}.npz"))
+    ref = np.load(os.path.join(HERE, "golden", "render", f"{case}.npz"))
     assert sorted(ours.files) == sorted(ref.files)
     for name in ref.files:
         a, b = ref[name], ours[name]

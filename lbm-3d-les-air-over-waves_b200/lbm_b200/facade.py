@@ -26,11 +26,14 @@ module namespace with:
     to pull whole fields; save_render_snapshot(): the render-snapshot npz of
     run_ab_case.py:140-202.
 
+The seed of the initial kick and of the random backscatter is the one a
+harness hands to taichi.init (run_ab_case.py:261-273), else LBM_RANDOM_SEED.
 The engine itself (buffers on the device, kernels) is created on first use.
 """
 from __future__ import annotations
 
 import os
+import sys
 
 import numpy as np
 
@@ -144,8 +147,37 @@ class Counter:
         return self._engine.dom.counters()[self._key]
 
 
+def harness_seed():
+    """The seed a harness hands to taichi.init, or None.
+
+    run_ab_case.py seeds a solver by replacing taichi.init with a wrapper
+    that adds random_seed=<its --random-seed> to every call, before it
+    loads the solver file (run_ab_case.py:261-273).  This module never
+    starts Taichi, so the wrapper is not called: the value is read from the
+    wrapper's closure."""
+    init = getattr(sys.modules.get("taichi"), "init", None)
+    code, cells = getattr(init, "__code__", None), getattr(init, "__closure__", None)
+    if code is None or not cells:
+        return None
+    for name, cell in zip(code.co_freevars, cells):
+        if name == "random_seed":
+            try:
+                value = cell.cell_contents
+            except ValueError:   # an empty cell
+                return None
+            return value if isinstance(value, int) and not isinstance(value, bool) else None
+    return None
+
+
 def install(ns: dict, environ=None) -> None:
-    cfg = load_config(os.environ if environ is None else environ)
+    """Fill `ns` with the solver module surface.  The seed of the initial
+    kick and of the random backscatter is the harness's (harness_seed())
+    when a harness wrapped taichi.init, else LBM_RANDOM_SEED."""
+    env = dict(os.environ if environ is None else environ)
+    seed = harness_seed()
+    if seed is not None:
+        env["LBM_RANDOM_SEED"] = str(seed)
+    cfg = load_config(env)
     for k, v in cfg.values.items():
         if not k.startswith("_"):
             ns[k] = v

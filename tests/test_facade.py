@@ -40,6 +40,36 @@ def test_module_surface_matches_the_reference_globals(monkeypatch):
     assert callable(m.main) and callable(m.visualize)
 
 
+def _harness_wrap(ti, random_seed):
+    """What run_ab_case.py:261-273 does to taichi.init before loading a solver."""
+    original_init = ti.init
+
+    def init_with_seed(*args, **kwargs):
+        kwargs.setdefault("random_seed", random_seed)
+        return original_init(*args, **kwargs)
+
+    ti.init = init_with_seed
+
+
+def test_seed_comes_from_the_harness_when_it_wrapped_taichi_init(monkeypatch):
+    import sys
+    import types
+
+    from lbm_b200.config import air_wave_env
+
+    def never(*args, **kwargs):
+        raise AssertionError("the module must not start Taichi")
+
+    fake = types.ModuleType("taichi")
+    fake.init = never
+    _harness_wrap(fake, 777)
+    monkeypatch.setitem(sys.modules, "taichi", fake)
+    env = dict(air_wave_env(32, 16, 16), LBM_RANDOM_SEED="5")
+    assert _load(env, monkeypatch, "harness_seed").random_seed == 777
+    monkeypatch.delitem(sys.modules, "taichi")
+    assert _load(env, monkeypatch, "env_seed").random_seed == 5
+
+
 @pytest.mark.gpu
 def test_main_drives_the_engine_like_the_reference_loop(monkeypatch, capsys):
     from lbm_b200.config import air_wave_env

@@ -71,6 +71,157 @@ COUNTERS = (
 )
 
 
+# The columns of the harness's metrics CSV, in its order (run_ab_case.py:15-35).
+METRIC_FIELDNAMES = (
+    "label", "step", "time_phys", "max_speed_phys", "max_speed_x", "max_speed_y", "max_speed_z", "max_speed_fs_type",
+    "max_speed_fs_fill", "max_speed_wet_neighbors", "max_speed_full_neighbors", "max_speed_gas_neighbors", "p_rms",
+    "p_hp_rms", "p_total_rms", "p_total_hp_rms", "p_linear_resid_rms", "p_linear_resid_hp_rms", "vort_rms",
+    "vort_hp_rms", "fs_p_rms", "fs_p_hp_rms", "fs_p_total_rms", "fs_p_total_hp_rms", "fs_p_linear_resid_rms",
+    "fs_p_linear_resid_hp_rms", "fs_vort_rms", "fs_vort_hp_rms", "cut_links", "fs_cut_links", "refill", "fs_refill",
+    "fs_coalesce", "fs_bridge", "vof_detached_count", "vof_detached_mass", "vof_compact_count", "vof_compact_mass",
+    "surface_min", "surface_max", "water_volume", "vof_mass_total", "vof_excess_count", "vof_orphan_count",
+    "vof_collapse_cells", "vof_collapse_candidate_volume", "vof_collapse_applied_volume", "vof_min_interface_fill",
+    "vof_tiny_interface_count", "vof_pending_excess_mass", "vof_pending_excess_count", "surface_symmetry_l2",
+    "surface_eta_hp_rms", "surface_left_max", "surface_right_max",
+)
+
+# metric column -> engine counter, for the counters the row carries in every mode
+_ROW_COUNTERS = {
+    "cut_links": "boundary_cut_link_count", "fs_cut_links": "free_surface_cut_link_count",
+    "refill": "boundary_refill_count", "fs_refill": "free_surface_refill_count",
+    "fs_coalesce": "free_surface_coalescence_repair_count", "fs_bridge": "free_surface_thin_gap_bridge_count",
+    "vof_detached_count": "free_surface_vof_detached_advect_count",
+    "vof_detached_mass": "free_surface_vof_detached_advect_mass",
+    "vof_compact_count": "free_surface_vof_detached_compress_count",
+    "vof_compact_mass": "free_surface_vof_detached_compress_mass",
+}
+# metric column -> engine counter, reported with VOF tracking only
+_VOF_COUNTERS = {
+    "vof_excess_count": "free_surface_vof_excess_count", "vof_orphan_count": "free_surface_vof_orphan_count",
+    "vof_collapse_cells": "free_surface_vof_collapse_cell_count",
+    "vof_collapse_candidate_volume": "free_surface_vof_collapse_candidate_volume_m3",
+    "vof_collapse_applied_volume": "free_surface_vof_collapse_applied_volume_m3",
+}
+_ALWAYS = ("max_speed_phys", "p_rms", "p_hp_rms", "p_total_rms", "p_total_hp_rms", "vort_rms", "vort_hp_rms")
+_FREE_SURFACE = ("max_speed_fs_fill", "fs_p_rms", "fs_p_hp_rms", "fs_p_total_rms", "fs_p_total_hp_rms", "fs_vort_rms",
+                 "fs_vort_hp_rms", "surface_min", "surface_max", "water_volume", "surface_symmetry_l2",
+                 "surface_eta_hp_rms", "surface_left_max", "surface_right_max")
+_FREE_SURFACE_COUNTS = ("max_speed_fs_type", "max_speed_wet_neighbors", "max_speed_full_neighbors",
+                        "max_speed_gas_neighbors")
+_VOF = ("vof_mass_total", "vof_min_interface_fill", "vof_pending_excess_mass")
+_VOF_COUNTS = ("vof_tiny_interface_count", "vof_pending_excess_count")
+
+
+def metric_row(cfg, label: str, step: int, time_phys: float, diag: dict, counters: dict) -> dict:
+    """One row of the harness's metrics CSV (make_visualize,
+    run_ab_case.py:283-679) from a device diagnostics record (lbm_diagnostics)
+    and the engine's counters: the same columns, and per mode the same
+    not-applicable values (-1 for counts, NaN for values) the harness writes.
+    The four linear-wave residual columns are NaN: the device does not
+    compute them."""
+    nan = float("nan")
+    fs = int(cfg.water_free_surface_enabled) == 1
+    vof = fs and str(cfg.free_surface_tracking_mode) == "vof"
+    dx = float(cfg.dx)
+    row = dict.fromkeys(METRIC_FIELDNAMES, nan)
+    row.update(label=label, step=step, time_phys=time_phys)
+    for k in _ALWAYS:
+        row[k] = float(diag[k])
+    row.update(max_speed_x=(int(diag["max_i"]) + 0.5) * dx, max_speed_y=(int(diag["max_j"]) + 0.5) * dx,
+               max_speed_z=(int(diag["max_k"]) + 0.5) * dx)
+    for col, key in _ROW_COUNTERS.items():
+        row[col] = counters[key]
+    for k in _FREE_SURFACE_COUNTS:
+        row[k] = int(diag[k]) if fs else -1
+    if fs:
+        for k in _FREE_SURFACE:
+            row[k] = float(diag[k])
+    for k in _VOF_COUNTS:
+        row[k] = int(diag[k]) if vof else -1
+    for col, key in _VOF_COUNTERS.items():
+        row[col] = counters[key] if vof else (-1 if col in ("vof_excess_count", "vof_orphan_count",
+                                                            "vof_collapse_cells") else nan)
+    if vof:
+        for k in _VOF:
+            row[k] = float(diag[k])
+    return row
+
+
+def make_device_visualize(ns: dict, label: str, output_dir, metrics_writer):
+    """A visualize callback like the harness's make_visualize
+    (run_ab_case.py:283-880) that needs no plotting: each call writes the
+    metric row of the current state, reduced on the device, to
+    `metrics_writer` (a csv.DictWriter over METRIC_FIELDNAMES), writes the
+    render snapshot when LBM_SAVE_RENDER_SNAPSHOT is set, and prints the
+    harness's frame line.  The frame PNGs are not drawn."""
+    from pathlib import Path
+
+    out = Path(output_dir)
+    out.mkdir(parents=True, exist_ok=True)
+
+    def visualize(step, time_phys, Re_phys_air, Re_lb_base):
+        dom = ns["_engine"].domain()
+        r = metric_row(dom.cfg, label, step, time_phys, dom.diagnostics(), dom.counters())
+        metrics_writer.writerow(r)
+        note = ""
+        if str(os.environ.get("LBM_SAVE_RENDER_SNAPSHOT", "")).strip().lower() in ("1", "true", "yes", "on"):
+            note = f", render_snapshot={write_render_snapshot(ns, label=label, step=step, time_phys=time_phys, output_dir=out)}"
+        surface = "column_surface" if str(dom.cfg.free_surface_tracking_mode) == "vof" else "surface"
+        print(
+            f"[{label}] Boundary band <=10 cells: p_dyn_rms={r['p_rms']:.3e} Pa, "
+            f"p_dyn_hp_rms={r['p_hp_rms']:.3e} Pa, p_total_hp_rms={r['p_total_hp_rms']:.3e} Pa, "
+            f"p_lin_resid_hp={r['p_linear_resid_hp_rms']:.3e} Pa, vort_rms={r['vort_rms']:.3e}, "
+            f"vort_hp_rms={r['vort_hp_rms']:.3e}, cut_links={r['cut_links']}, fs_cut_links={r['fs_cut_links']}, "
+            f"refill={r['refill']}, fs_refill={r['fs_refill']}, fs_coalesce={r['fs_coalesce']}, "
+            f"fs_bridge={r['fs_bridge']}, {surface}=[{r['surface_min']:.3f},{r['surface_max']:.3f}] m, "
+            f"volume={r['water_volume']:.3f} m^3, vof_mass={r['vof_mass_total']:.3f}, "
+            f"vof_excess={r['vof_excess_count']}, vof_orphans={r['vof_orphan_count']}, "
+            f"vof_detached={r['vof_detached_count']} ({r['vof_detached_mass']:.3e}), "
+            f"vof_compact={r['vof_compact_count']} ({r['vof_compact_mass']:.3e}), "
+            f"vof_collapse={r['vof_collapse_applied_volume']:.3f}/{r['vof_collapse_candidate_volume']:.3f} m^3 "
+            f"({r['vof_collapse_cells']} cells), vof_min_fill={r['vof_min_interface_fill']:.3f}, "
+            f"vof_tiny={r['vof_tiny_interface_count']}, vof_pending={r['vof_pending_excess_mass']:.3e} "
+            f"({r['vof_pending_excess_count']}), sym_l2={r['surface_symmetry_l2']:.3e} m, "
+            f"eta_hp={r['surface_eta_hp_rms']:.3e} m, fs_p_dyn_hp={r['fs_p_hp_rms']:.3e} Pa, "
+            f"fs_p_total_hp={r['fs_p_total_hp_rms']:.3e} Pa, fs_p_lin_resid_hp={r['fs_p_linear_resid_hp_rms']:.3e} Pa, "
+            f"fs_vort_hp={r['fs_vort_hp_rms']:.3e}, "
+            f"Umax_loc=({r['max_speed_x']:.2f},{r['max_speed_y']:.2f},{r['max_speed_z']:.2f}) m, "
+            f"Umax_type={r['max_speed_fs_type']}, Umax_fill={r['max_speed_fs_fill']:.3f}, "
+            f"Umax_nbrs(wet/full/gas)={r['max_speed_wet_neighbors']}/{r['max_speed_full_neighbors']}/"
+            f"{r['max_speed_gas_neighbors']}, "
+            f"L/R max=[{r['surface_left_max']:.3f},{r['surface_right_max']:.3f}] m{note}",
+            flush=True,
+        )
+
+    return visualize
+
+
+def configure_direct_visualization(ns: dict):
+    """Direct runs of the solver file (CODEX.py:3735-3753): the metrics CSV
+    <LBM_RUN_LABEL>_metrics.csv (label default "direct") in LBM_OUTPUT_DIR
+    (default "frames"), written by make_device_visualize.  Returns the open
+    file, which the caller closes after main()."""
+    import csv
+    from pathlib import Path
+
+    label = os.environ.get("LBM_RUN_LABEL", "direct")
+    output_dir = Path(os.environ.get("LBM_OUTPUT_DIR", "frames")).resolve()
+    output_dir.mkdir(parents=True, exist_ok=True)
+    metrics_file = (output_dir / f"{label}_metrics.csv").open("w", newline="")
+    writer = csv.DictWriter(metrics_file, fieldnames=list(METRIC_FIELDNAMES))
+    writer.writeheader()
+    ns["visualize"] = make_device_visualize(ns, label, output_dir, writer)
+    return metrics_file
+
+
+def _visualize_unbound(step, time_phys, Re_phys_air, Re_lb_base):
+    """The solver's visualize before a harness binds one (CODEX.py:3728-3732)."""
+    raise RuntimeError(
+        "Visualization has not been configured. Use run_ab_case.py or run "
+        "this solver as a script so direct-run visualization can be bound."
+    )
+
+
 class _Engine:
     """Lazily created Domain shared by the field and counter views."""
 
@@ -197,7 +348,7 @@ def install(ns: dict, environ=None) -> None:
     ns["cx"], ns["cy"], ns["cz"] = _Const(D3Q19_CX), _Const(D3Q19_CY), _Const(D3Q19_CZ)
     for key in COUNTERS:
         ns[key] = Counter(eng, key)
-    ns.setdefault("visualize", lambda *a, **k: None)
+    ns.setdefault("visualize", _visualize_unbound)
 
     def main():
         """Initialisation and time loop of the reference (CODEX.py:3757-3954)."""

@@ -9,10 +9,12 @@ PATH is the reference checkout (default: the LBM_REFERENCE_DIR environment
 variable).  For each case, metrics_inputs() builds seeded fields and options:
 an air domain over a wavy bed, height-function water in the hydrostatic-
 balanced and the total-pressure formulation, and VOF with the component-
-balanced one.  The reference's visualize callback (run_ab_case.py:283-596)
-runs on a stand-in solver module that serves those fields as float64 copies
-(so its formulas run in float64, like the restatement they pin); the row it
-hands to the metrics writer is kept and the plotting after it is skipped.
+balanced one; metrics_counters() gives seeded counter values.  The
+reference's visualize callback (run_ab_case.py:283-679) runs on a stand-in
+solver module that serves those fields as float64 copies (so its formulas
+run in float64, like the restatement they pin) and the counters through
+[None]; the row it hands to the metrics writer is kept and the plotting
+after it is skipped.
 The rows go to tests/golden/metrics_rows.json.  run_ab_case.py imports
 matplotlib at the top; it is absent here and the row does not use it, so an
 empty stand-in module takes its place for the import.
@@ -106,6 +108,34 @@ def metrics_inputs(case: str):
     return g, opts
 
 
+COUNTER_INTS = ("boundary_cut_link_count", "free_surface_cut_link_count", "boundary_refill_count",
+                "free_surface_refill_count", "free_surface_coalescence_repair_count",
+                "free_surface_thin_gap_bridge_count", "free_surface_vof_excess_count", "free_surface_vof_orphan_count",
+                "free_surface_vof_collapse_cell_count", "free_surface_vof_detached_advect_count",
+                "free_surface_vof_detached_compress_count")
+COUNTER_FLOATS = ("free_surface_vof_collapse_candidate_volume_m3", "free_surface_vof_collapse_applied_volume_m3",
+                  "free_surface_vof_detached_advect_mass", "free_surface_vof_detached_compress_mass")
+
+
+def metrics_counters(case: str) -> dict:
+    """Seeded values of the solver's scalar counters (floats exact in float32)."""
+    rng = np.random.default_rng(100 + CASES.index(case))
+    out = {k: int(rng.integers(0, 500)) for k in COUNTER_INTS}
+    out.update({k: float(rng.integers(1, 4096)) / 256.0 for k in COUNTER_FLOATS})
+    return out
+
+
+class _Scalar:
+    """A scalar counter as the harness reads it: counter[None]."""
+
+    def __init__(self, value):
+        self._v = value
+
+    def __getitem__(self, index):
+        assert index is None
+        return self._v
+
+
 class _Field:
     def __init__(self, values):
         self._v = np.asarray(values)
@@ -152,6 +182,8 @@ def reference_row(reference: str, case: str) -> dict:
                              ("fs_mass_excess", "free_surface_mass_excess"),
                              ("pressure_reference_head", "pressure_reference_head")):
             setattr(m, theirs, _Field(f64[ours]))
+    for name, value in metrics_counters(case).items():
+        setattr(m, name, _Scalar(value))
     rows = []
 
     class Writer:

@@ -70,6 +70,47 @@ def test_seed_comes_from_the_harness_when_it_wrapped_taichi_init(monkeypatch):
     assert _load(env, monkeypatch, "env_seed").random_seed == 5
 
 
+def test_visualize_before_a_harness_binds_one_raises_like_the_reference(monkeypatch):
+    from lbm_b200.config import air_wave_env
+
+    m = _load(air_wave_env(32, 16, 16), monkeypatch, "unbound")
+    with pytest.raises(RuntimeError, match="Visualization has not been configured"):
+        m.visualize(100, 1.0, 1.0, 1.0)
+
+
+def test_direct_run_writes_the_harness_metrics_csv(monkeypatch, tmp_path, capsys):
+    """configure_direct_visualization binds a visualize that writes one CSV row
+    per plot in the harness's columns (the device record comes from a
+    stand-in engine here; its values are checked in test_metrics_golden)."""
+    import csv
+    import types
+
+    from lbm_b200 import facade
+    from lbm_b200.abi import COUNTER_FLOAT_NAMES, COUNTER_INT_NAMES, DIAG_FIELDS
+    from lbm_b200.config import water_gaussian_env
+
+    m = _load(water_gaussian_env(32, 8, 16), monkeypatch, "direct")
+    rec = {name: 0 if ctype.__name__.startswith("c_int") else 0.25 for name, ctype in DIAG_FIELDS}
+    rec.update(max_i=3, max_j=1, max_k=5)
+    counters = dict({k: 7 for k in COUNTER_INT_NAMES}, **{k: 0.5 for k in COUNTER_FLOAT_NAMES})
+    dom = types.SimpleNamespace(cfg=m._engine.cfg, diagnostics=lambda: rec, counters=lambda: counters)
+    monkeypatch.setattr(m._engine, "domain", lambda: dom)
+    monkeypatch.setenv("LBM_OUTPUT_DIR", str(tmp_path))
+    monkeypatch.setenv("LBM_RUN_LABEL", "direct_t")
+    fh = facade.configure_direct_visualization(vars(m))
+    m.visualize(100, 1.5, 1.0, 1.0)
+    m.visualize(200, 3.0, 1.0, 1.0)
+    fh.close()
+    with open(tmp_path / "direct_t_metrics.csv", newline="") as f:
+        rows = list(csv.DictReader(f))
+    assert [r["step"] for r in rows] == ["100", "200"]
+    assert tuple(rows[0]) == facade.METRIC_FIELDNAMES
+    dx = float(m.dx)
+    assert float(rows[0]["max_speed_x"]) == 3.5 * dx and float(rows[0]["max_speed_z"]) == 5.5 * dx
+    assert rows[0]["cut_links"] == "7" and rows[0]["vof_excess_count"] == "-1" and rows[0]["vof_mass_total"] == "nan"
+    assert capsys.readouterr().out.count("[direct_t] Boundary band <=10 cells:") == 2
+
+
 @pytest.mark.gpu
 def test_main_drives_the_engine_like_the_reference_loop(monkeypatch, capsys):
     from lbm_b200.config import air_wave_env

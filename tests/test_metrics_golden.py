@@ -20,8 +20,11 @@ import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "golden"))
-from gen_metrics_golden import CASES, metrics_inputs  # noqa: E402
+from gen_metrics_golden import CASES, metrics_counters, metrics_inputs  # noqa: E402
 from metrics_restatement import metrics_from_fields  # noqa: E402
+
+from lbm_b200.abi import DIAG_FIELDS  # noqa: E402
+from lbm_b200.facade import METRIC_FIELDNAMES, metric_row  # noqa: E402
 
 with open(os.path.join(HERE, "golden", "metrics_rows.json"), encoding="utf-8") as _fh:
     ROWS = json.load(_fh)
@@ -67,3 +70,38 @@ def test_restatement_matches_the_reference_row(case):
         compared += 1
     # every metric of the mode is compared: air has no free-surface metrics, the height path no VOF ones
     assert compared == {"air_periodic": 10, "vof_component_balanced": 32}.get(case, 27), compared
+
+
+def _device_record(case):
+    """A diagnostics record as lbm_diagnostics returns it, with the values of
+    the restatement (every field present, whatever the mode)."""
+    g, opts = metrics_inputs(case)
+    ours = metrics_from_fields(g, types.SimpleNamespace(**opts))
+    rec = {name: -1 if ctype.__name__.startswith("c_int") else float("nan") for name, ctype in DIAG_FIELDS}
+    rec.update(ours)
+    rec["max_speed_fs_fill"] = float(g["fs_fill"][ours["max_k"], ours["max_j"], ours["max_i"]])
+    return rec, opts
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_metric_row_matches_the_reference_row(case):
+    """The CSV row the drop-in module writes (facade.metric_row over a device
+    record and the counters) against the harness's row: every column, with
+    the same not-applicable values per mode; the linear-wave residual columns
+    are NaN in ours (not computed on the device)."""
+    rec, opts = _device_record(case)
+    row = metric_row(types.SimpleNamespace(**opts), case, 40, 12.5, rec, metrics_counters(case))
+    ref = ROWS[case]
+    assert tuple(row) == METRIC_FIELDNAMES and sorted(ref) == sorted(METRIC_FIELDNAMES)
+    for key in METRIC_FIELDNAMES:
+        v, r = row[key], ref[key]
+        if "linear_resid" in key:
+            assert math.isnan(v), key
+        elif r is None:
+            assert isinstance(v, float) and math.isnan(v), (key, v)
+        elif isinstance(r, str) or isinstance(r, int) and not isinstance(r, bool) and key != "time_phys":
+            assert v == r and type(v) is type(r), (key, v, r)
+        elif key == "max_speed_phys":
+            assert abs(v - r) <= 2e-7 * abs(r), (key, v, r)
+        else:
+            assert abs(v - r) <= 1e-9 * max(1.0, abs(r)), (key, v, r)

@@ -112,13 +112,78 @@ _VOF = ("vof_mass_total", "vof_min_interface_fill", "vof_pending_excess_mass")
 _VOF_COUNTS = ("vof_tiny_interface_count", "vof_pending_excess_count")
 
 
-def metric_row(cfg, label: str, step: int, time_phys: float, diag: dict, counters: dict) -> dict:
+LINEAR_RESIDUAL_COLUMNS = ("p_linear_resid_rms", "p_linear_resid_hp_rms", "fs_p_linear_resid_rms",
+                           "fs_p_linear_resid_hp_rms")
+
+
+def _high_pass_xz(field: np.ndarray, x_periodic: bool) -> np.ndarray:
+    """Grid-scale residual of an xz slice (run_ab_case.py:111-137): the value
+    minus the mean of its four neighbours, with linear extrapolation past
+    the top and bottom rows and past solid x ends, wrap-around in periodic x."""
+    zp, zm = np.empty_like(field), np.empty_like(field)
+    zp[:-1], zp[-1] = field[1:], 2.0 * field[-1] - field[-2]
+    zm[1:], zm[0] = field[:-1], 2.0 * field[0] - field[1]
+    if x_periodic:
+        xp, xm = np.roll(field, -1, axis=1), np.roll(field, 1, axis=1)
+    else:
+        xp, xm = np.empty_like(field), np.empty_like(field)
+        xp[:, :-1], xp[:, -1] = field[:, 1:], 2.0 * field[:, -1] - field[:, -2]
+        xm[:, 1:], xm[:, 0] = field[:, :-1], 2.0 * field[:, 0] - field[:, 1]
+    return field - 0.25 * (zp + zm + xp + xm)
+
+
+def linear_residual_metrics(cfg, rho_xz, phi_xz, inactive_xz, surface_line, bed_line) -> dict:
+    """The four linear-wave residual columns of the metric row
+    (run_ab_case.py:52-108, 505-595) from the mid-y xz slice: the lattice
+    pressure minus the pressure of linear finite-depth theory under the
+    instantaneous surface line (hostinit.linear_wave_heads, plus the still-
+    water head unless the formulation is hydrostatic-balanced), as RMS over
+    the near-bed band 0 < phi <= 10 dx and over the free-surface band, plain
+    and high-passed.  NaN where the harness has none: no free surface, VOF
+    tracking, or a bed line that is not flat.  One slice, on the host."""
+    from .hostinit import linear_wave_heads
+
+    out = dict.fromkeys(LINEAR_RESIDUAL_COLUMNS, float("nan"))
+    if int(cfg.water_free_surface_enabled) != 1 or str(cfg.free_surface_tracking_mode) == "vof":
+        return out
+    bed_line = np.asarray(bed_line, dtype=np.float64)
+    if not np.allclose(bed_line, bed_line[0], atol=1.0e-12, rtol=0.0):
+        return out
+    rho_xz = np.asarray(rho_xz, dtype=np.float64)
+    nz, nx = rho_xz.shape
+    dx, base = float(cfg.dx), float(cfg.free_surface_base_m)
+    rho_phys, gravity = float(cfg.rho_phys), float(cfg.gravity_phys)
+    z = (np.arange(nz, dtype=np.float64) + 0.5) * dx
+    bed = float(bed_line[0])
+    surface = np.asarray(surface_line, dtype=np.float64)
+    heads = np.array(linear_wave_heads(surface - base, dx, bed, max(base - bed, dx), z,
+                                       str(cfg.x_boundary_mode) == "solid"))
+    if int(cfg.use_hydrostatic_balanced_pressure) != 1:
+        heads = np.maximum(base - z, 0.0)[:, None] + heads
+    p_lattice = rho_phys * float(cfg.vel_scale) ** 2 * ((1.0 / 3.0) * (rho_xz - float(cfg.rho0)))
+    resid = p_lattice - rho_phys * gravity * heads
+    resid_hp = _high_pass_xz(resid, str(cfg.x_boundary_mode) == "periodic")
+    inactive = np.asarray(inactive_xz, dtype=bool)
+    zz = z[:, None]
+    bands = {"": (np.asarray(phi_xz) > 0.0) & (np.asarray(phi_xz) <= 10.0 * dx) & ~inactive,
+             "fs_": (zz <= surface[None, :] + 0.5 * dx) & (zz >= surface[None, :] - 3.0 * dx) & ~inactive}
+    for prefix, band in bands.items():
+        if band.any():
+            v, h = resid[band], resid_hp[band]
+            if np.isfinite(v).any():
+                out[prefix + "p_linear_resid_rms"] = float(np.sqrt(np.nanmean((v - np.nanmean(v)) ** 2)))
+                out[prefix + "p_linear_resid_hp_rms"] = float(np.sqrt(np.nanmean(h ** 2)))
+    return out
+
+
+def metric_row(cfg, label: str, step: int, time_phys: float, diag: dict, counters: dict,
+               linear: dict | None = None) -> dict:
     """One row of the harness's metrics CSV (make_visualize,
-    run_ab_case.py:283-679) from a device diagnostics record (lbm_diagnostics)
-    and the engine's counters: the same columns, and per mode the same
-    not-applicable values (-1 for counts, NaN for values) the harness writes.
-    The four linear-wave residual columns are NaN: the device does not
-    compute them."""
+    run_ab_case.py:283-679) from a device diagnostics record (lbm_diagnostics),
+    the engine's counters and the linear-wave residual columns
+    (linear_residual_metrics; NaN when not given): the same columns, and per
+    mode the same not-applicable values (-1 for counts, NaN for values) the
+    harness writes."""
     nan = float("nan")
     fs = int(cfg.water_free_surface_enabled) == 1
     vof = fs and str(cfg.free_surface_tracking_mode) == "vof"
@@ -144,7 +209,28 @@ def metric_row(cfg, label: str, step: int, time_phys: float, diag: dict, counter
     if vof:
         for k in _VOF:
             row[k] = float(diag[k])
+    if linear:
+        for k in LINEAR_RESIDUAL_COLUMNS:
+            row[k] = float(linear[k])
     return row
+
+
+def _linear_residual_from_device(eng, cfg) -> dict | None:
+    """linear_residual_metrics from the mid-y slices of the device fields
+    (a few rows copied to the host), or None where the harness has none."""
+    if int(cfg.water_free_surface_enabled) != 1 or str(cfg.free_surface_tracking_mode) == "vof":
+        return None
+    mj = int(cfg.Ny) // 2
+
+    def row(name, diag=False):
+        return eng.buffer(name, diag)[..., mj, :].detach().cpu().numpy()
+
+    bed_line = row("water_h")
+    if not np.allclose(bed_line, bed_line[0], atol=1.0e-12, rtol=0.0):
+        return None
+    obstacle = row("obstacle", True) != 0
+    inactive = obstacle | ((row("fs_type") == 0) & ~obstacle)
+    return linear_residual_metrics(cfg, row("rho"), row("phi", True), inactive, row("fs_h"), bed_line)
 
 
 def make_device_visualize(ns: dict, label: str, output_dir, metrics_writer):
@@ -153,7 +239,8 @@ def make_device_visualize(ns: dict, label: str, output_dir, metrics_writer):
     metric row of the current state, reduced on the device, to
     `metrics_writer` (a csv.DictWriter over METRIC_FIELDNAMES), writes the
     render snapshot when LBM_SAVE_RENDER_SNAPSHOT is set, and prints the
-    harness's frame line.  The frame PNGs are not drawn."""
+    harness's frame line.  The linear-wave residual columns come from one
+    mid-y slice of the fields on the host.  The frame PNGs are not drawn."""
     from pathlib import Path
 
     out = Path(output_dir)
@@ -161,7 +248,8 @@ def make_device_visualize(ns: dict, label: str, output_dir, metrics_writer):
 
     def visualize(step, time_phys, Re_phys_air, Re_lb_base):
         dom = ns["_engine"].domain()
-        r = metric_row(dom.cfg, label, step, time_phys, dom.diagnostics(), dom.counters())
+        r = metric_row(dom.cfg, label, step, time_phys, dom.diagnostics(), dom.counters(),
+                       _linear_residual_from_device(ns["_engine"], dom.cfg))
         metrics_writer.writerow(r)
         note = ""
         if str(os.environ.get("LBM_SAVE_RENDER_SNAPSHOT", "")).strip().lower() in ("1", "true", "yes", "on"):

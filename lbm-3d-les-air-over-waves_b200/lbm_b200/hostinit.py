@@ -21,6 +21,40 @@ def make_init_noise(cfg, seed: int | None = None) -> np.ndarray:
     return rng.uniform(-1.0, 1.0, size=(3, cfg.Nz, cfg.Ny, cfg.Nx)).astype(np.float32)
 
 
+def linear_wave_heads(eta: np.ndarray, dx: float, bed: float, depth: float, z, solid_x: bool) -> list:
+    """Pressure heads of linear finite-depth wave theory under the surface
+    elevation eta(x) (cell centres, spacing dx), at each height in z: the
+    modes of eta (a cosine series for walls at x = 0 and Lx, Fourier modes for
+    periodic x), each scaled by cosh(k z_rel) / cosh(k depth) with z_rel =
+    z - bed clipped to [0, depth].  One row of len(eta) per height; the
+    reference evaluates the same theory for its linear-wave initial pressure
+    (CODEX.py:754-803) and its linear-pressure diagnostic
+    (run_ab_case.py:52-108)."""
+    nx = len(eta)
+    x = (np.arange(nx, dtype=np.float64) + 0.5) * dx
+
+    def vertical_factor(wavenumbers, zc):
+        z_rel = min(max(zc - bed, 0.0), depth)
+        factor = np.ones_like(wavenumbers)
+        active = wavenumbers > 0.0
+        kh = wavenumbers[active] * depth
+        kz = wavenumbers[active] * z_rel
+        # cosh(k z_rel) / cosh(k h), written with decaying exponentials
+        factor[active] = (np.exp(kz - kh) + np.exp(-kz - kh)) / (1.0 + np.exp(-2.0 * kh))
+        return factor
+
+    if solid_x:
+        # cosine series for walls at x = 0 and x = Lx
+        kx = np.arange(nx, dtype=np.float64) * np.pi / (nx * dx)
+        basis = np.cos(np.outer(kx, x))
+        coeff = (2.0 / nx) * (basis @ eta)
+        coeff[0] = np.mean(eta)
+        return [coeff @ (vertical_factor(kx, zc)[:, None] * basis) for zc in z]
+    modes = np.fft.rfftfreq(nx, d=dx) * 2.0 * np.pi
+    eta_hat = np.fft.rfft(eta)
+    return [np.fft.irfft(eta_hat * vertical_factor(modes, zc), n=nx) for zc in z]
+
+
 def prepare_initial_density(cfg, fs_h: np.ndarray, water_h: np.ndarray) -> np.ndarray:
     """rho_initial[k, j, i] (float32) from the column heights at t = 0."""
     Nx, Ny, Nz, dx = cfg.Nx, cfg.Ny, cfg.Nz, cfg.dx
@@ -31,7 +65,6 @@ def prepare_initial_density(cfg, fs_h: np.ndarray, water_h: np.ndarray) -> np.nd
         return rho_np
     h_np = np.asarray(fs_h, dtype=np.float64)
     bed_np = np.asarray(water_h, dtype=np.float64)
-    x = (np.arange(Nx, dtype=np.float64) + 0.5) * dx
     z = (np.arange(Nz, dtype=np.float64) + 0.5) * dx
     balanced = cfg.use_hydrostatic_balanced_pressure == 1
     use_linear = (
@@ -43,28 +76,7 @@ def prepare_initial_density(cfg, fs_h: np.ndarray, water_h: np.ndarray) -> np.nd
         bed = float(bed_np[0, 0])
         depth0 = max(base - bed, dx)
         eta = h_np.mean(axis=0) - base
-
-        def vertical_factor(wavenumbers, zc):
-            z_rel = min(max(zc - bed, 0.0), depth0)
-            factor = np.ones_like(wavenumbers)
-            active = wavenumbers > 0.0
-            kh = wavenumbers[active] * depth0
-            kz = wavenumbers[active] * z_rel
-            # cosh(k z_rel) / cosh(k h), written with decaying exponentials
-            factor[active] = (np.exp(kz - kh) + np.exp(-kz - kh)) / (1.0 + np.exp(-2.0 * kh))
-            return factor
-
-        if cfg.x_boundary_mode == "solid":
-            # cosine series for walls at x = 0 and x = Lx
-            kx = np.arange(Nx, dtype=np.float64) * np.pi / (Nx * dx)
-            basis = np.cos(np.outer(kx, x))
-            coeff = (2.0 / Nx) * (basis @ eta)
-            coeff[0] = np.mean(eta)
-            heads = [coeff @ (vertical_factor(kx, zc)[:, None] * basis) for zc in z]
-        else:
-            modes = np.fft.rfftfreq(Nx, d=dx) * 2.0 * np.pi
-            eta_hat = np.fft.rfft(eta)
-            heads = [np.fft.irfft(eta_hat * vertical_factor(modes, zc), n=Nx) for zc in z]
+        heads = linear_wave_heads(eta, dx, bed, depth0, z, cfg.x_boundary_mode == "solid")
         for kk, zc in enumerate(z):
             head = heads[kk]
             if not balanced:

@@ -3,6 +3,7 @@ solver (run_ab_case.py:261-280), driven through steps / plot_freq /
 plot_step_start / visualize / main() (899-912), read through module globals,
 .to_numpy() fields and [None] counters (283-679)."""
 import importlib.util
+import math
 import os
 
 import numpy as np
@@ -89,11 +90,26 @@ def test_direct_run_writes_the_harness_metrics_csv(monkeypatch, tmp_path, capsys
     from lbm_b200.abi import COUNTER_FLOAT_NAMES, COUNTER_INT_NAMES, DIAG_FIELDS
     from lbm_b200.config import water_gaussian_env
 
+    import torch
+
     m = _load(water_gaussian_env(32, 8, 16), monkeypatch, "direct")
     rec = {name: 0 if ctype.__name__.startswith("c_int") else 0.25 for name, ctype in DIAG_FIELDS}
     rec.update(max_i=3, max_j=1, max_k=5)
-    counters = dict({k: 7 for k in COUNTER_INT_NAMES}, **{k: 0.5 for k in COUNTER_FLOAT_NAMES})
-    dom = types.SimpleNamespace(cfg=m._engine.cfg, diagnostics=lambda: rec, counters=lambda: counters)
+    counters = dict({k: 7 for k in COUNTER_INT_NAMES}, **{k: 0.5 for k in COUNTER_FLOAT_NAMES}, step=100)
+    nz, ny, nx = m.Nz, m.Ny, m.Nx
+    gen = torch.Generator().manual_seed(3)
+    z = (torch.arange(nz) + 0.5) * m.dx
+    level = 0.6 * nz * float(m.dx)
+    fields = {  # a flat bed at 2 m, a surface at 0.6 of the height, a perturbed density
+        "water_h": torch.full((ny, nx), 2.0),
+        "fs_h": level + 0.2 * torch.rand(ny, nx, generator=gen),
+        "rho": 1.0 + 1e-3 * torch.rand(nz, ny, nx, generator=gen),
+        "phi": (z - 2.0)[:, None, None].expand(nz, ny, nx).clone(),
+        "obstacle": (z < 2.0)[:, None, None].expand(nz, ny, nx).to(torch.int32),
+        "fs_type": (z < level)[:, None, None].expand(nz, ny, nx).to(torch.int32),
+    }
+    dom = types.SimpleNamespace(cfg=m._engine.cfg, diagnostics=lambda: rec, counters=lambda: counters,
+                                field=fields.__getitem__, synchronize=lambda: None, export_diagnostics=lambda: None)
     monkeypatch.setattr(m._engine, "domain", lambda: dom)
     monkeypatch.setenv("LBM_OUTPUT_DIR", str(tmp_path))
     monkeypatch.setenv("LBM_RUN_LABEL", "direct_t")
@@ -108,6 +124,7 @@ def test_direct_run_writes_the_harness_metrics_csv(monkeypatch, tmp_path, capsys
     dx = float(m.dx)
     assert float(rows[0]["max_speed_x"]) == 3.5 * dx and float(rows[0]["max_speed_z"]) == 5.5 * dx
     assert rows[0]["cut_links"] == "7" and rows[0]["vof_excess_count"] == "-1" and rows[0]["vof_mass_total"] == "nan"
+    assert all(math.isfinite(float(rows[0][k])) for k in facade.LINEAR_RESIDUAL_COLUMNS)
     assert capsys.readouterr().out.count("[direct_t] Boundary band <=10 cells:") == 2
 
 

@@ -24,7 +24,7 @@ from gen_metrics_golden import CASES, metrics_counters, metrics_inputs  # noqa: 
 from metrics_restatement import metrics_from_fields  # noqa: E402
 
 from lbm_b200.abi import DIAG_FIELDS  # noqa: E402
-from lbm_b200.facade import METRIC_FIELDNAMES, metric_row  # noqa: E402
+from lbm_b200.facade import METRIC_FIELDNAMES, linear_residual_metrics, metric_row  # noqa: E402
 
 with open(os.path.join(HERE, "golden", "metrics_rows.json"), encoding="utf-8") as _fh:
     ROWS = json.load(_fh)
@@ -83,21 +83,44 @@ def _device_record(case):
     return rec, opts
 
 
+def _linear(case):
+    """linear_residual_metrics on the mid-y slices of the case's fields."""
+    g, opts = metrics_inputs(case)
+    mj = opts["Ny"] // 2
+    obstacle = g["obstacle"][:, mj, :] != 0
+    inactive = obstacle
+    if opts["water_free_surface_enabled"]:
+        inactive = obstacle | ((g["fs_type"][:, mj, :] == 0) & ~obstacle)
+    return linear_residual_metrics(types.SimpleNamespace(**opts), g["rho"][:, mj, :], g["phi"][:, mj, :], inactive,
+                                   g["fs_h"][mj, :], g["water_h"][mj, :])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_linear_residual_matches_the_reference_row(case):
+    """The harness's finite-depth linear pressure residual (run_ab_case.py:52-108,
+    505-595): present for the height-function cases, NaN for air and VOF."""
+    ours, ref = _linear(case), ROWS[case]
+    for key, v in ours.items():
+        if ref[key] is None:
+            assert math.isnan(v), (key, v)
+        else:
+            assert abs(v - ref[key]) <= 1e-9 * max(1.0, abs(ref[key])), (key, v, ref[key])
+    assert (ref["p_linear_resid_rms"] is not None) == case.startswith("water_height")
+
+
 @pytest.mark.parametrize("case", CASES)
 def test_metric_row_matches_the_reference_row(case):
     """The CSV row the drop-in module writes (facade.metric_row over a device
-    record and the counters) against the harness's row: every column, with
-    the same not-applicable values per mode; the linear-wave residual columns
-    are NaN in ours (not computed on the device)."""
+    record, the counters and the linear-wave residual of one slice) against
+    the harness's row: every column, with the same not-applicable values per
+    mode."""
     rec, opts = _device_record(case)
-    row = metric_row(types.SimpleNamespace(**opts), case, 40, 12.5, rec, metrics_counters(case))
+    row = metric_row(types.SimpleNamespace(**opts), case, 40, 12.5, rec, metrics_counters(case), _linear(case))
     ref = ROWS[case]
     assert tuple(row) == METRIC_FIELDNAMES and sorted(ref) == sorted(METRIC_FIELDNAMES)
     for key in METRIC_FIELDNAMES:
         v, r = row[key], ref[key]
-        if "linear_resid" in key:
-            assert math.isnan(v), key
-        elif r is None:
+        if r is None:
             assert isinstance(v, float) and math.isnan(v), (key, v)
         elif isinstance(r, str) or isinstance(r, int) and not isinstance(r, bool) and key != "time_phys":
             assert v == r and type(v) is type(r), (key, v, r)

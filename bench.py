@@ -494,8 +494,9 @@ def run_serving(requests: int, min_steps: int, max_steps: int, storage: str) -> 
     rep = Server(budget_bytes=150e9, chunk=50, arith=ARITH).run(reqs)
     return {
         "value": rep["mlups"], "unit": UNIT, "p50_s": rep["p50_s"], "p99_s": rep["p99_s"], "wall_s": rep["wall_s"],
-        "requests": rep["requests"], "rounds": rep["rounds"], "peak_active": rep["peak_active"],
-        "setup_s": rep["setup_s"], "storage": storage, "arithmetic": ARITH, "steps_range": [min_steps, max_steps],
+        "requests": rep["requests"], "failed": len(rep["failed"]), "rounds": rep["rounds"],
+        "peak_active": rep["peak_active"], "setup_s": rep["setup_s"], "storage": storage, "arithmetic": ARITH,
+        "steps_range": [min_steps, max_steps],
         "workload": f"Poisson(20/s) arrivals, {requests} requests, half air-over-wave, half water Gaussian, cells "
                     f"log-uniform [1e5, 2e7], steps uniform [{min_steps}, {max_steps}], seed 3, HBM budget 150 GB",
     }
@@ -534,7 +535,7 @@ def serving(args):
         "metric": "MLUPS (served trace)", "value": r["value"], "unit": UNIT, "n_gpus": 1,
         "higher_is_better": True, "mode": "serving", "data": "synthetic",
         "p50_s": r["p50_s"], "p99_s": r["p99_s"], "wall_s": r["wall_s"], "requests": r["requests"],
-        "rounds": r["rounds"], "peak_active": r["peak_active"], "setup_s": r["setup_s"],
+        "failed": r["failed"], "rounds": r["rounds"], "peak_active": r["peak_active"], "setup_s": r["setup_s"],
         "config": {"workload": r["workload"], "storage": storage, "hbm_budget_gb": 150, "round_steps": 50},
     }
     print(json.dumps(line), flush=True)

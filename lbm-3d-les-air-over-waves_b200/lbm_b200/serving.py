@@ -36,6 +36,7 @@ class Request:
     admitted_s: float = -1.0
     done_s: float = -1.0
     result: dict = field(default_factory=dict)
+    error: str | None = None     # why the solve failed (set-up or a step call raised); None when it finished
 
     @property
     def latency_s(self) -> float:
@@ -169,8 +170,22 @@ class Server:
         chunks = 0
         peak_active = 0
         setup_s = 0.0
+        failed = []
         pool = ThreadPoolExecutor(max_workers=1)
         t0 = self.clock()
+
+        def fail(q, dom, exc):
+            nonlocal used
+            q.error = f"{type(exc).__name__}: {exc}"
+            q.done_s = self.clock() - t0
+            if dom is not None:
+                try:
+                    dom.close()
+                except Exception:  # noqa: BLE001 - the solve has already failed
+                    pass
+            used -= need[q.rid]
+            failed.append(q)
+
         try:
             while pending or building or active or finishing:
                 progress = False
@@ -182,12 +197,17 @@ class Server:
                     used += need[q.rid]
                     building.append((q, pool.submit(self._build, q.env)))
                     progress = True
-                # solves whose set-up finished join the active set, in admission order
+                # solves whose set-up finished join the active set, in admission order; a
+                # set-up that raised fails its request alone and releases its memory
                 while building and building[0][1].done():
                     q, fut = building.popleft()
-                    dom, build_s = fut.result()
-                    setup_s += build_s
-                    active.append({"q": q, "dom": dom, "rem": q.steps, "ev": deque()})
+                    try:
+                        dom, build_s = fut.result()
+                    except Exception as exc:  # noqa: BLE001 - reported on the request
+                        fail(q, None, exc)
+                    else:
+                        setup_s += build_s
+                        active.append({"q": q, "dom": dom, "rem": q.steps, "ev": deque()})
                     progress = True
                 peak_active = max(peak_active, len(active))
                 # keep `depth` calls queued per solve
@@ -195,12 +215,17 @@ class Server:
                 for it in active:
                     while it["ev"] and self._done(it["ev"][0]):
                         it["ev"].popleft()
-                    while it["rem"] > 0 and len(it["ev"]) < self.depth:
-                        k = min(self.chunk, it["rem"])
-                        it["ev"].append(self._issue(it["dom"], k))
-                        it["rem"] -= k
-                        chunks += 1
+                    try:
+                        while it["rem"] > 0 and len(it["ev"]) < self.depth:
+                            k = min(self.chunk, it["rem"])
+                            it["ev"].append(self._issue(it["dom"], k))
+                            it["rem"] -= k
+                            chunks += 1
+                            progress = True
+                    except Exception as exc:  # noqa: BLE001 - a step call of this solve raised
+                        fail(it["q"], it["dom"], exc)
                         progress = True
+                        continue
                     if it["rem"] == 0 and not it["ev"]:
                         host, ev = self._start_result(it["dom"])
                         finishing.append((it["q"], it["dom"], host, ev))
@@ -233,10 +258,19 @@ class Server:
                         time.sleep(idle_sleep_s)
         finally:
             pool.shutdown(wait=True)
+            # leaving early (an exception of the loop itself): release every solve still held
+            for q, fut in building:
+                if fut.done() and fut.exception() is None:
+                    fut.result()[0].close()
+            for it in active:
+                it["dom"].close()
+            for _, dom, _, _ in finishing:
+                dom.close()
         wall = self.clock() - t0
         lat = np.array([q.latency_s for q in finished]) if finished else np.zeros(1)
         return {
             "requests": len(finished), "wall_s": wall, "mlups": lups / wall / 1e6 if wall > 0 else 0.0,
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "rounds": chunks, "peak_active": peak_active, "setup_s": setup_s, "finished": finished,
+            "failed": failed,
         }

@@ -90,6 +90,35 @@ def test_server_admits_by_budget_and_finishes_every_request():
     assert rep["p99_s"] >= rep["p50_s"] > 0
 
 
+def test_a_failing_solve_fails_its_request_alone():
+    """A set-up that raises and a step call that raises each fail their own
+    request (error recorded, memory released); the other requests finish."""
+    reqs = poisson_trace(8, rate_hz=200.0, seed=9, cells_range=(2e4, 6e4), steps_range=(40, 200))
+    bad_build, bad_step = reqs[2].rid, reqs[5].rid
+    by_env = {id(q.env): q.rid for q in reqs}
+
+    class Flaky(_FakeDomain):
+        def __init__(self, env):
+            if by_env[id(env)] == bad_build:
+                raise RuntimeError("set-up refused")
+            super().__init__(env)
+            self.rid = by_env[id(env)]
+
+        def step(self, k):
+            if self.rid == bad_step and self.steps > 0:
+                raise RuntimeError("step refused")
+            super().step(k)
+
+    _FakeDomain.live = _FakeDomain.peak = _FakeDomain.live_bytes = _FakeDomain.peak_bytes = 0
+    need = max(domain_bytes(load_config(q.env)) for q in reqs)
+    rep = Server(budget_bytes=2.2 * need, chunk=25, domain_factory=Flaky, clock=_Clock()).run(reqs, idle_sleep_s=0.0)
+    assert sorted(q.rid for q in rep["failed"]) == sorted([bad_build, bad_step])
+    assert {q.rid: q.error for q in rep["failed"]} == {bad_build: "RuntimeError: set-up refused",
+                                                        bad_step: "RuntimeError: step refused"}
+    assert rep["requests"] == 6 and all(q.error is None and q.result["steps"] == q.steps for q in rep["finished"])
+    assert _FakeDomain.live == 0 and _FakeDomain.live_bytes == 0
+
+
 def test_server_rejects_a_request_over_the_budget():
     q = poisson_trace(1, seed=1, cells_range=(1e6, 1e6))[0]
     with pytest.raises(ValueError):

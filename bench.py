@@ -175,11 +175,45 @@ def oracle_sample_rate(budget_s: float, max_steps: int):
     return rate, sample
 
 
+def reference_configs(args):
+    """The oracle on the stated-size configurations (C1 air, C2 water, C3
+    VOF) on all host cores: one untimed step, then steps until a few seconds
+    have passed (at most --steps), MLUPS per step extrapolated from them.
+    One JSON line."""
+    from oracle_runner import OracleSim
+
+    names = args.only.split(",") if args.only else list(CONFIGS)
+    out = {}
+    for name in names:
+        what, storage = CONFIGS[name]
+        sim = OracleSim(_config_env(name, storage))
+        sim.step(1)
+        n = sim.cfg.Nx * sim.cfg.Ny * sim.cfg.Nz
+        k, t0 = 0, time.perf_counter()
+        while k < max(1, args.steps) and (k == 0 or time.perf_counter() - t0 < 10.0):
+            sim.step(1)
+            k += 1
+        dt = time.perf_counter() - t0
+        sim.close()
+        out[name] = {"workload": what, "storage": storage, "cells": n, "steps": k, "ms_per_step": dt / k * 1e3,
+                     "value": n * k / dt / 1e6, "unit": UNIT,
+                     "sample": f"{k} steps after 1 untimed step, extrapolated per step"}
+    print(json.dumps({"metric": METRIC, "mode": "configs", "impl": "reference", "n_gpus": 0, "data": "synthetic",
+                      "cpu_baseline": {"kind": "port", "cores": host_cores(),
+                                       "note": "FP32 C++ restatement of the reference kernels (oracle), OpenMP"},
+                      "configs": out}), flush=True)
+    return 0
+
+
 def reference_arm(args):
     """Reference CPU implementation of the path on the host cores."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.mode == "configs":
+        if TESTS not in sys.path:
+            sys.path.insert(0, TESTS)
+        return reference_configs(args)
     if TESTS not in sys.path:
         sys.path.insert(0, TESTS)
     from oracle_runner import OracleSim

@@ -40,3 +40,15 @@ def test_reference_arm_other_ranks_exit_quietly():
     p = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert p.returncode == 0, p.stderr[-2000:]
     assert not [ln for ln in p.stdout.splitlines() if ln.strip().startswith("{")]
+
+
+def test_reference_arm_times_the_stated_configs():
+    """--mode configs on the reference arm: the oracle on each stated-size
+    configuration, one JSON line with MLUPS per configuration."""
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--mode", "configs",
+                        "--only", "C1", "--steps", "1"], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    rec = json.loads([ln for ln in p.stdout.splitlines() if ln.strip().startswith("{")][-1])
+    assert rec["impl"] == "reference" and rec["mode"] == "configs" and rec["cpu_baseline"]["cores"] >= 1
+    c1 = rec["configs"]["C1"]
+    assert c1["cells"] == 128 * 64 * 64 and c1["steps"] == 1 and c1["value"] > 0 and c1["unit"] == "MLUPS"

@@ -800,6 +800,7 @@ const char *lbm_last_error(lbm_ctx *ctx) { return ctx ? ctx->impl->err.c_str() :
 
 /* oracle only: the deterministic FP64 tree sum, exposed for tests */
 double lbm_oracle_tree_sum(const double *v, int64_t n) {
+    if (!v || n <= 0) return 0.0;
     std::vector<double> x(v, v + n);
     return tree_sum(x);
 }

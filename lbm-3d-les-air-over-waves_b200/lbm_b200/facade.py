@@ -302,6 +302,82 @@ def configure_direct_visualization(ns: dict):
     return metrics_file
 
 
+def tau_line(cfg) -> str:
+    """The line the reference prints when it is imported (CODEX.py:471)."""
+    return f"tau used in current simulation: {cfg.tau0:.10f}"
+
+
+def run_summary(cfg) -> list:
+    """The configuration summary the reference's main() prints after its
+    initialisation (CODEX.py:3794-3871), line for line, from the same
+    globals, so that logs of either solver read alike."""
+    c = cfg
+    out = [f"Grid Size (Nx, Ny, Nz):  {c.Nx} {c.Ny} {c.Nz}",
+           f"Physics mode: {c.physics_mode} ({c.fluid_name})",
+           f"Free-surface mode: {c.free_surface_mode}, initial={c.free_surface_initial_condition}, "
+           f"tracking={c.free_surface_tracking_mode}"]
+    if int(c.water_free_surface_enabled) == 1:
+        out.append(
+            f"Free surface: base={c.free_surface_base_m:.3f} m, depth={c.free_surface_depth_m:.3f} m, "
+            f"solitary_amp={c.solitary_amp_m:.3f} m, H/h={c.solitary_height_depth_ratio:.3f}, "
+            f"solitary_c={c.solitary_celerity_phys:.3f} m/s, "
+            f"solitary_dir={c.solitary_direction:+.0f}, solitary_1/kappa={c.solitary_length_scale_m:.3f} m, "
+            f"solitary_u0={c.solitary_initial_velocity_mode}, "
+            f"boundary={c.free_surface_boundary_mode}, refill={c.free_surface_refill_mode}, "
+            f"initial_pressure={c.initial_pressure_mode}, pressure_formulation={c.pressure_formulation}")
+        if c.pressure_formulation_auto_corrected:
+            out.append("Pressure formulation auto-corrected from total_pressure to vof_component_balanced for "
+                       "disconnected VOF. Set LBM_ALLOW_TOTAL_PRESSURE_VOF_DIAGNOSTIC=1 only for a known-bad "
+                       "full-pressure diagnostic.")
+        if c.free_surface_tracking_mode == "vof":
+            out.append(
+                f"VOF state change: empty_fill_threshold={c.vof_empty_fill_threshold:.4f}, "
+                f"orphan_empty_threshold={c.vof_orphan_empty_threshold:.4f}, "
+                f"orphan_search_radius={c.vof_orphan_search_radius}, "
+                f"orphan_max_weak_neighbors={c.vof_orphan_max_weak_neighbors}, "
+                f"detached_advection={bool(c.vof_detached_advection_enabled)}, "
+                f"detached_max_wet_neighbors={c.vof_detached_max_wet_neighbors}, "
+                f"detached_max_resolved_neighbors={c.vof_detached_max_resolved_neighbors}, "
+                f"detached_residual_fill_threshold={c.vof_detached_residual_fill_threshold:.4f}, "
+                f"link_aperture={int(c.vof_link_aperture_enabled) == 1}, "
+                f"thin_gap_bridge={bool(c.vof_thin_gap_bridge_enabled)}, "
+                f"bridge_strength={c.vof_thin_gap_bridge_strength:.3f}, "
+                f"collapse_trapped_gas={bool(c.vof_collapse_trapped_gas_enabled)}, "
+                f"collapse_interval={c.vof_collapse_interval}, "
+                f"collapse_max_volume={c.vof_collapse_max_volume_m3:.3f} m^3, "
+                f"collapse_flood_sweeps={c.vof_collapse_flood_sweeps}")
+            if c.vof_initial_shape == "block":
+                out.append(
+                    f"VOF initial block: center=({c.vof_block_center_x_m:.3f}, {c.vof_block_center_y_m:.3f}, "
+                    f"{c.vof_block_center_z_m:.3f}) m, size=({c.vof_block_size_x_m:.3f}, "
+                    f"{c.vof_block_size_y_m:.3f}, {c.vof_block_size_z_m:.3f}) m")
+        if c.free_surface_initial_condition == "gaussian":
+            out.append(f"Gaussian hump: amp={c.gaussian_amp_m:.3f} m, center_x={c.gaussian_center_x_m:.3f} m, "
+                       f"sigma={c.gaussian_sigma_m:.3f} m, zero initial velocity")
+    out.append(f"Bed profile: {c.bed_profile}, bed_level={c.offset_m:.3f} m")
+    if c.bed_profile == "piecewise_linear":
+        m = c.piecewise_bed_metadata
+        out.append(f"Piecewise bottom: file={m['path']}, points={m['point_count']}, x_first={m['first_x']:.3f} m, "
+                   f"x_last={m['last_x']:.3f} m, z_min={m['min_z']:.3f} m, z_max={m['max_z']:.3f} m, "
+                   f"z_at_Lx={m['z_at_lx']:.3f} m")
+    out.append(f"Obstacle mode: {c.obstacle_mode}")
+    if int(c.include_cube_geometry) == 1:
+        out.append(f"Cube size/center/yaw/pitch: size=({c.cube_size_x_m:.3f}, {c.cube_size_y_m:.3f}, "
+                   f"{c.cube_size_z_m:.3f}) m, center=({c.cube_center_x_m:.3f}, {c.cube_center_y_m:.3f}, "
+                   f"{c.cube_center_z_m:.3f}) m, yaw={c.cube_yaw_deg:.3f} deg, pitch={c.cube_pitch_deg:.3f} deg")
+    out += [f"Boundary geometry mode: {c.boundary_geometry_mode}",
+            f"X boundary mode: {c.x_boundary_mode}",
+            f"Wall velocity sampling: {c.wall_velocity_sampling}",
+            f"Initial free-surface population projection: {bool(c.initialize_free_surface_populations)}",
+            f"Collision model: {c.collision_model}",
+            f"Fluid rho={c.rho_phys:.3f} kg/m^3, nu={c.nu_phys:.6e} m^2/s, gravity={c.gravity_phys:.3f} m/s^2",
+            f"Reference speed={c.U_ref_phys:.3f} m/s, dt={c.dt_phys:.6e} s, g_lb={c.g_lb:.6e}, "
+            f"g_body_lb={c.g_body_lb:.6e}",
+            f"Physical Re ({c.fluid_name}): {c.Re_phys_air:.3e}",
+            f"Lattice Re (base): {c.Re_lb_base:.2f}"]
+    return out
+
+
 def _visualize_unbound(step, time_phys, Re_phys_air, Re_lb_base):
     """The solver's visualize before a harness binds one (CODEX.py:3728-3732)."""
     raise RuntimeError(
@@ -417,6 +493,7 @@ def install(ns: dict, environ=None) -> None:
     if seed is not None:
         env["LBM_RANDOM_SEED"] = str(seed)
     cfg = load_config(env)
+    print(tau_line(cfg), flush=True)
     for k, v in cfg.values.items():
         if not k.startswith("_"):
             ns[k] = v
@@ -443,6 +520,7 @@ def install(ns: dict, environ=None) -> None:
         dom = eng.domain()
         dom.initialize()
         eng.export_step = -1
+        print("\n".join(run_summary(cfg)), flush=True)
         steps = int(ns["steps"])
         plot_freq = max(1, int(ns["plot_freq"]))
         plot_start = int(ns["plot_step_start"])

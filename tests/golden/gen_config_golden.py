@@ -13,7 +13,10 @@ variables.  The import evaluates the option surface (CODEX.py:35-529,
 lbm_env.py:9-22) and stops before main().  tests/golden/config_cases.json
 then holds, per case, either every scalar module global (numbers, flags,
 strings; the piecewise bed and its metadata when the bed is piecewise) or
-the exception's class and message.  A case's "files" are written to a
+the exception's class and message; for valid cases also the lines the
+import printed (without Taichi's cache line) and, on the small grids, the
+lines main() prints when it has no steps to run (its initialisation and
+configuration summary).  A case's "files" are written to a
 scratch folder first and "{name}" in an option value or a message stands
 for that file's absolute path, so the fixture does not depend on where it
 was made.
@@ -200,7 +203,8 @@ def scalar_globals(mod, placeholders: dict) -> dict:
 
 
 def import_reference(reference: str, env: dict):
-    """Import the reference module with `env` as its only LBM_* options."""
+    """Import the reference module with `env` as its only LBM_* options.
+    Returns the module and what the import printed."""
     saved = dict(os.environ)
     try:
         for key in list(os.environ):
@@ -212,15 +216,30 @@ def import_reference(reference: str, env: dict):
         sys.path.insert(0, reference)
         spec = importlib.util.spec_from_file_location("ref_options", os.path.join(reference, SOLVER_FILE))
         mod = importlib.util.module_from_spec(spec)
-        with warnings.catch_warnings(), contextlib.redirect_stdout(io.StringIO()):
+        printed = io.StringIO()
+        with warnings.catch_warnings(), contextlib.redirect_stdout(printed):
             warnings.simplefilter("ignore")
             spec.loader.exec_module(mod)
-        return mod
+        return mod, printed.getvalue()
     finally:
         os.environ.clear()
         os.environ.update(saved)
         if reference in sys.path:
             sys.path.remove(reference)
+
+
+def main_stdout(mod) -> str:
+    """What the module's main() prints with no steps to run: its
+    initialisation and configuration summary (CODEX.py:3757-3871).  The
+    initial kick's random draws are fixed at 0.5; they print nothing."""
+    taichi_shim._state["random_hook"] = lambda kernel, cell: 0.5
+    taichi_shim._state["calls"] = {}
+    mod.steps, mod.plot_freq, mod.plot_step_start = 0, 1, 0
+    printed = io.StringIO()
+    with warnings.catch_warnings(), contextlib.redirect_stdout(printed), np.errstate(all="ignore"):
+        warnings.simplefilter("ignore")
+        mod.main()
+    return printed.getvalue()
 
 
 def main():
@@ -237,11 +256,15 @@ def main():
             options, placeholders = materialize(env, files, folder)
             case = {"name": name, "env": env, "files": files}
             try:
-                mod = import_reference(reference, options)
+                mod, printed = import_reference(reference, options)
             except Exception as exc:  # noqa: BLE001 - the exception is the expected output
                 case["error"] = {"type": type(exc).__name__, "message": unplace(str(exc), placeholders)}
             else:
                 case["values"] = scalar_globals(mod, placeholders)
+                case["import_stdout"] = [ln for ln in unplace(printed, placeholders).splitlines()
+                                         if not ln.startswith("Taichi offline cache:")]
+                if not name.startswith("defaults_"):   # the defaults' grids are too large for the numpy stand-in
+                    case["main_stdout"] = unplace(main_stdout(mod), placeholders).splitlines()
         cases.append(case)
         print(f"{name}: {'error ' + case['error']['type'] if 'error' in case else len(case['values'])}", flush=True)
     with open(OUT, "w", encoding="utf-8") as fh:

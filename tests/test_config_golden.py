@@ -17,6 +17,7 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 from gen_config_golden import CASES, materialize, unplace  # noqa: E402
 
 from lbm_b200.config import load_config  # noqa: E402
+from lbm_b200.facade import run_summary, tau_line  # noqa: E402
 
 with open(os.path.join(HERE, "golden", "config_cases.json"), encoding="utf-8") as _fh:
     GOLDEN = json.load(_fh)["cases"]
@@ -81,3 +82,24 @@ def test_golden_covers_every_error_message_of_the_option_surface():
     seen = {c["error"]["message"].split(" ")[0] for c in GOLDEN if "error" in c}
     ours_only = {"LBM_B200_TAU0", "LBM_B200_INIT_U0", "LBM_B200_TOP"}   # build options, not in the reference
     assert fixed - ours_only <= seen, sorted(fixed - ours_only - seen)
+
+
+PRINTED = [c for c in GOLDEN if "main_stdout" in c]
+
+
+@pytest.mark.parametrize("case", PRINTED, ids=[c["name"] for c in PRINTED])
+def test_printed_lines_match_the_reference(case, tmp_path):
+    """The line the module prints at import and the configuration summary
+    its main() prints after initialisation (CODEX.py:471, 3794-3871, 3957),
+    line for line, as the reference printed them for the same options."""
+    options, placeholders = materialize(case["env"], case["files"], str(tmp_path))
+    cfg = load_config(options)
+    assert [tau_line(cfg)] == case["import_stdout"]
+    ours = [unplace(ln, placeholders) for ln in run_summary(cfg)] + ["Simulation Complete."]
+    assert ours == case["main_stdout"]
+
+
+def test_printed_cases_cover_every_mode():
+    names = {c["name"] for c in PRINTED}
+    assert {"air_piecewise_bed", "air_cube_yaw_pitch", "water_gaussian_hydrostatic_boundary", "vof_options",
+            "vof_block_total_pressure_corrected"} <= names

@@ -599,15 +599,14 @@ def write_render_snapshot(ns, *, label: str, step: int, time_phys: float, output
     return str(path)
 
 
-def _health(ns, dom, step):
-    """The reference's periodic health line (CODEX.py:3930-3954).  The
-    maximum speed over active cells is reduced on the device
-    (lbm_diagnostics); only scalars come back to the host."""
-    max_u = float(dom.diagnostics()["max_speed_lb"])
-    c = dom.counters()
-    print(
+def health_line(step: int, max_u, vel_scale: float, c: dict) -> str:
+    """The reference's periodic health line (CODEX.py:3930-3954) from the
+    maximum speed over active cells (lattice units, float32 as the
+    reference reduces it) and the counters."""
+    max_u = np.float32(max_u)
+    return (
         f"Time Step {step}, Max |U| (LB units) = {max_u:.4f}, "
-        f"Max U (phys) ~ {max_u * ns['vel_scale']:.2f} m/s, "
+        f"Max U (phys) ~ {max_u * np.float32(vel_scale):.2f} m/s, "
         f"cut_links={c['boundary_cut_link_count']}, refill={c['boundary_refill_count']}, "
         f"fs_refill={c['free_surface_refill_count']}, fs_coalesce={c['free_surface_coalescence_repair_count']}, "
         f"fs_bridge={c['free_surface_thin_gap_bridge_count']}, "
@@ -618,6 +617,12 @@ def _health(ns, dom, step):
         f"vof_compact={c['free_surface_vof_detached_compress_count']} "
         f"({c['free_surface_vof_detached_compress_mass']:.3e}), "
         f"vof_collapse_cells={c['free_surface_vof_collapse_cell_count']}, "
-        f"vof_collapse_vol={c['free_surface_vof_collapse_applied_volume_m3']:.3f} m^3",
-        flush=True,
+        f"vof_collapse_vol={c['free_surface_vof_collapse_applied_volume_m3']:.3f} m^3"
     )
+
+
+def _health(ns, dom, step):
+    """The health line of the current state.  The maximum speed over active
+    cells is reduced on the device (lbm_diagnostics); only scalars come back
+    to the host."""
+    print(health_line(step, dom.diagnostics()["max_speed_lb"], ns["vel_scale"], dom.counters()), flush=True)

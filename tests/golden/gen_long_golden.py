@@ -1,0 +1,67 @@
+"""Generate 100-step goldens with the reference solver's own kernels.
+
+Run where a checkout of the reference is available (it is read, never
+written; GPU machines do not need it):
+
+    python tests/golden/gen_long_golden.py --reference PATH [--only NAME] [--steps N]
+
+PATH is the reference checkout (default: the LBM_REFERENCE_DIR environment
+variable).  For each case (a golden case of gen_golden.py), main() runs N
+steps (default 100) exactly as gen_golden.py runs it (taichi_shim for
+Taichi, the same seeded initial kick and backscatter draws), and
+tests/golden/long/<case>.npz keeps:
+  env, noise, seed, nsteps   as in the short goldens
+  s<N>_<field>              the state after the last step
+  health                    the health lines main() printed (every 100 steps,
+                            CODEX.py:3930-3954)
+"""
+from __future__ import annotations
+
+import argparse
+import contextlib
+import io
+import os
+
+import numpy as np
+
+import gen_golden as gg
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LONG_CASES = ("air_kbc_default", "water_height_gaussian", "vof_block_kbc")
+
+
+def run_long(name: str, steps: int) -> dict:
+    gg.STEPS[name] = steps
+    printed = io.StringIO()
+    with contextlib.redirect_stdout(printed):
+        out = gg.run_case(name, gg.CASES[name])
+    last = f"s{steps}_"
+    keep = {k: v for k, v in out.items() if k.startswith(last) or k in ("env", "noise", "seed", "nsteps",
+                                                                          "injected")}
+    keep["health"] = np.array([ln for ln in printed.getvalue().splitlines() if ln.startswith("Time Step")])
+    return keep
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("LBM_REFERENCE_DIR", ""),
+                    help="reference checkout (default: $LBM_REFERENCE_DIR)")
+    ap.add_argument("--only", default=None)
+    ap.add_argument("--steps", type=int, default=100)
+    args = ap.parse_args()
+    gg.REFERENCE = os.path.abspath(args.reference) if args.reference else ""
+    if not gg.REFERENCE or not os.path.exists(os.path.join(gg.REFERENCE, gg.SOLVER_FILE)):
+        raise SystemExit(f"{gg.SOLVER_FILE} not found: pass --reference PATH or set LBM_REFERENCE_DIR")
+    os.makedirs(os.path.join(HERE, "long"), exist_ok=True)
+    for name in LONG_CASES:
+        if args.only and name != args.only:
+            continue
+        data = run_long(name, args.steps)
+        path = os.path.join(HERE, "long", f"{name}.npz")
+        np.savez_compressed(path, **data)
+        print(f"wrote {path} ({os.path.getsize(path) / 1024:.0f} KiB), health lines: {len(data['health'])}",
+              flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -6,12 +6,14 @@ written; GPU machines do not need it):
     python tests/golden/gen_long_golden.py --reference PATH [--only NAME] [--steps N]
 
 PATH is the reference checkout (default: the LBM_REFERENCE_DIR environment
-variable).  For each case (a golden case of gen_golden.py), main() runs N
+variable).  For each golden case of gen_golden.py, main() runs N
 steps (default 100) exactly as gen_golden.py runs it (taichi_shim for
 Taichi, the same seeded initial kick and backscatter draws), and
 tests/golden/long/<case>.npz keeps:
   env, noise, seed, nsteps   as in the short goldens
   s<N>_<field>              the state after the last step
+  s0_<field>                the initial state, for the cases edited after the
+                            reference's init (they start from it)
   health                    the health lines main() printed (every 100 steps,
                             CODEX.py:3930-3954)
 """
@@ -27,7 +29,7 @@ import numpy as np
 import gen_golden as gg
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LONG_CASES = ("air_kbc_default", "water_height_gaussian", "vof_block_kbc")
+LONG_CASES = tuple(gg.CASES)
 
 
 def run_long(name: str, steps: int) -> dict:
@@ -36,8 +38,10 @@ def run_long(name: str, steps: int) -> dict:
     with contextlib.redirect_stdout(printed):
         out = gg.run_case(name, gg.CASES[name])
     last = f"s{steps}_"
-    keep = {k: v for k, v in out.items() if k.startswith(last) or k in ("env", "noise", "seed", "nsteps",
-                                                                          "injected")}
+    # an edited case starts from its s0 snapshot (the edit follows the reference's init)
+    first = "s0_" if name in gg.INJECT else last
+    keep = {k: v for k, v in out.items() if k.startswith(last) or k.startswith(first) or
+            k in ("env", "noise", "seed", "nsteps", "injected", "rho_initial")}
     keep["health"] = np.array([ln for ln in printed.getvalue().splitlines() if ln.startswith("Time Step")])
     return keep
 

@@ -1,10 +1,11 @@
 """The oracle against the reference's own kernels after 100 steps.
 
 tests/golden/long/<case>.npz were made by tests/golden/gen_long_golden.py:
-the reference's main() runs 100 steps of three golden cases (air with the
-reference's defaults: KBC, LES, backscatter, fringe, top drive and sponge;
-height-function water; the VOF falling block with collapse and bridge) and
-keeps the final state and the health line it printed.  The oracle must
+the reference's main() runs 100 steps of the golden cases (among them air
+with the reference's defaults: KBC, LES, backscatter, fringe, top drive and
+sponge; height-function water; the VOF falling block with collapse and
+bridge; the edited VOF pools whose orphan, detached-cell and collapse
+kernels act) and keeps the final state and the health line it printed.  The oracle must
 reproduce the state bit for bit (the scalar FP64 tallies to f32 rounding,
 as in the short goldens), and the drop-in module's health-line formatter
 must print the same line from the oracle's state.  The GPU library is
@@ -15,7 +16,7 @@ import os
 import numpy as np
 import pytest
 
-from golden_compare import EXACT, FIELD_MAP
+from golden_compare import EXACT, FIELD_MAP, FILE_OPTIONS, GOLDEN_DIR, golden_state, is_injected, load_state_numpy
 from lbm_b200.facade import health_line
 from oracle_runner import OracleSim
 
@@ -38,9 +39,15 @@ def test_long_goldens_present():
 def test_oracle_matches_the_reference_after_100_steps(name):
     data = np.load(os.path.join(LONG_DIR, f"{name}.npz"))
     env = json.loads(str(data["env"]))
+    for key in FILE_OPTIONS:   # files stored beside the short goldens
+        if key in env and not os.path.isabs(env[key]):
+            env[key] = os.path.join(GOLDEN_DIR, env[key])
     n = int(data["nsteps"])
     sim = OracleSim(env, noise=data["noise"])
     try:
+        if is_injected(data):
+            # state edited after the reference's init: start from its s0 snapshot
+            load_state_numpy(sim.arrays, "f1" if sim.counters()["current_f"] else "f0", golden_state(data, "s0"))
         sim.step(n)
         sim.export()
         arrays = dict(sim.arrays)

@@ -9,7 +9,7 @@ PATH is the reference checkout (default: the LBM_REFERENCE_DIR environment
 variable).  For each golden case of gen_golden.py, main() runs N
 steps (default 100) exactly as gen_golden.py runs it (taichi_shim for
 Taichi, the same seeded initial kick and backscatter draws), and
-tests/golden/long/<case>.npz keeps:
+tests/golden/long/<case>.npz (<case>_<N>.npz for other N) keeps:
   env, noise, seed, nsteps   as in the short goldens
   s<N>_<field>              the state after the last step
   s0_<field>                the initial state, for the cases edited after the
@@ -61,7 +61,7 @@ def main():
         if args.only and name != args.only:
             continue
         data = run_long(name, args.steps)
-        path = os.path.join(HERE, "long", f"{name}.npz")
+        path = os.path.join(HERE, "long", f"{name}.npz" if args.steps == 100 else f"{name}_{args.steps}.npz")
         np.savez_compressed(path, **data)
         print(f"wrote {path} ({os.path.getsize(path) / 1024:.0f} KiB), health lines: {len(data['health'])}",
               flush=True)

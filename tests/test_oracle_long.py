@@ -79,6 +79,6 @@ def test_oracle_matches_the_reference_after_100_steps(name):
             active &= a["fs_type"] != 0
         speed = np.sqrt(a["ux"] ** 2 + a["uy"] ** 2 + a["uz"] ** 2)
         line = health_line(n, np.nanmax(speed[active]), cfg.vel_scale, c)
-        assert [line] == [str(s) for s in data["health"]]
+        assert len(data["health"]) == n // 100 and line == str(data["health"][-1])
     finally:
         sim.close()

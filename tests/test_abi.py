@@ -23,6 +23,21 @@ def test_header_declares_the_abi():
     assert set(abi.ABI_SYMBOLS) <= set(names), set(abi.ABI_SYMBOLS) - set(names)
 
 
+@pytest.mark.parametrize("lang,std", [("c", "-std=c99"), ("c++", "-std=c++17")])
+def test_header_compiles_as_plain_c_and_cpp(lang, std):
+    """The boundary is a plain C header: it compiles alone, warning-free, as
+    C99 (what a cgo / ctypes / JNI binding would include) and as C++."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc" if lang == "c" else "g++")
+    if cc is None:
+        pytest.skip("no host compiler")
+    p = subprocess.run([cc, "-x", lang, std, "-fsyntax-only", "-Wall", "-Wextra", "-Werror", HEADER],
+                       capture_output=True, text=True)
+    assert p.returncode == 0, p.stderr
+
+
 def test_oracle_exports_every_declared_symbol():
     lib = oracle_lib()
     for name in declared_functions():

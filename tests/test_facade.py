@@ -128,6 +128,62 @@ def test_direct_run_writes_the_harness_metrics_csv(monkeypatch, tmp_path, capsys
     assert capsys.readouterr().out.count("[direct_t] Boundary band <=10 cells:") == 2
 
 
+class _OracleEngine:
+    """The CPU oracle behind the drop-in module's engine interface (test
+    stand-in for the CUDA Domain): same state arrays, same step calls; the
+    health line's maximum speed is reduced on the host as the reference does."""
+
+    def __init__(self, env, noise):
+        from oracle_runner import OracleSim
+
+        self.sim = OracleSim(env, noise=noise)
+        self.cfg = self.sim.cfg
+
+    def initialize(self):
+        pass   # OracleSim ran the init sequence
+
+    def step(self, n):
+        self.sim.step(n)
+
+    def counters(self):
+        return self.sim.counters()
+
+    def diagnostics(self, slice_j=None):
+        a = self.sim.arrays
+        active = a["obstacle"] == 0
+        if int(self.cfg.water_free_surface_enabled) == 1:
+            active &= a["fs_type"] != 0
+        speed = np.sqrt(a["ux"] ** 2 + a["uy"] ** 2 + a["uz"] ** 2)
+        return {"max_speed_lb": float(np.nanmax(speed[active]))}
+
+    def export_diagnostics(self):
+        self.sim.export()
+
+    def synchronize(self):
+        pass
+
+
+@pytest.mark.parametrize("case", ["air_kbc_default", "vof_block_kbc"])
+def test_main_loop_prints_the_reference_health_line(monkeypatch, capsys, case):
+    """The drop-in module's main() driven like the reference's loop, with the
+    CPU oracle as its engine, prints at step 100 the health line the
+    reference printed for the same case (tests/golden/long)."""
+    import json
+
+    from golden_compare import GOLDEN_DIR
+
+    data = np.load(os.path.join(GOLDEN_DIR, "long", f"{case}.npz"))
+    env = json.loads(str(data["env"]))
+    m = _load(env, monkeypatch, f"oracle_{case}")
+    m._engine.dom = _OracleEngine(env, data["noise"])
+    m.steps, m.plot_freq, m.plot_step_start = 100, 1000, 0
+    m.main()
+    out = capsys.readouterr().out.splitlines()
+    assert [ln for ln in out if ln.startswith("Time Step")] == [str(data["health"][0])]
+    assert out[-1] == "Simulation Complete."
+    m._engine.dom.sim.close()
+
+
 @pytest.mark.gpu
 def test_main_drives_the_engine_like_the_reference_loop(monkeypatch, capsys):
     from lbm_b200.config import air_wave_env

@@ -78,6 +78,8 @@ def test_oracle_matches_the_reference_after_100_steps(name):
         if int(cfg.water_free_surface_enabled) == 1:
             active &= a["fs_type"] != 0
         speed = np.sqrt(a["ux"] ** 2 + a["uy"] ** 2 + a["uz"] ** 2)
+        # a run that diverged would match vacuously (NaN states): the reference's run must still be finite
+        assert np.isfinite(speed[active]).all() and np.isfinite(data[f"{tag}_f"]).all()
         line = health_line(n, np.nanmax(speed[active]), cfg.vel_scale, c)
         assert len(data["health"]) == n // 100 and line == str(data["health"][-1])
     finally:

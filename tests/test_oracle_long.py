@@ -1,7 +1,8 @@
-"""The oracle against the reference's own kernels after 100 steps.
+"""The oracle against the reference's own kernels after 100 to 1000 steps.
 
 tests/golden/long/<case>.npz were made by tests/golden/gen_long_golden.py:
-the reference's main() runs 100 steps of the golden cases (among them air
+the reference's main() runs 100 steps of every golden case, and up to 1000
+steps of a few (among them air
 with the reference's defaults: KBC, LES, backscatter, fringe, top drive and
 sponge; height-function water; the VOF falling block with collapse and
 bridge; the edited VOF pools whose orphan, detached-cell and collapse
@@ -9,7 +10,7 @@ kernels act) and keeps the final state and the health line it printed.  The orac
 reproduce the state bit for bit (the scalar FP64 tallies to f32 rounding,
 as in the short goldens), and the drop-in module's health-line formatter
 must print the same line from the oracle's state.  The GPU library is
-bit-equal to the oracle, so this pins it over 100 steps too."""
+bit-equal to the oracle, so this pins it over such runs too."""
 import json
 import os
 
@@ -36,7 +37,7 @@ def test_long_goldens_present():
 
 
 @pytest.mark.parametrize("name", LONG)
-def test_oracle_matches_the_reference_after_100_steps(name):
+def test_oracle_matches_the_reference_after_a_long_run(name):
     data = np.load(os.path.join(LONG_DIR, f"{name}.npz"))
     env = json.loads(str(data["env"]))
     for key in FILE_OPTIONS:   # files stored beside the short goldens

@@ -2,15 +2,15 @@
 
 tests/golden/long/<case>.npz were made by tests/golden/gen_long_golden.py:
 the reference's main() runs 100 steps of every golden case, and up to 1000
-steps of a few (among them air
-with the reference's defaults: KBC, LES, backscatter, fringe, top drive and
-sponge; height-function water; the VOF falling block with collapse and
-bridge; the edited VOF pools whose orphan, detached-cell and collapse
-kernels act) and keeps the final state and the health line it printed.  The oracle must
-reproduce the state bit for bit (the scalar FP64 tallies to f32 rounding,
-as in the short goldens), and the drop-in module's health-line formatter
-must print the same line from the oracle's state.  The GPU library is
-bit-equal to the oracle, so this pins it over such runs too."""
+steps of a few (among them air with the reference's defaults: KBC, LES,
+backscatter, fringe, top drive and sponge; height-function water; the VOF
+falling block with collapse and bridge; the edited VOF pools whose orphan,
+detached-cell and collapse kernels act), and keeps the final state and the
+health line it printed.  The oracle must reproduce the state bit for bit
+(the scalar FP64 tallies to f32 rounding, as in the short goldens), and the
+drop-in module's health-line formatter must print the same line from the
+oracle's state.  The GPU library is bit-equal to the oracle, so this pins it
+over such runs too."""
 import json
 import os
 

@@ -28,7 +28,6 @@ configurations specify lattice-unit values the reference only hard-codes:
 """
 from __future__ import annotations
 
-import math
 import os
 from dataclasses import dataclass, field
 from typing import Mapping
